@@ -1,0 +1,319 @@
+"""Benchmark: cell-updates/s of the ECOGEN Cartesian FV step on one B200 (or N replicas).
+
+Default workload (the configuration the headline metric is quoted on): 2D shock-bubble
+interaction, Kapila 2-phase, MUSCL-Hancock + van Leer, FP64, 2048 x 2048 cells on 1 x 1 cm,
+CFL 0.6 — seeded synthetic input generated by ecogen_b200.cases.shock_bubble_2d and read through
+the library's own XML reader.  One "step" is one full time step of the whole grid
+(predictor + corrector + relaxations + dt update).  The state (2048^2 x 8 doubles = 268 MB per
+copy) is larger than L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5]
+
+Multi-GPU: the path does not shard (one case per GPU; a single large domain would need halo
+exchange, which this workload does not use), so N ranks run N independent replicas ("replicas
+only"); value = total cell-updates of all ranks / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s on 1 B200: plain FP64 vs MLP-seeded relaxation, same residual"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_case(config: str, size: int | None):
+    from ecogen_b200 import cases
+    if config == "c1":
+        return cases.shock_tube_1d(ncells=size or 1000, iterations=10 ** 6)
+    if config == "c3":
+        return cases.cavity_collapse_3d(n=size or 256, iterations=10 ** 6)
+    if config == "c5":
+        return cases.expansion_tube_2d(n=size or 1024, iterations=10 ** 6)
+    return cases.shock_bubble_2d(n=size or 2048, iterations=10 ** 6)
+
+
+def bytes_per_cell_update(case) -> int:
+    """Algorithmic bytes: read + write of (alpha_k, rho_k)_k, p, u (d components), E."""
+    return 16 * (2 * case.nphases + 2 + case.dim)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------------- reference arm
+
+
+def reference_sample(steps: int, warmup: int, size: int = 256, iters: int = 4, procs: int | None = None,
+                     config: str = "c2"):
+    """Time the reference CPU solver (oracle/_ref/ECOGEN, built from the reference sources).
+
+    Each sample runs `procs` independent reference processes concurrently (one per host core) on a
+    `size`^2 version of the workload for `iters` iterations, and once for 1 iteration; the
+    difference removes initialisation and output, giving cell-updates/s over all cores.
+    """
+    from ecogen_b200 import cases
+    from oracle import refrun
+    if not refrun.available():
+        return None
+    procs = procs or len(os.sched_getaffinity(0))
+    base = tempfile.mkdtemp(prefix="ecg_ref_", dir=os.path.join(ROOT, "_work") if os.path.isdir(os.path.join(ROOT, "_work")) else None)
+
+    def prepare(nit):
+        dirs = []
+        for p in range(procs):
+            w = os.path.join(base, f"n{nit}_p{p}")
+            c = make_case(config, size)
+            c.iterations = nit
+            c.name = f"refsample{p}"
+            d = c.write(w)
+            cases.write_ecogen_list(w, [d])
+            dirs.append(w)
+        return dirs
+
+    def run_all(dirs):
+        t0 = time.perf_counter()
+        ps = [subprocess.Popen([refrun.REF_BINARY, os.path.abspath(w) + os.sep], cwd=w, stdout=subprocess.DEVNULL,
+                               stderr=subprocess.DEVNULL) for w in dirs]
+        for p in ps:
+            p.wait()
+        return time.perf_counter() - t0
+
+    d1, dn = prepare(1), prepare(iters)
+    c = make_case(config, size)
+    cells = c.ncells
+    samples = []
+    for i in range(warmup + steps):
+        t1 = run_all(d1)
+        tn = run_all(dn)
+        if i >= warmup:
+            samples.append(procs * cells * (iters - 1) / max(tn - t1, 1e-9))
+    shutil.rmtree(base, ignore_errors=True)
+    return {"value": statistics.median(samples), "cores": procs,
+            "sample": f"{procs} concurrent reference processes, {size}^2 cells each, {iters}-1 iterations "
+                      f"(time of an {iters}-iteration run minus a 1-iteration run)", "samples": samples}
+
+
+# ------------------------------------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = env_rank()
+    case = make_case(args.config, args.size)
+    workload = {"c1": "1D water/air shock tube, Kapila, first order",
+                "c2": "2D shock-bubble, Kapila 2-phase, MUSCL + van Leer",
+                "c3": "3D three-phase cavity collapse, Kapila, MUSCL + minmod",
+                "c5": "2D liquid/vapour expansion, Kapila + p-T-mu relaxation, MUSCL + van Leer"}[args.config]
+    config = {"workload": f"{workload}, {'x'.join(str(n) for n in case.cells if n > 1)} cells, FP64",
+              "cells": case.ncells, "phases": case.nphases, "dim": case.dim, "order": 2 if case.second_order else 1,
+              "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = reference_sample(args.steps, args.warmup, config=args.config)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/ECOGEN not built"}))
+            return
+        line = {"metric": METRIC, "value": r["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
+                "cpu_baseline": {"value": r["value"], "unit": "cell-updates/s", "cores": r["cores"],
+                                 "kind": "reference", "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    from ecogen_b200 import api
+
+    work = tempfile.mkdtemp(prefix=f"ecg_bench_{rank}_")
+    d = case.write(work)
+    inp = api.Input(d, os.path.join(work, "libEOS"))
+    fields0 = inp.fill()
+    ctx = api.Context(inp.case)
+    ctx.upload(fields0)
+    ctx.step(args.warmup)
+    stream = torch.cuda.ExternalStream(api.lib().ecg_stream(ctx.h))
+
+    # ---- device-timed region: K steps replayed from captured graphs, events on the context stream
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        st = ctx.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = case.ncells * args.steps * world / (ms_max * 1e-3)
+
+    # ---- per-kernel attribution (separate launches, events between kernels)
+    st_p, kms = ctx.step_profiled(max(2, min(args.steps, 10)))
+    nprof = max(2, min(args.steps, 10))
+    step_ms = sum(kms) / nprof
+    pass_ms = [k / nprof for k in kms]
+
+    # ---- end to end through the C ABI with host buffers: upload from pinned host memory, one
+    #      ecg_step call per step (host -> device dt/t, device -> host dt/t/counters), download
+    nf = len(fields0)
+    pinned_in = [torch.from_numpy(f).pin_memory() for f in fields0]
+    pinned_out = [torch.empty(case.ncells, dtype=torch.float64).pin_memory() for _ in range(nf)]
+    in_np = [p.numpy() for p in pinned_in]
+    out_np = [p.numpy() for p in pinned_out]
+    ctx2 = api.Context(inp.case)
+    ctx2.upload(in_np)
+    ctx2.step(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    ptrs_in = api._field_ptrs(in_np)
+    api.check(api.lib().ecg_upload_prim(ctx2.h, ptrs_in, case.ncells), "upload")
+    for _ in range(args.steps):
+        ctx2.step(1)
+    ptrs_out = api._field_ptrs(out_np)
+    api.check(api.lib().ecg_download_prim(ctx2.h, ptrs_out, case.ncells), "download")
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = case.ncells * args.steps * world / float(te.item())
+    state_bytes = 8 * case.ncells * nf
+    scal_bytes = 64
+    stat_bytes = 8 * 24
+    ctx2.close()
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        B = bytes_per_cell_update(case)
+        achieved = B * case.ncells / (step_ms * 1e-3) / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = reference_sample(steps=2, warmup=0, config=args.config)
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / args.steps + scal_bytes,
+                    "d2h_bytes_per_step": state_bytes / args.steps + scal_bytes + stat_bytes,
+                    "note": "state uploaded from pinned host memory once and downloaded once per timed run; "
+                            "one ecg_step call per step"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "one full step (predictor + corrector + dt update)",
+                         "bytes_per_cell_update": B},
+            "kernels_ms": {"pass1": pass_ms[0], "pass2": pass_ms[1], "update": pass_ms[2]},
+            "gpu_launches": args.steps * (3 if case.second_order else 2),
+            "clocks": clk.summary(),
+            "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max,
+                       "fallback": st.newton_fallback, "hist": list(st.newton_hist)},
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": "cell-updates/s", "cores": cpu["cores"],
+                                    "kind": "reference", "sample": cpu["sample"]}
+        print(json.dumps(line))
+    ctx.close()
+    shutil.rmtree(work, ignore_errors=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

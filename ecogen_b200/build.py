@@ -1,0 +1,97 @@
+"""Builds the CUDA library ``ecogen_b200/libecg.so`` (sm_100a) and the ``ecogen-b200`` driver.
+
+nvcc compiles every translation unit for ``-gencode arch=compute_100a,code=sm_100a`` with
+``--fmad=false`` (no multiply-add contraction, as in the reference's x86-64 build) and links them
+into one shared library with a plain C ABI (``include/ecogen_b200.h``).  Objects are rebuilt only
+when a source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libecg.so")
+DRIVER = os.path.join(HERE, "ecogen-b200")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+           "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
+
+
+def _nvcc() -> str:
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return p
+
+
+def _headers():
+    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h"))
+
+
+def _stale(obj: str, src: str) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(f) > t for f in [src] + _headers())
+
+
+def _compile(src: str, extra=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    if not _stale(obj, src):
+        return obj
+    if src.endswith(".cu"):
+        cmd = [_nvcc()] + ARCH + NVFLAGS + (extra or []) + ["-c", src, "-o", obj]
+    else:
+        cmd = ["g++"] + CXXFLAGS + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
+def build(verbose: bool = False, jobs: int = 8) -> str:
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    lib_srcs = [s for s in srcs if not os.path.basename(s).startswith("ecogen_main")]
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(_compile, lib_srcs))
+    if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+        cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    main_src = os.path.join(CSRC, "ecogen_main.cpp")
+    if os.path.exists(main_src):
+        mobj = _compile(main_src)
+        if not os.path.exists(DRIVER) or os.path.getmtime(mobj) > os.path.getmtime(DRIVER) or \
+                os.path.getmtime(LIB) > os.path.getmtime(DRIVER):
+            cmd = ["g++", "-o", DRIVER, mobj, "-L" + HERE, "-lecg", "-Wl,-rpath,$ORIGIN"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print("built", LIB)
+    return LIB
+
+
+def ptxas_report(src: str) -> str:
+    """Register / shared-memory / spill report of one .cu file (nvcc -Xptxas -v)."""
+    cmd = [_nvcc()] + ARCH + NVFLAGS + ["-Xptxas", "-v", "-c", src, "-o", os.devnull]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return r.stdout + r.stderr
+
+
+if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "ptxas":
+        print(ptxas_report(sys.argv[2]))
+    else:
+        build(verbose=True)

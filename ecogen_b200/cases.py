@@ -72,6 +72,7 @@ AIR_IG = Eos("IG_air.xml", "IG", gamma=1.4, cv=800.0)
 GAS_B_IG = Eos("IG_gasB.xml", "IG", gamma=1.67, cv=3116.0)
 LIQ_PC = Eos("SG_liquidPC.xml", "SG", gamma=2.35, pinf=1.0e9, cv=1816.0, eref=-1167.0e3, sref=0.0)
 VAP_PC = Eos("SG_vapourPC.xml", "SG", gamma=1.43, pinf=0.0, cv=1040.0, eref=2030.0e3, sref=-23.0e3)
+WATER_NASG = Eos("NASG_water.xml", "NASG", gamma=1.19, pinf=7.028e8, b=6.61e-4, cv=3610.0, eref=-1177788.0)
 
 
 # ----------------------------------------------------------------------------- case description
@@ -288,7 +289,8 @@ def write_ecogen_list(work: str, case_dirs: Sequence[str]) -> str:
 
 def shock_tube_1d(ncells: int = 1000, iterations: Optional[int] = None, total_time: Optional[float] = 240e-6,
                   order: Optional[str] = None, p_left: float = 1e9, x_interface: float = 0.7,
-                  alpha_floor: float = 1e-6, name: str = "shockTube1D") -> Case:
+                  alpha_floor: float = 1e-6, name: str = "shockTube1D", liquid: Eos = WATER_SG,
+                  alpha_null: bool = False) -> Case:
     """1D two-phase water/air shock tube on [0,1] m (Kapila, CFL 0.8, transmissive ends).
 
     Left of ``x_interface``: water-rich (alpha_water = 1-floor), p = ``p_left``;
@@ -303,7 +305,7 @@ def shock_tube_1d(ncells: int = 1000, iterations: Optional[int] = None, total_ti
                Domain("HP", "waterSide", "halfSpace", {"axis": "x", "origin": x_interface, "direction": "negative"})]
     if iterations is not None:
         total_time = None
-    return Case(name, [WATER_SG, AIR_IG], (1.0, 0.1, 0.1), (ncells, 1, 1), states, domains,
+    return Case(name, [liquid, AIR_IG], (1.0, 0.1, 0.1), (ncells, 1, 1), states, domains, alpha_null=alpha_null,
                 cfl=0.8, iterations=iterations, total_time=total_time, second_order=order)
 
 

@@ -1,0 +1,678 @@
+// C ABI: contexts, device state, the time loop and CUDA-graph capture of step sequences.
+//
+// A context owns, on one GPU, two copies of the state S (ping-pong: a step reads S^n and writes
+// S^{n+1}), the MUSCL half-step state, the mesh distance tables, device scalars (dt, t, dtMax,
+// stop flag) and counters, and one stream.  Every step is a fixed launch sequence
+//   first order : step(O1) -> finalize
+//   MUSCL       : step(PRED) -> step(CORR) -> finalize
+// whose only data-dependent quantity (dt) lives in device memory, so sequences of steps are
+// captured once as CUDA graphs and replayed without host round trips.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ecg_internal.h"
+#include "ecg_mlp_device.cuh"
+#include "ecg_step.cuh"
+
+namespace ecg {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+cudaError_t kapila_launch(int np, int dim, bool ptmu, int pass, const StepParams& P, const Geometry& G,
+                          const ecg_eos* eos, double eps, cudaStream_t s, bool prepare);
+cudaError_t euler_launch(int dim, int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
+                         cudaStream_t s, bool prepare);
+
+__global__ void k_finalize(DevScalars* s) {
+  // Run::solver src/Run.cpp:417-440: t += dt, iteration++, stop test, dt = cfl * dtMax
+  if (s->done) return;
+  double dtmax = __longlong_as_double((long long)s->dtmax_bits);
+  s->t += s->dt;
+  s->it += 1;
+  if (s->mode == 1 && s->it >= s->max_it) s->done = 1;
+  if (s->mode == 2 && s->t >= s->t_end) s->done = 1;
+  s->dt = s->cfl * dtmax;
+  s->dtmax_bits = (unsigned long long)__double_as_longlong(1.e10);
+}
+
+// Mixture pressure sum_k alpha_k p_k of the stored state (what the reference writes as
+// Pressure_Mixture after fulfillState), optionally per-phase temperature and mass fraction.
+__global__ void k_derived(const double* __restrict__ S, int64_t n, int np, int dim, ecg_eos e0, ecg_eos e1, ecg_eos e2,
+                          double eps, double* pmix, double* T, double* Y) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const ecg_eos eos[3] = {e0, e1, e2};
+  double p = S[(int64_t)(2 * np) * n + i];
+  double a[ECG_MAX_PHASES], r[ECG_MAX_PHASES], pk[ECG_MAX_PHASES];
+  double rho = 0., pm = 0.;
+  for (int k = 0; k < np; k++) {
+    a[k] = S[(int64_t)k * n + i];
+    r[k] = S[(int64_t)(np + k) * n + i];
+    EosParams q{eos[k].type, eos[k].gamma, eos[k].pinf, eos[k].b, eos[k].cv, eos[k].eref, eos[k].sref};
+    pk[k] = eos_fix_p(q, p);
+    rho += a[k] * r[k];
+    pm += a[k] * pk[k];
+  }
+  if (pmix) pmix[i] = pm;
+  for (int k = 0; k < np; k++) {
+    EosParams q{eos[k].type, eos[k].gamma, eos[k].pinf, eos[k].b, eos[k].cv, eos[k].eref, eos[k].sref};
+    if (T) T[(int64_t)k * n + i] = eos_T(q, eps, r[k], pk[k]);
+    if (Y) Y[(int64_t)k * n + i] = a[k] * r[k] / dmax(rho, eps);
+  }
+}
+
+__global__ void k_euler_derived(const double* __restrict__ S, int64_t n, ecg_eos e0, double eps, double* T) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  EosParams q{e0.type, e0.gamma, e0.pinf, e0.b, e0.cv, e0.eref, e0.sref};
+  T[i] = eos_T(q, eps, S[i], S[n + i]);
+}
+
+}  // namespace ecg
+
+using namespace ecg;
+
+struct ecg_ctx {
+  ecg_case c;
+  int dim = 1, np = 2, nstate = 0, nq = 0;
+  int64_t n = 0;
+  double eps = 0.;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double* state[2] = {nullptr, nullptr};
+  double* half = nullptr;     // MUSCL half-step primitives
+  double* dist = nullptr;     // distance tables (3 axes x 3 tables)
+  double* tmp = nullptr;      // download scratch (mixture pressure)
+  DevScalars* scal = nullptr;
+  DevStats* stats = nullptr;
+  int cur = 0;
+  int newton_cap = 100;
+  float* mlp = nullptr;
+  int mlp_nin = 0;
+  float* rec_x = nullptr;
+  float* rec_y = nullptr;
+  unsigned long long* rec_count = nullptr;
+  unsigned long long rec_max = 0;
+  double pcrit = 0.;
+  Geometry geo{};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step sequences starting from state[0] / state[1]
+  bool graph_dirty = true;
+};
+
+namespace {
+
+ecg_status cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return ECG_ERR_CUDA;
+}
+#define ECG_CUDA(call)                                    \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+ecg_status validate_case(const ecg_case* c) {
+  if (!c) { set_error("null case"); return ECG_ERR_INVALID; }
+  if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER) { set_error("unknown model"); return ECG_ERR_INVALID; }
+  if (c->model == ECG_MODEL_KAPILA && (c->nphases < 2 || c->nphases > 3)) { set_error("Kapila needs 2 or 3 phases"); return ECG_ERR_UNSUPPORTED; }
+  if (c->model == ECG_MODEL_EULER && c->nphases != 1) { set_error("Euler has one phase"); return ECG_ERR_INVALID; }
+  if (c->order != 1 && c->order != 2) { set_error("order must be 1 or 2"); return ECG_ERR_INVALID; }
+  for (int i = 0; i < 3; i++)
+    if (c->ncells[i] < 1 || !(c->length[i] > 0.)) { set_error("bad mesh"); return ECG_ERR_INVALID; }
+  if (c->ncells[0] <= 1) { set_error("Number of cells in the x-direction has to be superior to 1"); return ECG_ERR_INVALID; }
+  if (c->ncells[2] > 1 && c->ncells[1] <= 1) { set_error("z cells without y cells"); return ECG_ERR_INVALID; }
+  for (int i = 0; i < 4; i++)
+    if (c->limiter[i] < 0 || c->limiter[i] > ECG_LIM_THINC) { set_error("bad limiter"); return ECG_ERR_INVALID; }
+  if (c->order == 2 && (c->limiter[2] == ECG_LIM_THINC || c->limiter[3] == ECG_LIM_THINC)) {
+    set_error("THINC volume-fraction reconstruction is not supported");
+    return ECG_ERR_UNSUPPORTED;
+  }
+  if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
+  int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
+  if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
+  int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
+  if (n > (int64_t)1 << 31) { set_error("more than 2^31 cells"); return ECG_ERR_TOO_LARGE; }
+  return ECG_OK;
+}
+
+// Distances of the MUSCL reconstruction per axis, with the reference's arithmetic: cell centres
+// (i + 0.5) * d, face position centre + 0.5 * d, lengths as Coord::norm of a difference
+// (src/Meshes/Element.cpp:77-113, src/Maths/Coord.cpp:82).
+void distance_tables(const ecg_case& c, std::vector<double>& h) {
+  h.assign(9 * (size_t)std::max({c.ncells[0], c.ncells[1], c.ncells[2]}), 0.);
+  int nmax = std::max({c.ncells[0], c.ncells[1], c.ncells[2]});
+  for (int a = 0; a < 3; a++) {
+    double d = c.length[a] / (double)c.ncells[a];
+    for (int i = 0; i + 1 < c.ncells[a]; i++) {
+      double pl = (i + 0.5) * d, pr = (i + 1 + 0.5) * d, pf = pl + 0.5 * d;
+      double x = pl - pr, y = pf - pl, z = pf - pr;
+      h[(size_t)(3 * a + 0) * nmax + i] = std::sqrt(x * x + 0. * 0. + 0. * 0.);
+      h[(size_t)(3 * a + 1) * nmax + i] = std::sqrt(y * y + 0. * 0. + 0. * 0.);
+      h[(size_t)(3 * a + 2) * nmax + i] = std::sqrt(z * z + 0. * 0. + 0. * 0.);
+    }
+  }
+}
+
+ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
+  StepParams P{};
+  P.done = &x->scal->done;
+  P.n = x->n;
+  P.dt = &x->scal->dt;
+  P.dtmax_bits = &x->scal->dtmax_bits;
+  P.stats = x->stats;
+  for (int i = 0; i < 4; i++) P.lim[i] = x->c.limiter[i];
+  P.newton_cap = x->newton_cap;
+  P.mlp = x->mlp;
+  P.mlp_nin = x->mlp_nin;
+  P.rec_x = x->rec_x;
+  P.rec_y = x->rec_y;
+  P.rec_count = x->rec_count;
+  P.rec_max = x->rec_max;
+  P.ptmu = x->c.ptmu;
+  P.ptmu_liq = x->c.ptmu_liquid;
+  P.ptmu_vap = x->c.ptmu_vapor;
+  P.pcrit = x->pcrit;
+  double* sn = x->state[parity];
+  double* s1 = x->state[1 - parity];
+  const bool euler = x->c.model == ECG_MODEL_EULER;
+  auto run = [&](int pass) -> cudaError_t {
+    if (euler) return euler_launch(x->dim, pass, P, x->geo, x->c.eos, x->eps, x->stream, false);
+    return kapila_launch(x->np, x->dim, x->c.ptmu != 0, pass, P, x->geo, x->c.eos, x->eps, x->stream, false);
+  };
+  cudaError_t e;
+  if (ev) cudaEventRecord(ev[0], x->stream);
+  if (x->c.order == 1) {
+    P.q = sn;
+    P.sn = sn;
+    P.out = s1;
+    e = run(PASS_O1);
+    if (e != cudaSuccess) return cuda_fail(e, "step kernel");
+    if (ev) cudaEventRecord(ev[1], x->stream);
+  } else {
+    P.q = sn;
+    P.sn = sn;
+    P.out = x->half;
+    e = run(PASS_PRED);
+    if (e != cudaSuccess) return cuda_fail(e, "predictor kernel");
+    if (ev) cudaEventRecord(ev[1], x->stream);
+    P.q = x->half;
+    P.out = s1;
+    e = run(PASS_CORR);
+    if (e != cudaSuccess) return cuda_fail(e, "corrector kernel");
+  }
+  if (ev) cudaEventRecord(ev[2], x->stream);
+  k_finalize<<<1, 1, 0, x->stream>>>(x->scal);
+  if (ev) cudaEventRecord(ev[3], x->stream);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "finalize kernel");
+  return ECG_OK;
+}
+
+void drop_graphs(ecg_ctx* x) {
+  for (int i = 0; i < 2; i++)
+    if (x->graph[i]) {
+      cudaGraphExecDestroy(x->graph[i]);
+      x->graph[i] = nullptr;
+    }
+  x->graph_dirty = false;
+}
+
+// Captures two consecutive steps starting from state[parity] (the pair returns to state[parity]).
+ecg_status build_graph(ecg_ctx* x, int parity) {
+  cudaGraph_t g = nullptr;
+  ECG_CUDA(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+  ecg_status s1 = launch_step(x, parity);
+  ecg_status s2 = (s1 == ECG_OK) ? launch_step(x, 1 - parity) : s1;
+  cudaError_t e = cudaStreamEndCapture(x->stream, &g);
+  if (s2 != ECG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s2;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&x->graph[parity], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return ECG_OK;
+}
+
+ecg_status advance(ecg_ctx* x, int nsteps) {
+  if (x->graph_dirty) drop_graphs(x);
+  while (nsteps >= 2) {
+    if (!x->graph[x->cur]) {
+      ecg_status s = build_graph(x, x->cur);
+      if (s != ECG_OK) return s;
+    }
+    ECG_CUDA(cudaGraphLaunch(x->graph[x->cur], x->stream));
+    nsteps -= 2;
+  }
+  if (nsteps == 1) {
+    ecg_status s = launch_step(x, x->cur);
+    if (s != ECG_OK) return s;
+    x->cur = 1 - x->cur;
+  }
+  return ECG_OK;
+}
+
+void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
+  std::memset(st, 0, sizeof(*st));
+  st->cell_updates = updates;
+  st->relax_calls = (int64_t)d.relax_calls;
+  st->newton_evals = (int64_t)d.newton_evals;
+  st->newton_fallback = (int64_t)d.newton_fallback;
+  st->newton_max = (int64_t)d.newton_max;
+  st->seeded = (int64_t)d.seeded;
+  st->seed_rejected = (int64_t)d.seed_rejected;
+  st->ptmu_errors = (int64_t)d.ptmu_errors;
+  st->nonfinite_cells = (int64_t)d.nonfinite;
+  for (int i = 0; i < 16; i++) st->newton_hist[i] = (int64_t)d.hist[i];
+}
+
+}  // namespace
+
+extern "C" const char* ecg_status_str(ecg_status s) {
+  switch (s) {
+    case ECG_OK: return "ok";
+    case ECG_ERR_INVALID: return "invalid argument";
+    case ECG_ERR_UNSUPPORTED: return "unsupported case";
+    case ECG_ERR_CUDA: return "CUDA error";
+    case ECG_ERR_XML: return "case input error";
+    case ECG_ERR_PHYSICS: return "physics check failed";
+    case ECG_ERR_NOMEM: return "out of memory";
+    case ECG_ERR_TOO_LARGE: return "size above the stated maximum";
+    case ECG_ERR_TIMEOUT: return "device wait timed out";
+  }
+  return "unknown status";
+}
+
+extern "C" const char* ecg_last_error(void) { return g_last_error.c_str(); }
+extern "C" int ecg_version(void) { return 10000; }
+
+extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
+  if (!out) { set_error("null out"); return ECG_ERR_INVALID; }
+  *out = nullptr;
+  ecg_status vs = validate_case(c);
+  if (vs != ECG_OK) return vs;
+  auto x = new ecg_ctx();
+  x->c = *c;
+  x->dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
+  x->np = c->nphases;
+  x->n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
+  x->eps = c->alpha_null ? 1.e-15 : 0.;
+  const bool euler = c->model == ECG_MODEL_EULER;
+  x->nstate = euler ? (3 + x->dim) : (2 * x->np + 2 + x->dim);  // Euler: rho, p, u, E
+  x->nq = x->nstate - 1;
+  auto fail_free = [&](ecg_status s) {
+    ecg_destroy(x);
+    return s;
+  };
+  cudaError_t e = cudaGetDevice(&x->device);
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaGetDevice"));
+  e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaStreamCreate"));
+  size_t sbytes = sizeof(double) * (size_t)x->nstate * (size_t)x->n;
+  for (int i = 0; i < 2; i++) {
+    e = cudaMalloc(&x->state[i], sbytes);
+    if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(state)"));
+    cudaMemsetAsync(x->state[i], 0, sbytes, x->stream);
+  }
+  if (c->order == 2) {
+    e = cudaMalloc(&x->half, sizeof(double) * (size_t)x->nq * (size_t)x->n);
+    if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(half)"));
+  }
+  e = cudaMalloc(&x->tmp, sizeof(double) * (size_t)x->n);
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(tmp)"));
+  std::vector<double> h;
+  distance_tables(*c, h);
+  e = cudaMalloc(&x->dist, sizeof(double) * h.size());
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(dist)"));
+  cudaMemcpy(x->dist, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice);
+  int nmax = std::max({c->ncells[0], c->ncells[1], c->ncells[2]});
+  for (int a = 0; a < 3; a++) {
+    x->geo.n[a] = c->ncells[a];
+    x->geo.dcc[a] = x->dist + (size_t)(3 * a + 0) * nmax;
+    x->geo.dfl[a] = x->dist + (size_t)(3 * a + 1) * nmax;
+    x->geo.dfr[a] = x->dist + (size_t)(3 * a + 2) * nmax;
+  }
+  x->geo.dim = x->dim;
+  // MeshCartesian::initializeGeometrieMonoCpu :228-236 and face surfaces :287, :320, :353
+  double dX = c->length[0] / (double)c->ncells[0], dY = c->length[1] / (double)c->ncells[1],
+         dZ = c->length[2] / (double)c->ncells[2];
+  double vol = dX * dY * dZ;
+  x->geo.coefA[0] = (dY * dZ) / vol;
+  x->geo.coefA[1] = (dX * dZ) / vol;
+  x->geo.coefA[2] = (dX * dY) / vol;
+  double l = 1.e10;
+  if (c->ncells[0] != 1) l = std::min(l, dX);
+  if (c->ncells[1] != 1) l = std::min(l, dY);
+  if (c->ncells[2] != 1) l = std::min(l, dZ);
+  if (x->dim > 1) l *= 0.6;
+  x->geo.lcfl = l;
+  if (c->ptmu) {  // Mixture::computeCriticalPressure src/Models/Mixture.cpp:146
+    const ecg_eos& L = c->eos[c->ptmu_liquid];
+    const ecg_eos& V = c->eos[c->ptmu_vapor];
+    double piL = L.type == ECG_EOS_IG ? 0. : L.pinf, piV = V.type == ECG_EOS_IG ? 0. : V.pinf;
+    double pc = piL * (V.gamma - 1.) * V.cv - piV * (L.gamma - 1.) * L.cv;
+    pc /= (L.gamma - 1.) * L.cv - (V.gamma - 1.) * V.cv;
+    x->pcrit = pc;
+  }
+  e = cudaMalloc(&x->scal, sizeof(DevScalars));
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(scalars)"));
+  e = cudaMalloc(&x->stats, sizeof(DevStats));
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(stats)"));
+  DevScalars s0{};
+  s0.dt = 1.e-15;
+  s0.cfl = c->cfl;
+  s0.dtmax_bits = (unsigned long long)0;
+  double big = 1.e10;
+  std::memcpy(&s0.dtmax_bits, &big, sizeof(double));
+  cudaMemcpy(x->scal, &s0, sizeof(s0), cudaMemcpyHostToDevice);
+  cudaMemset(x->stats, 0, sizeof(DevStats));
+  // kernel attributes (dynamic shared memory) for every pass of this case shape
+  for (int pass = 0; pass < 3; pass++) {
+    StepParams P{};
+    cudaError_t pe = euler ? euler_launch(x->dim, pass, P, x->geo, c->eos, x->eps, x->stream, true)
+                           : kapila_launch(x->np, x->dim, c->ptmu != 0, pass, P, x->geo, c->eos, x->eps, x->stream, true);
+    if (pe == cudaErrorNotSupported) {
+      set_error("no kernel built for this model / phases / dimension");
+      ecg_destroy(x);
+      return ECG_ERR_UNSUPPORTED;
+    }
+    if (pe != cudaSuccess) return fail_free(cuda_fail(pe, "cudaFuncSetAttribute"));
+  }
+  e = cudaStreamSynchronize(x->stream);
+  if (e != cudaSuccess) return fail_free(cuda_fail(e, "create"));
+  *out = x;
+  return ECG_OK;
+}
+
+extern "C" void ecg_destroy(ecg_ctx* x) {
+  if (!x) return;
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  drop_graphs(x);
+  cudaFree(x->state[0]);
+  cudaFree(x->state[1]);
+  cudaFree(x->half);
+  cudaFree(x->dist);
+  cudaFree(x->tmp);
+  cudaFree(x->scal);
+  cudaFree(x->stats);
+  cudaFree(x->mlp);
+  cudaFree(x->rec_x);
+  cudaFree(x->rec_y);
+  cudaFree(x->rec_count);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+extern "C" int64_t ecg_ncells(const ecg_ctx* x) { return x ? x->n : 0; }
+extern "C" void* ecg_stream(const ecg_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+extern "C" ecg_status ecg_set_newton_cap(ecg_ctx* x, int32_t cap) {
+  if (!x || cap < 1 || cap > 100000) { set_error("bad Newton cap"); return ECG_ERR_INVALID; }
+  x->newton_cap = cap;
+  x->graph_dirty = true;
+  return ECG_OK;
+}
+
+static ecg_status upload_impl(ecg_ctx* x, const double* const* f, int64_t ncells, cudaMemcpyKind kind) {
+  if (!x || !f) { set_error("null argument"); return ECG_ERR_INVALID; }
+  if (ncells != x->n) { set_error("ncells does not match the context"); return ECG_ERR_INVALID; }
+  const int nf = abi_nfields(x->c);
+  for (int i = 0; i < nf; i++)
+    if (!f[i]) { set_error("null field pointer"); return ECG_ERR_INVALID; }
+  const int64_t n = x->n;
+  const size_t fb = sizeof(double) * (size_t)n;
+  double* S = x->state[x->cur];
+  const bool euler = x->c.model == ECG_MODEL_EULER;
+  // ABI: [alpha_k, rho_k] p u_x u_y u_z E  -> device: [alpha_k, rho_k] p u_0..u_{dim-1} E
+  const int pre = euler ? 2 : 2 * x->np + 1;  // fields up to and including p
+  for (int i = 0; i < pre; i++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)i * n, f[i], fb, kind, x->stream));
+  for (int d = 0; d < x->dim; d++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)(pre + d) * n, f[pre + d], fb, kind, x->stream));
+  ECG_CUDA(cudaMemcpyAsync(S + (size_t)(pre + x->dim) * n, f[pre + 3], fb, kind, x->stream));
+  if (kind == cudaMemcpyHostToDevice) {
+    // transverse velocity components of a lower-dimensional case must be zero (they are not stored)
+    for (int d = x->dim; d < 3; d++)
+      for (int64_t i = 0; i < n; i++)
+        if (f[pre + d][i] != 0.) {
+          set_error("non-zero velocity component along an axis with one cell is not supported");
+          return ECG_ERR_UNSUPPORTED;
+        }
+  }
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_upload_prim(ecg_ctx* x, const double* const* f, int64_t ncells) {
+  ecg_status s = upload_impl(x, f, ncells, cudaMemcpyHostToDevice);
+  if (s != ECG_OK) return s;
+  ECG_CUDA(cudaStreamSynchronize(x->stream));
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_upload_prim_device(ecg_ctx* x, const double* const* f, int64_t ncells) {
+  return upload_impl(x, f, ncells, cudaMemcpyDeviceToDevice);
+}
+
+static ecg_status download_impl(ecg_ctx* x, double* const* f, int64_t ncells, cudaMemcpyKind kind) {
+  if (!x || !f) { set_error("null argument"); return ECG_ERR_INVALID; }
+  if (ncells != x->n) { set_error("ncells does not match the context"); return ECG_ERR_INVALID; }
+  const int nf = abi_nfields(x->c);
+  for (int i = 0; i < nf; i++)
+    if (!f[i]) { set_error("null field pointer"); return ECG_ERR_INVALID; }
+  const int64_t n = x->n;
+  const size_t fb = sizeof(double) * (size_t)n;
+  const double* S = x->state[x->cur];
+  const bool euler = x->c.model == ECG_MODEL_EULER;
+  if (euler) {
+    for (int i = 0; i < 2; i++) ECG_CUDA(cudaMemcpyAsync(f[i], S + (size_t)i * n, fb, kind, x->stream));
+  } else {
+    k_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, x->np, x->dim, x->c.eos[0], x->c.eos[1],
+                                                                 x->c.eos[2], x->eps, x->tmp, nullptr, nullptr);
+    ECG_CUDA(cudaGetLastError());
+    for (int i = 0; i < 2 * x->np; i++) ECG_CUDA(cudaMemcpyAsync(f[i], S + (size_t)i * n, fb, kind, x->stream));
+    ECG_CUDA(cudaMemcpyAsync(f[2 * x->np], x->tmp, fb, kind, x->stream));
+  }
+  const int pre = euler ? 2 : 2 * x->np + 1;
+  for (int d = 0; d < 3; d++) {
+    if (d < x->dim) ECG_CUDA(cudaMemcpyAsync(f[pre + d], S + (size_t)(pre + d) * n, fb, kind, x->stream));
+    else if (kind == cudaMemcpyDeviceToHost) {
+      ECG_CUDA(cudaStreamSynchronize(x->stream));
+      std::memset(f[pre + d], 0, fb);
+    } else ECG_CUDA(cudaMemsetAsync(f[pre + d], 0, fb, x->stream));
+  }
+  ECG_CUDA(cudaMemcpyAsync(f[pre + 3], S + (size_t)(pre + x->dim) * n, fb, kind, x->stream));
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_download_prim(ecg_ctx* x, double* const* f, int64_t ncells) {
+  ecg_status s = download_impl(x, f, ncells, cudaMemcpyDeviceToHost);
+  if (s != ECG_OK) return s;
+  ECG_CUDA(cudaStreamSynchronize(x->stream));
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_download_prim_device(ecg_ctx* x, double* const* f, int64_t ncells) {
+  return download_impl(x, f, ncells, cudaMemcpyDeviceToDevice);
+}
+
+extern "C" ecg_status ecg_download_derived(ecg_ctx* x, double* T, double* Y, int64_t ncells) {
+  if (!x || !T || !Y) { set_error("null argument"); return ECG_ERR_INVALID; }
+  if (ncells != x->n) { set_error("ncells does not match the context"); return ECG_ERR_INVALID; }
+  const int64_t n = x->n;
+  const int np = x->np;
+  double *dT = nullptr, *dY = nullptr;
+  ECG_CUDA(cudaMalloc(&dT, sizeof(double) * (size_t)np * n));
+  cudaError_t e = cudaMalloc(&dY, sizeof(double) * (size_t)np * n);
+  if (e != cudaSuccess) {
+    cudaFree(dT);
+    return cuda_fail(e, "cudaMalloc");
+  }
+  const double* S = x->state[x->cur];
+  if (x->c.model == ECG_MODEL_EULER) {
+    k_euler_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, x->c.eos[0], x->eps, dT);
+    cudaMemsetAsync(dY, 0, sizeof(double) * n, x->stream);
+  } else {
+    k_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, np, x->dim, x->c.eos[0], x->c.eos[1],
+                                                                 x->c.eos[2], x->eps, nullptr, dT, dY);
+  }
+  cudaMemcpyAsync(T, dT, sizeof(double) * (size_t)np * n, cudaMemcpyDeviceToHost, x->stream);
+  cudaMemcpyAsync(Y, dY, sizeof(double) * (size_t)np * n, cudaMemcpyDeviceToHost, x->stream);
+  e = cudaStreamSynchronize(x->stream);
+  cudaFree(dT);
+  cudaFree(dY);
+  if (e != cudaSuccess) return cuda_fail(e, "download_derived");
+  if (x->c.model == ECG_MODEL_EULER)
+    for (int64_t i = 0; i < n; i++) Y[i] = 1.;
+  return ECG_OK;
+}
+
+static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, double* t, int32_t* iterations,
+                              ecg_step_stats* stats, double* kernel_ms = nullptr) {
+  // host values of dt and t seed the device scalars (the caller owns the time loop state)
+  DevScalars h{};
+  h.dt = *dt;
+  h.t = *t;
+  h.cfl = x->c.cfl;
+  h.t_end = x->c.total_time;
+  double big = 1.e10;
+  std::memcpy(&h.dtmax_bits, &big, sizeof(double));
+  h.it = iterations ? *iterations : 0;
+  h.max_it = x->c.max_iterations;
+  h.mode = mode;
+  h.done = (mode == 1 && h.it >= h.max_it) || (mode == 2 && h.t >= h.t_end);
+  ECG_CUDA(cudaMemcpyAsync(x->scal, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+  ECG_CUDA(cudaMemsetAsync(x->stats, 0, sizeof(DevStats), x->stream));
+  int64_t done_steps = 0;
+  if (kernel_ms) {
+    cudaEvent_t ev[4];
+    for (int i = 0; i < 4; i++) ECG_CUDA(cudaEventCreate(&ev[i]));
+    for (int i = 0; i < nsteps; i++) {
+      ecg_status s = launch_step(x, x->cur, ev);
+      if (s != ECG_OK) return s;
+      x->cur = 1 - x->cur;
+      ECG_CUDA(cudaEventSynchronize(ev[3]));
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[1], ev[2]);
+      cudaEventElapsedTime(&c, ev[2], ev[3]);
+      kernel_ms[0] += a;
+      kernel_ms[1] += b;
+      kernel_ms[2] += c;
+    }
+    for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+  } else if (mode == 0) {
+    ecg_status s = advance(x, nsteps);
+    if (s != ECG_OK) return s;
+  } else {
+    // chunks of captured steps; steps after the stop condition are no-ops on the device
+    const int chunk = 64;
+    for (;;) {
+      ecg_status s = advance(x, chunk);
+      if (s != ECG_OK) return s;
+      DevScalars r{};
+      ECG_CUDA(cudaMemcpyAsync(&r, x->scal, sizeof(r), cudaMemcpyDeviceToHost, x->stream));
+      ECG_CUDA(cudaStreamSynchronize(x->stream));
+      if (r.done) break;
+    }
+  }
+  DevScalars r{};
+  DevStats ds{};
+  ECG_CUDA(cudaMemcpyAsync(&r, x->scal, sizeof(r), cudaMemcpyDeviceToHost, x->stream));
+  ECG_CUDA(cudaMemcpyAsync(&ds, x->stats, sizeof(ds), cudaMemcpyDeviceToHost, x->stream));
+  ECG_CUDA(cudaStreamSynchronize(x->stream));
+  done_steps = r.it - h.it;
+  *dt = r.dt;
+  *t = r.t;
+  if (iterations) *iterations = (int32_t)r.it;
+  if (stats) stats_out(ds, done_steps * x->n, stats);
+  if (ds.ptmu_errors) {
+    set_error("p-T-mu relaxation exceeded 50 iterations");
+    return ECG_ERR_PHYSICS;
+  }
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_step(ecg_ctx* x, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats) {
+  if (!x || !dt || !t || nsteps < 0) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  return step_common(x, 0, nsteps, dt, t, nullptr, stats);
+}
+
+extern "C" ecg_status ecg_step_profiled(ecg_ctx* x, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats,
+                                        double* kernel_ms) {
+  if (!x || !dt || !t || nsteps < 0 || !kernel_ms) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  return step_common(x, 0, nsteps, dt, t, nullptr, stats, kernel_ms);
+}
+
+extern "C" ecg_status ecg_run(ecg_ctx* x, double* dt, double* t, int32_t* iterations, ecg_step_stats* stats) {
+  if (!x || !dt || !t || !iterations) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  return step_common(x, x->c.time_iterations ? 1 : 2, 0, dt, t, iterations, stats);
+}
+
+extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
+  if (!x) { set_error("null context"); return ECG_ERR_INVALID; }
+  x->graph_dirty = true;
+  if (!m) {
+    cudaFree(x->mlp);
+    x->mlp = nullptr;
+    return ECG_OK;
+  }
+  if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
+  if (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * x->np) { set_error("seed model shape must be 3*nphases -> 64 -> 64 -> 1"); return ECG_ERR_INVALID; }
+  const int nin = m->n_in, H = ECG_MLP_HIDDEN;
+  std::vector<float> pk((size_t)mlp_packed_size(nin));
+  float* q = pk.data();
+  std::memcpy(q, m->w1, sizeof(float) * H * nin); q += H * nin;
+  std::memcpy(q, m->b1, sizeof(float) * H); q += H;
+  std::memcpy(q, m->w2, sizeof(float) * H * H); q += H * H;
+  std::memcpy(q, m->b2, sizeof(float) * H); q += H;
+  std::memcpy(q, m->w3, sizeof(float) * H); q += H;
+  *q++ = m->b3;
+  for (int i = 0; i < nin; i++) *q++ = m->in_shift[i];
+  for (int i = 0; i < nin; i++) *q++ = m->in_scale[i];
+  *q++ = m->out_shift;
+  *q++ = m->out_scale;
+  if (!x->mlp) ECG_CUDA(cudaMalloc(&x->mlp, sizeof(float) * pk.size()));
+  ECG_CUDA(cudaMemcpyAsync(x->mlp, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice, x->stream));
+  ECG_CUDA(cudaStreamSynchronize(x->stream));
+  x->mlp_nin = nin;
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs) {
+  if (!x || max_pairs < 0) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  x->graph_dirty = true;
+  cudaFree(x->rec_x);
+  cudaFree(x->rec_y);
+  cudaFree(x->rec_count);
+  x->rec_x = x->rec_y = nullptr;
+  x->rec_count = nullptr;
+  x->rec_max = 0;
+  if (max_pairs == 0) return ECG_OK;
+  const int nin = 3 * x->np;
+  ECG_CUDA(cudaMalloc(&x->rec_x, sizeof(float) * nin * (size_t)max_pairs));
+  ECG_CUDA(cudaMalloc(&x->rec_y, sizeof(float) * (size_t)max_pairs));
+  ECG_CUDA(cudaMalloc(&x->rec_count, sizeof(unsigned long long)));
+  ECG_CUDA(cudaMemset(x->rec_count, 0, sizeof(unsigned long long)));
+  x->rec_max = (unsigned long long)max_pairs;
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_fetch_pairs(ecg_ctx* x, float* features, float* targets, int64_t* count) {
+  if (!x || !count) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  if (!x->rec_count) { *count = 0; return ECG_OK; }
+  unsigned long long c = 0;
+  ECG_CUDA(cudaMemcpyAsync(&c, x->rec_count, sizeof(c), cudaMemcpyDeviceToHost, x->stream));
+  ECG_CUDA(cudaStreamSynchronize(x->stream));
+  if (c > x->rec_max) c = x->rec_max;
+  *count = (int64_t)c;
+  const int nin = 3 * x->np;
+  if (features && c) ECG_CUDA(cudaMemcpy(features, x->rec_x, sizeof(float) * nin * c, cudaMemcpyDeviceToHost));
+  if (targets && c) ECG_CUDA(cudaMemcpy(targets, x->rec_y, sizeof(float) * c, cudaMemcpyDeviceToHost));
+  return ECG_OK;
+}

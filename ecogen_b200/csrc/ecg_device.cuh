@@ -1,0 +1,543 @@
+// Device-side physics of the ECOGEN Cartesian FV step, in FP64.
+//
+// Every routine restates a reference routine (file:line relative to the ECOGEN
+// tree) with the same operation order, so that results agree with the CPU code
+// to the last bits except where CUDA's pow/log/exp differ from glibc's by an ulp.
+// Kernels are built with --fmad=false so that no multiply-add is contracted, as
+// in the reference's x86-64 SSE2 build.
+//
+// Compact state.  The reference keeps per phase (alpha, rho, p, T, e, c, Y) and per
+// cell a mixture record (rho, p, u, e, E, cF, cWood).  After each full step every
+// phase pressure equals the mixture-EOS pressure p clamped by that phase's EOS floor
+// (FluxPUEq::correctionEnergy src/Models/PUEq/FluxPUEq.cpp:68-112 sets p_k = p then
+// PhaseUEq::verifyAndCorrectPhase clamps it), and T, e, c, Y and the mixture record
+// are pure functions of (alpha_k, rho_k, p_k, u).  So the state that defines a step is
+// (alpha_k, rho_k)_k, p, u (DIM components) and E, and everything else is recomputed.
+#pragma once
+#include <cstdint>
+
+#include "ecg_types.h"
+
+namespace ecg {
+
+// std::max / std::min with libstdc++'s argument order (NaN behaviour included)
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+
+// ----------------------------------------------------------------------------------------- EOS
+// src/Eos/EosIG.cpp:64-257, src/Eos/EosSG.cpp:66-257, src/Eos/EosNASG.cpp:68-280
+
+__device__ __forceinline__ double eos_T(const EosParams& q, double eps, double rho, double p) {
+  if (q.type == ECG_EOS_IG) return p / (q.gamma - 1.) / dmax(rho, eps) / q.cv;
+  if (q.type == ECG_EOS_SG) return (p + q.pinf) / (q.gamma - 1.) / dmax(rho, eps) / q.cv;
+  return (p + q.pinf) * dmax(1. - rho * q.b, eps) / (q.gamma - 1.) / q.cv / dmax(rho, eps);
+}
+
+__device__ __forceinline__ double eos_e(const EosParams& q, double eps, double rho, double p) {
+  if (q.type == ECG_EOS_IG) return p / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
+  if (q.type == ECG_EOS_SG) return (p + q.gamma * q.pinf) / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
+  return (p + q.gamma * q.pinf) * dmax(1. - rho * q.b, eps) / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
+}
+
+__device__ __forceinline__ double eos_p(const EosParams& q, double eps, double rho, double e) {
+  if (q.type == ECG_EOS_IG) return (q.gamma - 1.) * rho * (e - q.eref);
+  if (q.type == ECG_EOS_SG) return (q.gamma - 1.) * rho * (e - q.eref) - q.gamma * q.pinf;
+  return (rho * (q.gamma - 1.) * (e - q.eref) / dmax(1. - rho * q.b, eps) - q.gamma * q.pinf);
+}
+
+__device__ __forceinline__ double eos_c(const EosParams& q, double eps, double rho, double p) {
+  if (q.type == ECG_EOS_IG) return sqrt(q.gamma * p / dmax(rho, eps));
+  if (q.type == ECG_EOS_SG) return sqrt(q.gamma * (p + q.pinf) / dmax(rho, eps));
+  return sqrt(q.gamma * (p + q.pinf) / dmax(rho * (1. - rho * q.b), eps));
+}
+
+__device__ __forceinline__ double nonzero(double a, double eps) {  // Tools::returnNonZeroValue src/Tools.cpp:134
+  if (a > eps || a < -eps) return a;
+  int sg = (0. < a) - (a < 0.);
+  return sg * eps;
+}
+
+__device__ __forceinline__ double eos_p_isentropic(const EosParams& q, double eps, double p0, double rho0,
+                                                   double rho1) {
+  if (q.type == ECG_EOS_IG) return p0 * pow(rho1 / dmax(rho0, eps), q.gamma);
+  if (q.type == ECG_EOS_SG) return (p0 + q.pinf) * pow(rho1 / dmax(rho0, eps), q.gamma) - q.pinf;
+  return (p0 + q.pinf) * pow(rho1 / dmax(rho0, eps), q.gamma) * pow((1. - rho0 * q.b) / (1. - rho1 * q.b), q.gamma) -
+         q.pinf;
+}
+
+__device__ __forceinline__ double eos_rho_pfinal(const EosParams& q, double eps, double p0, double rho0, double p1,
+                                                 double* drhodp) {
+  double num, denom, rho1;
+  if (q.type == ECG_EOS_IG) {
+    num = q.gamma * p1;
+    denom = num + p0 - p1;
+    rho1 = rho0 * num / dmax(denom, eps);
+    *drhodp = rho0 * q.gamma * p0 / dmax(denom * denom, eps);
+    return rho1;
+  }
+  if (q.type == ECG_EOS_SG) {
+    num = q.gamma * (p1 + q.pinf);
+    denom = num + p0 - p1;
+    rho1 = rho0 * num / nonzero(denom, eps);
+    *drhodp = rho0 * q.gamma * (p0 + q.pinf) / dmax(denom * denom, eps);
+    return rho1;
+  }
+  num = q.gamma * (p1 + q.pinf);
+  denom = num + p0 - p1 + q.b * rho0 * (p1 - p0);
+  rho1 = rho0 * num / nonzero(denom, eps);
+  *drhodp = rho0 * q.gamma * (p0 + q.pinf - q.b * rho0 * (p0 + q.pinf)) / nonzero(denom * denom, eps);
+  return rho1;
+}
+
+// verifyAndModifyPressure (EosIG.cpp:250, EosSG.cpp:252, EosNASG.cpp:268)
+__device__ __forceinline__ double eos_fix_p(const EosParams& q, double p) {
+  if (q.type == ECG_EOS_IG) return (p < 1.e-8) ? 1.e-8 : p;
+  double floor = -(1. - 1.e-15) * q.pinf + 1.e-15;
+  return (p <= floor) ? floor : p;
+}
+
+__device__ __forceinline__ void eos_rho_max(const EosParams& q, double& rho) {  // verifyAndCorrectDensityMax(density)
+  if (q.type == ECG_EOS_NASG && rho > 1. / q.b - 1.) rho = 1. / q.b - 1.;
+}
+
+// ------------------------------------------------------------------------------ model parameters
+
+template <int NP>
+struct Model {
+  EosParams eos[NP];
+  double eps;  // epsilonAlphaNull: 1e-15 with alphaNull, else 0 (src/Eos/Eos.cpp:88-97)
+};
+
+// PhaseUEq::verifyAndCorrectPhase src/Models/UEq/PhaseUEq.cpp:348 (alpha / density clamps)
+__device__ __forceinline__ void phase_fix_ar(double eps, double& a, double& r) {
+  if (eps > 1.e-20) {
+    if (a < 0.) a = 0.;
+    if (a > 1.) a = 1.;
+    if (r <= 1.e-15) r = 1.e-15;
+  } else {
+    if (a < 1e-15) a = 1e-14;
+    if (a > 1. - 1e-15) a = 1. - 1e-14;
+    if (r < 1.e-15) r = 1.e-14;
+  }
+}
+
+// Thermodynamic closure of one side of a face or of a cell: what fulfillState computes
+// (ModUEq::fulfillState src/Models/UEq/ModUEq.cpp:99 -> PhaseUEq::extendedCalculusPhase :97,
+// MixUEq::computeMixtureVariables src/Models/UEq/MixUEq.cpp:136).
+template <int NP>
+struct Thermo {
+  double a[NP], r[NP], p[NP], e[NP];
+  double rho, pm, cF, em;
+};
+
+template <int NP>
+__device__ __forceinline__ void fulfill(const Model<NP>& M, Thermo<NP>& t) {
+  double c[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    t.e[k] = eos_e(M.eos[k], M.eps, t.r[k], t.p[k]);
+    c[k] = eos_c(M.eos[k], M.eps, t.r[k], t.p[k]);
+  }
+  t.rho = 0.;
+  t.pm = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    t.rho += t.a[k] * t.r[k];
+    t.pm += t.a[k] * t.p[k];
+  }
+  double em = 0., cF = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double Y = t.a[k] * t.r[k] / dmax(t.rho, M.eps);
+    em += Y * t.e[k];
+    cF += Y * c[k] * c[k];
+  }
+  t.em = em;
+  t.cF = sqrt(cF);
+}
+
+// Face-frame projection of a Cartesian face (src/Maths/Coord.cpp:133-151 with the frames of
+// src/Meshes/MeshCartesian.cpp:281-557).  axis 0/1/2; neg = true for the Xm/Ym/Zm boundary frames.
+__device__ __forceinline__ void to_local(int axis, bool neg, const double u[3], double l[3]) {
+  if (axis == 0) {
+    if (!neg) { l[0] = u[0]; l[1] = u[1]; l[2] = u[2]; }
+    else { l[0] = -u[0]; l[1] = -u[1]; l[2] = u[2]; }
+  } else if (axis == 1) {
+    if (!neg) { l[0] = u[1]; l[1] = -u[0]; l[2] = u[2]; }
+    else { l[0] = -u[1]; l[1] = u[0]; l[2] = u[2]; }
+  } else {
+    if (!neg) { l[0] = u[2]; l[1] = u[0]; l[2] = u[1]; }
+    else { l[0] = -u[2]; l[1] = -u[0]; l[2] = u[1]; }
+  }
+}
+__device__ __forceinline__ void to_global(int axis, bool neg, const double f[3], double g[3]) {
+  if (axis == 0) {
+    if (!neg) { g[0] = f[0]; g[1] = f[1]; g[2] = f[2]; }
+    else { g[0] = -f[0]; g[1] = -f[1]; g[2] = f[2]; }
+  } else if (axis == 1) {
+    if (!neg) { g[0] = -f[1]; g[1] = f[0]; g[2] = f[2]; }
+    else { g[0] = f[1]; g[1] = -f[0]; g[2] = f[2]; }
+  } else {
+    if (!neg) { g[0] = f[1]; g[1] = f[2]; g[2] = f[0]; }
+    else { g[0] = -f[1]; g[1] = f[2]; g[2] = -f[0]; }
+  }
+}
+
+// Face flux of the Kapila / UEq system, in the absolute frame.
+template <int NP>
+struct Flux {
+  double a[NP], m[NP], en[NP];
+  double mom[3];
+  double E;
+  double sM, uStar;
+};
+
+// HLLC: ModUEq::solveRiemannIntern src/Models/UEq/ModUEq.cpp:113-267.  L and R carry local-frame
+// velocities ul/ur (normal first).  dtmax is min-updated with lCFL/|s|.
+template <int NP>
+__device__ __forceinline__ void hllc(const Model<NP>& M, const Thermo<NP>& L, const double ul[3],
+                                     const Thermo<NP>& R, const double ur[3], double dxL, double dxR,
+                                     double& dtmax, double Fn[3], Flux<NP>& F) {
+  double uL = ul[0], cL = L.cF, pL = L.pm, rhoL = L.rho;
+  double uR = ur[0], cR = R.cF, pR = R.pm, rhoR = R.rho;
+  double sL = dmin(uL - cL, uR - cR);
+  double sR = dmax(uR + cR, uL + cL);
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * dxL / fabs(sL));
+  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, 1. * dxR / fabs(sR));
+  double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
+  double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+  if (fabs(sM) < 1.e-8) sM = 0.;
+  F.sM = sM;
+  if (sL >= 0. || sR <= 0.) {
+    const bool left = (sL >= 0.);
+    const Thermo<NP>& S = left ? L : R;
+    const double* us = left ? ul : ur;
+    double un = us[0], rhoS = S.rho, pS = S.pm;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      F.a[k] = S.a[k] * sM;
+      F.m[k] = S.a[k] * S.r[k] * un;
+      F.en[k] = S.a[k] * S.r[k] * S.e[k] * un;
+    }
+    double Et = S.em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
+    Fn[0] = rhoS * un * un + pS;
+    Fn[1] = rhoS * us[1] * un;
+    Fn[2] = rhoS * us[2] * un;
+    F.E = (rhoS * Et + pS) * un;
+    F.uStar = un;
+  } else {
+    const bool left = (sM >= 0.);
+    const Thermo<NP>& S = left ? L : R;
+    const double* us = left ? ul : ur;
+    double sK = left ? sL : sR;
+    double mK = left ? mL : mR;
+    double uK = us[0], pK = S.pm;
+    double Et = S.em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
+    double rhoStar = mK / (sK - sM);
+    double EStar = Et + (sM - uK) * (sM + pK / mK);
+    double pStar = mK * (sM - uK) + pK;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      double mk = S.r[k] * (sK - uK);
+      double rks = mk / (sK - sM);
+      eos_rho_max(M.eos[k], rks);
+      double pks = eos_p_isentropic(M.eos[k], M.eps, S.p[k], S.r[k], rks);
+      double eks = eos_e(M.eos[k], M.eps, rks, pks);
+      F.a[k] = S.a[k] * sM;
+      F.m[k] = S.a[k] * rks * sM;
+      F.en[k] = S.a[k] * rks * eks * sM;
+    }
+    Fn[0] = rhoStar * sM * sM + pStar;
+    Fn[1] = rhoStar * us[1] * sM;
+    Fn[2] = rhoStar * us[2] * sM;
+    F.E = (rhoStar * EStar + pStar) * sM;
+    F.uStar = sM;
+  }
+}
+
+// Limiters src/Order2/Limiter{Minmod,VanLeer,VanAlbada,SuperBee,MC,THINC}.cpp:43-55
+__device__ __forceinline__ double limiter(int kind, double s1, double s2) {
+  double slope = 0., prod = s1 * s2;
+  switch (kind) {
+    case ECG_LIM_MINMOD:
+    case ECG_LIM_THINC:
+      if (prod > 1e-9) {
+        slope = dmin(fabs(s1), fabs(s2));
+        if (s1 < 0) slope = -slope;
+      }
+      return slope;
+    case ECG_LIM_VANLEER: {
+      double sum = s1 + s2;
+      if ((fabs(sum) > 1e-6) && (prod > 1e-6)) slope = 2. * prod / sum;
+      return slope;
+    }
+    case ECG_LIM_VANALBADA: {
+      double sum = s1 + s2;
+      if ((fabs(s1) > 1e-6) && (fabs(s2) > 1e-6) && (fabs(sum) > 1e-6) && (prod > 1e-6))
+        slope = prod * sum / (s1 * s1 + s2 * s2);
+      return slope;
+    }
+    case ECG_LIM_SUPERBEE:
+      if (prod > 1e-6) slope = dmax(dmin(2. * fabs(s1), fabs(s2)), dmin(fabs(s1), 2. * fabs(s2)));
+      if (s1 < 0.) slope = -slope;
+      return slope;
+    case ECG_LIM_MC:
+      if (prod > 1e-9) {
+        slope = dmin(2. * fabs(s1), 2. * fabs(s2));
+        slope = dmin(slope, 0.5 * (fabs(s1) + fabs(s2)));
+      }
+      if (s1 < 0.) slope = -slope;
+      return slope;
+    default:
+      return 0.;
+  }
+}
+
+// ------------------------------------------------------------------------ relaxation (pressure)
+
+struct RelaxStats {
+  int iters;      // Newton evaluations of this cell (0 if skipped)
+  bool fallback;  // reached 100 iterations -> interface pressure
+  bool seeded;    // a learned seed was used
+  bool rejected;  // the learned seed was rejected (plain start used)
+};
+
+// RelaxationPInfinite::relaxation src/Relaxations/RelaxationPInfinite.cpp:43-97 with
+// RelaxationP::NewtonRaphson src/Relaxations/RelaxationP.cpp:43-68.  a/r/p are the phase state
+// after buildPrim (p per phase); the phase sound speeds of that state are needed only by the
+// interface-pressure fallback, RelaxationP::computeInterfacePressure :72, recomputed there from
+// the same rho_k, p_k as PhaseUEq::extendedCalculusPhase does).  On return a/r hold
+// the relaxed state and pstar the relaxed pressure; returns false if the relaxation was skipped.
+template <int NP>
+__device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], double r[NP], const double p[NP],
+                                           double& pstar, RelaxStats& st, double seed, bool use_seed,
+                                           int max_iter) {
+  st.iters = 0;
+  st.fallback = false;
+  st.seeded = false;
+  st.rejected = false;
+  if (M.eps > 1.e-20) {
+    bool relax = true;
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+      if (a[k] > (1. - 1.e-5)) relax = false;
+    if (!relax) return false;
+  }
+  double ps = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) ps += a[k] * p[k];
+  if (use_seed) {
+    // A learned initial guess replaces sum_k alpha_k p_k only when it is finite and inside the
+    // bracket of the phase pressures; otherwise it is rejected and the plain start is kept.
+    double lo = p[0], hi = p[0];
+#pragma unroll
+    for (int k = 1; k < NP; k++) { lo = dmin(lo, p[k]); hi = dmax(hi, p[k]); }
+    if (isfinite(seed) && seed >= lo && seed <= hi) { ps = seed; st.seeded = true; }
+    else st.rejected = true;
+  }
+  double aS[NP], rS[NP];
+  double f = 0., df = 1., drhodp = 0.;
+  int iteration = 0;
+  do {
+    iteration++;
+    ps -= f / df;
+#pragma unroll
+    for (int k = 0; k < NP; k++) ps = eos_fix_p(M.eos[k], ps);
+    f = -1.;
+    df = 0.;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      rS[k] = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], ps, &drhodp);
+      aS[k] = a[k] * r[k] / rS[k];
+      double dalpha = a[k] * r[k] * drhodp / (rS[k] * rS[k]);
+      f += aS[k];
+      df -= dalpha;
+    }
+  } while (fabs(f) > 1e-10 && iteration < max_iter);
+  st.iters = iteration;
+  if (iteration < max_iter) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) { a[k] = aS[k]; r[k] = rS[k]; }
+    pstar = ps;
+    return true;
+  }
+  st.fallback = true;
+  double zk[NP], pI = 0., sumZk = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) zk[k] = r[k] * eos_c(M.eos[k], M.eps, r[k], p[k]);
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    sumZk += zk[k];
+    double sumZj = 0.;
+#pragma unroll
+    for (int j = 0; j < NP; j++)
+      if (j != k) sumZj += zk[j];
+    pI += sumZj * (p[k] - 0.);
+  }
+  pI /= sumZk * (NP - 1);
+#pragma unroll
+  for (int k = 0; k < NP; k++) pI = eos_fix_p(M.eos[k], pI);
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double rr = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], pI, &drhodp);
+    a[k] = a[k] * r[k] / rr;
+    r[k] = rr;
+  }
+  pstar = pI;
+  return true;
+}
+
+// ------------------------------------------------------------------ relaxation (p-T-mu, 2 phases)
+
+// Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
+__device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
+                                               bool& err) {
+  double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
+  double gV = V.gamma, piV = (V.type == ECG_EOS_IG) ? 0. : V.pinf, cvV = V.cv, e0V = V.eref, s0V = V.sref;
+  double A = (gL * cvL - gV * cvV + s0V - s0L) / (gV * cvV - cvV);
+  double B = (e0L - e0V) / (gV * cvV - cvV);
+  double C = (gV * cvV - gL * cvL) / (gV * cvV - cvV);
+  double D = (gL * cvL - cvL) / (gV * cvV - cvV);
+  int iteration = 0;
+  double Tsat = 0.1 * B / C, f = 0., df = 1.;
+  do {
+    Tsat -= f / df;
+    iteration++;
+    if (iteration > 50) {
+      err = true;
+      break;
+    }
+    f = A + B / Tsat + C * log(Tsat) - log(p + piV) + D * log(p + piL);
+    df = C / Tsat - B / (Tsat * Tsat);
+  } while (fabs(f) > 1e-10);
+  double dfdp = -1. / (p + piV) + D / (p + piL);
+  *dTsat = -dfdp / df;
+  return Tsat;
+}
+
+// computeDensitySaturation (EosIG.cpp:170, EosSG.cpp:172, EosNASG.cpp:189)
+__device__ __forceinline__ double eos_rho_sat(const EosParams& q, double eps, double p, double Tsat, double dTsat,
+                                              double* drhodp) {
+  double pp = (q.type == ECG_EOS_IG) ? p : p + q.pinf;
+  double g1cvT = (q.gamma - 1.) * q.cv * Tsat;
+  double den = (q.type == ECG_EOS_NASG) ? g1cvT + q.b * (p + q.pinf) : g1cvT;
+  double d = (q.gamma - 1.) * q.cv * Tsat - pp * (q.gamma - 1.) * q.cv * dTsat;
+  *drhodp = d / dmax(den * den, eps);
+  return pp / dmax(den, eps);
+}
+
+// computeDensityEnergySaturation (EosIG.cpp:184, EosSG.cpp:186, EosNASG.cpp:203)
+__device__ __forceinline__ double eos_rhoe_sat(const EosParams& q, double p, double rho, double drhodp,
+                                               double* drhoedp) {
+  if (q.type == ECG_EOS_IG) {
+    *drhoedp = 1. / (q.gamma - 1.) + drhodp * q.eref;
+    return p / (q.gamma - 1.) + rho * q.eref;
+  }
+  if (q.type == ECG_EOS_SG) {
+    *drhoedp = 1. / (q.gamma - 1.) + drhodp * q.eref;
+    return (p + q.gamma * q.pinf) / (q.gamma - 1.) + rho * q.eref;
+  }
+  *drhoedp = (1. - rho * q.b) / (q.gamma - 1.) + drhodp * (q.eref - q.b * (p + q.gamma * q.pinf) / (q.gamma - 1.));
+  return (p + q.gamma * q.pinf) * (1. - rho * q.b) / (q.gamma - 1.) + rho * q.eref;
+}
+
+// RelaxationPTMu::relaxation src/Relaxations/RelaxationPTMu.cpp:73-200.  rhomix / emix are the
+// mixture density and internal energy the cell holds at that point (from buildPrim).  Returns true
+// when the phases were updated (the reference then calls fulfillState, so the mixture density
+// is recomputed from the new phases).
+template <int NP>
+__device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap, double pcrit, double a[NP],
+                                           double r[NP], double p[NP], double rhomix, double emix, bool& err) {
+  const EosParams& EL = M.eos[liq];
+  const EosParams& EV = M.eos[vap];
+  double pStar = 0., Tsat, dTsat = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) pStar += a[k] * p[k];
+  if (pStar > pcrit) return false;
+  double rho = rhomix, rhoe = rho * emix;
+  double pv = eos_p(EV, M.eps, rho, emix);
+  double Tv = eos_T(EV, M.eps, rho, pv);
+  if (pv > 0) {
+    Tsat = compute_tsat(EL, EV, pv, &dTsat, err);
+    if (Tv >= Tsat) {
+      a[vap] = 1.;
+      a[liq] = 0.;
+      r[vap] = rho;
+      p[vap] = pv;
+      return true;
+    }
+  }
+  double pl = eos_p(EL, M.eps, rho, emix);
+  double Tl = eos_T(EL, M.eps, rho, pl);
+  if (pl > 0.) {
+    Tsat = compute_tsat(EL, EV, pl, &dTsat, err);
+    if (Tl <= Tsat) {
+      a[liq] = 1.;
+      a[vap] = 0.;
+      r[liq] = rho;
+      p[liq] = pl;
+      return true;
+    }
+  }
+  double rhoLSat = 0., rhoVSat = 0., drhoLSat, drhoVSat, aLSat = 0., aVSat = 0., daLSat, daVSat;
+  double rhoeLSat, rhoeVSat, drhoeLSat, drhoeVSat;
+  int iteration = 0;
+  double f = 0., df = 1.;
+  do {
+    pStar -= f / df;
+    iteration++;
+    if (iteration > 50) {
+      err = true;
+      break;
+    }
+#pragma unroll
+    for (int k = 0; k < NP; k++) pStar = eos_fix_p(M.eos[k], pStar);
+    Tsat = compute_tsat(EL, EV, pStar, &dTsat, err);
+    rhoLSat = eos_rho_sat(EL, M.eps, pStar, Tsat, dTsat, &drhoLSat);
+    rhoVSat = eos_rho_sat(EV, M.eps, pStar, Tsat, dTsat, &drhoVSat);
+    aLSat = (rho - rhoVSat) / (rhoLSat - rhoVSat);
+    daLSat = (-drhoVSat * (rhoLSat - rhoVSat) - (rho - rhoVSat) * (drhoLSat - drhoVSat)) /
+             ((rhoLSat - rhoVSat) * (rhoLSat - rhoVSat));
+    aVSat = 1. - aLSat;
+    daVSat = -daLSat;
+    f = rhoe;
+    df = 0.;
+    rhoeLSat = eos_rhoe_sat(EL, pStar, rhoLSat, drhoLSat, &drhoeLSat);
+    rhoeVSat = eos_rhoe_sat(EV, pStar, rhoVSat, drhoVSat, &drhoeVSat);
+    f -= (aLSat * rhoeLSat + aVSat * rhoeVSat);
+    df -= (daLSat * rhoeLSat + aLSat * drhoeLSat + daVSat * rhoeVSat + aVSat * drhoeVSat);
+    f /= rhoe;
+    df /= rhoe;
+  } while (fabs(f) > 1e-10);
+  a[liq] = aLSat;
+  r[liq] = rhoLSat;
+  p[liq] = pStar;
+  a[vap] = aVSat;
+  r[vap] = rhoVSat;
+  p[vap] = pStar;
+  return true;
+}
+
+// ------------------------------------------------------------------ energy correction
+
+// Cell::correctionEnergy src/Order1/Cell.cpp:327: MixUEq::totalEnergyToInternalEnergy :175 then
+// FluxPUEq::correctionEnergy src/Models/PUEq/FluxPUEq.cpp:68-112 (mixture-EOS pressure).
+template <int NP>
+__device__ __forceinline__ double correction_pressure(const Model<NP>& M, const double a[NP], const double r[NP],
+                                                      double rhomix, double E, double usq) {
+  double e = E - 0.5 * usq;
+  double rhoe = rhomix * e;
+  double pp = rhoe, denom = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    const EosParams& q = M.eos[k];
+    double gpi = (q.type == ECG_EOS_IG) ? 0. : q.gamma * q.pinf / (q.gamma - 1.);
+    double ig = 1. / (q.gamma - 1.);
+    double cov = (q.type == ECG_EOS_NASG) ? q.b : 0.;
+    pp -= a[k] * (gpi * (1. - r[k] * cov) + r[k] * q.eref);
+    denom += a[k] * ig * (1. - r[k] * cov);
+  }
+  return pp / denom;
+}
+
+}  // namespace ecg

@@ -1,0 +1,22 @@
+// Host-side helpers shared by the library's translation units.
+#pragma once
+#include <algorithm>
+#include <string>
+
+#include "../../include/ecogen_b200.h"
+
+namespace ecg {
+
+void set_error(const std::string& msg);
+
+// Number of field pointers in the ABI layout of a case (see include/ecogen_b200.h).
+inline int abi_nfields(const ecg_case& c) { return c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5; }
+
+// EOS internal energy e(rho, p), same expression as the kernels and the reference EOS classes.
+inline double host_eos_e(const ecg_eos& q, double eps, double rho, double p) {
+  if (q.type == ECG_EOS_IG) return p / (q.gamma - 1.) / std::max(rho, eps) + q.eref;
+  if (q.type == ECG_EOS_SG) return (p + q.gamma * q.pinf) / (q.gamma - 1.) / std::max(rho, eps) + q.eref;
+  return (p + q.gamma * q.pinf) * std::max(1. - rho * q.b, eps) / (q.gamma - 1.) / std::max(rho, eps) + q.eref;
+}
+
+}  // namespace ecg

@@ -1,0 +1,126 @@
+// Fused Kapila (PUEq) step kernels for uniform Cartesian meshes.
+//
+// One kernel launch performs one face-flux pass plus the cell update that follows it:
+//   PASS_O1   first order: fluxes on S^n, U^{n+1} = U^n + dt*sum F, buildPrim, relaxation,
+//             energy correction                           (Run::solveHyperbolic + solveRelaxations)
+//   PASS_PRED MUSCL predictor: fluxes of the reconstructed S^n, U^{n+1/2} = U^n + dt/2*sum F,
+//             buildPrim, relaxation, energy correction     (CellO2::predictionOrdre2, src/Order2/CellO2.cpp:111)
+//   PASS_CORR MUSCL corrector: fluxes of the reconstructed S^{n+1/2}, U^{n+1} = U^n + dt*sum F,
+//             buildPrim, relaxation, energy correction     (Run::solveHyperbolicO2 steps 6-8 + solveRelaxations)
+//
+// Work decomposition.  A block owns a tile of cells (TX x TY x TZ, one thread per cell).  For
+// each axis in turn it stages the tile plus a halo of H cells along that axis in shared
+// memory (H = 1 first order, 2 MUSCL), computes every face slope once, then every face flux of
+// the tile once (one thread per face), and each cell thread accumulates its two faces of that
+// axis in the reference order (left face added, right face subtracted,
+// CellInterface::addFlux/subtractFlux src/Order1/CellInterface.cpp:267-297).  Boundary faces
+// come last in the order Xm, Xp, Ym, Yp, Zm, Zp, as MeshCartesian enumerates them
+// (src/Meshes/MeshCartesian.cpp:384-557).  Accumulation therefore happens in exactly the
+// reference's order, with no atomics: each cell is written by one thread.
+#pragma once
+#include "ecg_device.cuh"
+
+namespace ecg {
+
+enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
+
+template <int DIM>
+struct TileShape;
+template <>
+struct TileShape<1> { static constexpr int X = 256, Y = 1, Z = 1; };
+template <>
+struct TileShape<2> { static constexpr int X = 32, Y = 8, Z = 1; };
+template <>
+struct TileShape<3> { static constexpr int X = 16, Y = 4, Z = 4; };
+
+// Field indices of a state array (stride = ncells):
+//   alpha_k [0,NP), rho_k [NP,2NP), p 2NP, u_d 2NP+1+d, E 2NP+1+DIM
+template <int NP, int DIM>
+struct Fields {
+  static constexpr int A = 0, R = NP, P = 2 * NP, U = 2 * NP + 1, E = 2 * NP + 1 + DIM;
+  static constexpr int NQ = 2 * NP + 1 + DIM;    // primitive fields used by fluxes
+  static constexpr int NS = NQ + 1;              // full state (with E)
+  static constexpr int NSL = 3 * NP + DIM;       // slope components: alpha_k, rho_k, p_k, u_d
+  static constexpr int NFL = 3 * NP + DIM + 3;   // flux components: a_k, m_k, e_k, mom_d, E, sM, uStar
+};
+
+// Device scalars of a context's time loop (Run::solver src/Run.cpp:385-490).
+struct DevScalars {
+  double dt;                       // step being taken (1e-15 before the first step, src/Run.cpp:38)
+  double t;                        // physical time
+  double cfl;
+  double t_end;
+  unsigned long long dtmax_bits;   // min over faces of lCFL/|s|, as ordered bits of a positive double
+  long long it, max_it;
+  int mode;                        // 0: free stepping, 1: stop after max_it, 2: stop once t >= t_end
+  int done;                        // set once the stop condition holds; later steps are no-ops
+};
+
+struct StepParams {
+  const int* done;      // device flag: skip the launch when set
+  const double* q;      // primitives the fluxes are built from (S^n, or S^{n+1/2} in the corrector)
+  const double* sn;     // S^n (U^n, non-conservative terms, time-n alpha_0 of neighbours)
+  double* out;          // S^{n+1/2} (predictor) or S^{n+1}
+  int64_t n;            // cells
+  const double* dt;     // device scalar: current time step
+  unsigned long long* dtmax_bits;  // device scalar: min over faces of lCFL/|s| as ordered bits
+  DevStats* stats;
+  int lim[4];
+  int newton_cap;
+  // learned seed (optional)
+  const float* mlp;     // packed weights (nullptr = plain start)
+  int mlp_nin;
+  // recording of (features, converged pressure) pairs
+  float* rec_x;
+  float* rec_y;
+  unsigned long long* rec_count;
+  unsigned long long rec_max;
+  // p-T-mu relaxation
+  int ptmu, ptmu_liq, ptmu_vap;
+  double pcrit;
+};
+
+__device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, double v) {
+  // positive doubles order like their bit patterns
+  atomicMin(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+
+// Reduces the per-thread relaxation counters of a block (warp reductions, then shared atomics)
+// and adds them to the device counters with one global atomic per counter and block.
+// Every thread of the block must call it.
+__device__ __forceinline__ void block_counters(DevStats* st, unsigned int relax, unsigned int iters,
+                                               unsigned int fallback, unsigned int seeded, unsigned int rejected,
+                                               unsigned int nonfinite, unsigned int ptmu) {
+  __shared__ unsigned int sc[24];
+  const int tid = threadIdx.x;
+  if (tid < 24) sc[tid] = 0u;
+  __syncthreads();
+  const unsigned full = 0xffffffffu;
+  unsigned int v[7] = {relax, iters, fallback, seeded, rejected, nonfinite, ptmu};
+#pragma unroll
+  for (int i = 0; i < 7; i++) {
+    unsigned int w = __reduce_add_sync(full, v[i]);
+    if ((tid & 31) == 0 && w) atomicAdd(&sc[i], w);
+  }
+  unsigned int mx = __reduce_max_sync(full, iters);
+  if ((tid & 31) == 0 && mx) atomicMax(&sc[7], mx);
+  if (relax) atomicAdd(&sc[8 + (iters < 16 ? (iters >= 1 ? iters - 1 : 0) : 15)], 1u);
+  __syncthreads();
+  if (tid < 24 && sc[tid]) {
+    unsigned long long x = sc[tid];
+    switch (tid) {
+      case 0: atomicAdd(&st->relax_calls, x); break;
+      case 1: atomicAdd(&st->newton_evals, x); break;
+      case 2: atomicAdd(&st->newton_fallback, x); break;
+      case 3: atomicAdd(&st->seeded, x); break;
+      case 4: atomicAdd(&st->seed_rejected, x); break;
+      case 5: atomicAdd(&st->nonfinite, x); break;
+      case 6: atomicAdd(&st->ptmu_errors, x); break;
+      case 7: atomicMax(&st->newton_max, x); break;
+      default: atomicAdd(&st->hist[tid - 8], x); break;
+    }
+  }
+}
+
+}  // namespace ecg

@@ -1,0 +1,213 @@
+/*
+ * ecogen_b200 — C ABI of the B200 (sm_100a) explicit finite-volume step of ECOGEN.
+ *
+ * The library replaces, for Cartesian non-AMR Euler / Kapila (PUEq) cases, the part of the
+ * reference CPU run loop that advances the solution by one time step:
+ *   Run::solveHyperbolic / Run::solveHyperbolicO2 + Run::solveRelaxations
+ *   (src/Run.cpp:696, :627, :771) and the dt update of Run::solver (src/Run.cpp:406-440).
+ * The entry points below take plain host pointers and sizes; device memory, streams and
+ * CUDA graphs belong to a context.  Calls on one context are not reentrant; independent
+ * contexts may be used from different threads.
+ *
+ * Field layout used by upload/download (n = number of cells, cell index i + j*nx + k*nx*ny as
+ * src/Meshes/MeshCartesian.cpp:141 orders cells): a caller passes an array of pointers, one per
+ * field, in the order
+ *   alpha_0 .. alpha_{N-1}, rho_0 .. rho_{N-1}, p, u_x, u_y, u_z, E            (Kapila, N phases)
+ *   rho, p, u_x, u_y, u_z, E                                                   (Euler)
+ * each pointing at n doubles.  For Kapila, p is the mixture pressure sum_k alpha_k p_k as the
+ * reference writes it ("Pressure_Mixture", src/Models/UEq/MixUEq.cpp:201); E is the specific
+ * total energy ("Total_energy_Mixture").
+ */
+#ifndef ECOGEN_B200_H
+#define ECOGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  ECG_OK = 0,
+  ECG_ERR_INVALID = 1,      /* bad argument (null pointer, size mismatch, bad enum) */
+  ECG_ERR_UNSUPPORTED = 2,  /* case outside this library's scope (AMR, unstructured, add-phys, ...) */
+  ECG_ERR_CUDA = 3,         /* a CUDA runtime call failed; see ecg_last_error() */
+  ECG_ERR_XML = 4,          /* malformed or incomplete case input (reference: ErrorXML*) */
+  ECG_ERR_PHYSICS = 5,      /* a physics check failed during the step (reference: errors vector) */
+  ECG_ERR_NOMEM = 6,        /* device or host allocation failed */
+  ECG_ERR_TOO_LARGE = 7,    /* size above a stated maximum */
+  ECG_ERR_TIMEOUT = 8       /* a bounded device-side wait gave up */
+} ecg_status;
+
+enum { ECG_MODEL_KAPILA = 0, ECG_MODEL_EULER = 1 };
+enum { ECG_EOS_IG = 0, ECG_EOS_SG = 1, ECG_EOS_NASG = 2 };
+enum {
+  ECG_LIM_NONE = 0, ECG_LIM_MINMOD = 1, ECG_LIM_VANLEER = 2, ECG_LIM_VANALBADA = 3,
+  ECG_LIM_SUPERBEE = 4, ECG_LIM_MC = 5, ECG_LIM_THINC = 6
+};
+#define ECG_MAX_PHASES 3
+
+/* One EOS (src/Eos/EosIG.h, EosSG.h, EosNASG.h parameters). */
+typedef struct {
+  int32_t type;                 /* ECG_EOS_* */
+  double gamma, pinf, b, cv, eref, sref;
+} ecg_eos;
+
+/* A case as the four ECOGEN XML files describe it (Input::readInputXML src/InputOutput/Input.cpp:54). */
+typedef struct {
+  int32_t model;                /* ECG_MODEL_* */
+  int32_t nphases;              /* Kapila: 2..3 ; Euler: 1 */
+  int32_t alpha_null;           /* model.xml alphaNull */
+  int32_t order;                /* 1 first order, 2 MUSCL-Hancock (secondOrder) */
+  int32_t limiter[4];           /* global, interface, global vol.-fraction, interface vol.-fraction */
+  int32_t ncells[3];            /* nx, ny, nz (mesh.xml numberCells) */
+  double length[3];             /* lx, ly, lz (mesh.xml dimensions) */
+  double cfl;                   /* main.xml computationControl CFL */
+  int32_t time_iterations;      /* 1: stop after max_iterations ; 0: stop at total_time */
+  int32_t max_iterations;
+  double total_time;
+  int32_t ptmu;                 /* p-T-mu relaxation (model.xml <relaxation type="PTMu">) */
+  int32_t ptmu_liquid, ptmu_vapor;
+  ecg_eos eos[ECG_MAX_PHASES];
+} ecg_case;
+
+/* Counters of one ecg_step call (replace the reference's errors / warnings vectors). */
+typedef struct {
+  int64_t cell_updates;         /* cells x steps advanced */
+  int64_t relax_calls;          /* pressure relaxations performed (not skipped) */
+  int64_t newton_evals;         /* Newton evaluations summed over relaxations */
+  int64_t newton_fallback;      /* relaxations that hit the iteration cap (interface pressure used) */
+  int64_t newton_max;           /* largest Newton evaluation count of one relaxation */
+  int64_t seeded;               /* relaxations started from the learned seed */
+  int64_t seed_rejected;        /* learned seeds rejected (plain start used) */
+  int64_t ptmu_errors;          /* p-T-mu solves above 50 iterations (reference: error, run stops) */
+  int64_t nonfinite_cells;      /* cells whose state became NaN/inf */
+  int64_t newton_hist[16];      /* histogram of Newton evaluations: bins 1..15, 16+ in [15] */
+} ecg_step_stats;
+
+typedef struct ecg_ctx ecg_ctx;
+typedef struct ecg_input ecg_input;
+
+/* ------------------------------------------------------------------ status / version */
+const char* ecg_status_str(ecg_status s);
+/* Text of the last error seen on this thread (CUDA error string, XML path, ...). */
+const char* ecg_last_error(void);
+int ecg_version(void);
+
+/* ------------------------------------------------------------------ case input (XML) */
+/* Reads <case_dir>/{main,mesh,model,initialConditions}.xml and the EOS files they name from
+ * <eos_dir> (ECOGEN reads them from <work>/libEOS, Input::inputEOS src/InputOutput/Input.cpp:865).
+ * Replaces Input::readInputXML for the Cartesian Euler / Kapila cases this library runs. */
+ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, ecg_input** out);
+void ecg_input_free(ecg_input* in);
+ecg_status ecg_input_case(const ecg_input* in, ecg_case* out);
+/* Run name (main.xml <run>) and output format; strings are owned by the input. */
+const char* ecg_input_run_name(const ecg_input* in);
+/* Fills the initial primitive fields on the host, domain by domain in document order
+ * (GeometricalDomain::fillIn src/Geometries/GeometricalDomain.cpp:64).  Field layout as above. */
+ecg_status ecg_input_fill(const ecg_input* in, double* const* fields, int64_t ncells);
+
+/* ------------------------------------------------------------------ one case on one GPU */
+/* Creates a context on the current CUDA device: device state, stream, dt accumulator.
+ * Replaces Run::initialize's mesh and cell allocation (src/Run.cpp:69-160). */
+ecg_status ecg_create(const ecg_case* c, ecg_ctx** out);
+void ecg_destroy(ecg_ctx* ctx);
+/* Host -> device copy of the primitive fields (initial condition or restart); completes the
+ * thermodynamic state like Cell::completeFulfillState (src/Order1/Cell.cpp:344). */
+ecg_status ecg_upload_prim(ecg_ctx* ctx, const double* const* fields, int64_t ncells);
+/* Device -> host copy of the fields as the reference writes them. */
+ecg_status ecg_download_prim(ecg_ctx* ctx, double* const* fields, int64_t ncells);
+/* Per-phase temperature and mass fraction (reference output "F<k>_Temperature" / "F<k>_Mass fraction");
+ * T and Y each receive nphases*n doubles, phase-major. */
+ecg_status ecg_download_derived(ecg_ctx* ctx, double* T, double* Y, int64_t ncells);
+/* Advances nsteps time steps.  *dt is the step to take first (1e-15 before the first step,
+ * src/Run.cpp:38) and on return the next one, cfl*dtMax (src/Run.cpp:439); *t accumulates.
+ * stats may be NULL.  Returns ECG_ERR_PHYSICS if a physics check failed (the state is kept). */
+ecg_status ecg_step(ecg_ctx* ctx, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats);
+/* Diagnostic form of ecg_step: launches every kernel separately (no graph) and adds each one's
+ * device time, measured with CUDA events on the context's stream, to kernel_ms[0..2]:
+ * [0] first-order or MUSCL predictor pass, [1] MUSCL corrector pass, [2] time-step update. */
+ecg_status ecg_step_profiled(ecg_ctx* ctx, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats,
+                             double* kernel_ms);
+/* Runs the reference time loop to its stop condition (iterations or total time), in chunks
+ * captured as CUDA graphs. */
+ecg_status ecg_run(ecg_ctx* ctx, double* dt, double* t, int32_t* iterations, ecg_step_stats* stats);
+/* Number of cells, phases and the CUDA stream of a context. */
+int64_t ecg_ncells(const ecg_ctx* ctx);
+void* ecg_stream(const ecg_ctx* ctx);
+/* Newton iteration cap (default 100, RelaxationP::NewtonRaphson src/Relaxations/RelaxationP.cpp:66);
+ * a lower cap forces the interface-pressure fallback and is used to test that path. */
+ecg_status ecg_set_newton_cap(ecg_ctx* ctx, int32_t cap);
+/* Device-resident variants for callers that keep their own device buffers: fields[] point at
+ * device memory laid out as above.  Run on the context's stream. */
+ecg_status ecg_upload_prim_device(ecg_ctx* ctx, const double* const* dfields, int64_t ncells);
+ecg_status ecg_download_prim_device(ecg_ctx* ctx, double* const* dfields, int64_t ncells);
+
+/* ------------------------------------------------------------------ learned relaxation seed */
+/* A 9 -> 64 -> 64 -> 1 (or nin -> h -> h -> 1) GELU MLP whose output seeds the pressure-relaxation
+ * Newton iteration (RelaxationP::NewtonRaphson start, src/Relaxations/RelaxationPInfinite.cpp:58-63).
+ * Newton still iterates to |f| <= 1e-10, so the plain iteration remains the judge. */
+#define ECG_MLP_MAX_IN 16
+#define ECG_MLP_HIDDEN 64
+typedef struct {
+  int32_t n_in;                 /* input features (<= ECG_MLP_MAX_IN) */
+  int32_t hidden;               /* must be ECG_MLP_HIDDEN */
+  const float* w1;              /* [hidden][n_in] */
+  const float* b1;              /* [hidden] */
+  const float* w2;              /* [hidden][hidden] */
+  const float* b2;              /* [hidden] */
+  const float* w3;              /* [hidden] */
+  float b3;
+  float in_shift[ECG_MLP_MAX_IN], in_scale[ECG_MLP_MAX_IN]; /* feature normalisation */
+  float out_shift, out_scale;   /* target de-normalisation */
+} ecg_mlp;
+/* Installs (copies) the weights; NULL restores the plain start sum_k alpha_k p_k. */
+ecg_status ecg_set_seed_model(ecg_ctx* ctx, const ecg_mlp* mlp);
+/* Records up to max_pairs (features, converged pressure) pairs from the relaxations of the next
+ * ecg_step calls into an internal device buffer; ecg_fetch_pairs copies them out. */
+ecg_status ecg_record_pairs(ecg_ctx* ctx, int64_t max_pairs);
+ecg_status ecg_fetch_pairs(ecg_ctx* ctx, float* features, float* targets, int64_t* count);
+
+/* ------------------------------------------------------------------ MLP training on the GPU */
+typedef struct ecg_trainer ecg_trainer;
+ecg_status ecg_trainer_create(int32_t n_in, int32_t hidden, uint64_t seed, ecg_trainer** out);
+void ecg_trainer_destroy(ecg_trainer* tr);
+/* One AdamW epoch over (x, y) (host arrays, n rows), minibatches of `batch`; returns mean loss. */
+ecg_status ecg_trainer_epoch(ecg_trainer* tr, const float* x, const float* y, int64_t n, int32_t batch, float lr,
+                             float weight_decay, float* mean_loss);
+/* Forward + backward of one batch: loss and the gradients of every parameter (for gradient checks). */
+ecg_status ecg_trainer_grad(ecg_trainer* tr, const float* x, const float* y, int32_t n, float* loss, float* gw1,
+                            float* gb1, float* gw2, float* gb2, float* gw3, float* gb3);
+ecg_status ecg_trainer_forward(ecg_trainer* tr, const float* x, int32_t n, float* yhat);
+/* Current parameters (host copies owned by the trainer) in ecg_mlp form, with normalisation fields
+ * set from the last ecg_trainer_set_norm call. */
+ecg_status ecg_trainer_export(ecg_trainer* tr, ecg_mlp* out);
+ecg_status ecg_trainer_import(ecg_trainer* tr, const ecg_mlp* in);
+ecg_status ecg_trainer_set_norm(ecg_trainer* tr, const float* in_shift, const float* in_scale, float out_shift,
+                                float out_scale);
+
+/* ------------------------------------------------------------------ batched independent cases */
+/* Many independent 1D cases of uneven cell counts advanced together by one persistent kernel per
+ * pass that pulls (case, tile) work items from a device queue; each case keeps its own dt
+ * (segmented min-reduction) and time.  All cases must share model, phases, EOS, order and
+ * limiters; their cell counts, lengths, CFL and initial states differ.  The reference runs such
+ * cases one after another (src/main.cpp:82-133). */
+typedef struct ecg_batch ecg_batch;
+ecg_status ecg_batch_create(const ecg_case* cases, int32_t ncases, ecg_batch** out);
+void ecg_batch_destroy(ecg_batch* b);
+/* fields[f] points at sum(ncells) doubles: case 0's cells, then case 1's, ... */
+ecg_status ecg_batch_upload_prim(ecg_batch* b, const double* const* fields, int64_t total_cells);
+ecg_status ecg_batch_download_prim(ecg_batch* b, double* const* fields, int64_t total_cells);
+/* Advance every case nsteps steps (each with its own dt); dt/t arrays of ncases (may be NULL). */
+ecg_status ecg_batch_step(ecg_batch* b, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats);
+ecg_status ecg_batch_set_seed_model(ecg_batch* b, const ecg_mlp* mlp);
+/* Tile size (cells per work item) and threads per block; 0 = autotuned. */
+ecg_status ecg_batch_set_shape(ecg_batch* b, int32_t tile, int32_t threads);
+ecg_status ecg_batch_autotune(ecg_batch* b, int32_t* tile, int32_t* threads);
+int64_t ecg_batch_total_cells(const ecg_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

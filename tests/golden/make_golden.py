@@ -1,0 +1,88 @@
+"""Generates the golden fixtures of tests/golden/ by running the reference ECOGEN solver.
+
+The reference is built from its own sources by ``make -C oracle ref`` (single-rank MPI stand-in,
+``oracle/Makefile``).  Each fixture is the final state the reference writes (base64 Float64 VTK,
+read back exactly by oracle/refrun.py) for one small case from ecogen_b200/cases.py, plus the
+initial state (result file 0).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from ecogen_b200 import cases  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def golden_cases():
+    """Name -> case.  Small versions of every workload family plus edge cases."""
+    g = {}
+    g["tube1d_o1_full"] = cases.shock_tube_1d(ncells=1000)  # 1000 cells to t = 240 us (797 steps)
+    g["tube1d_o2_vanleer"] = cases.shock_tube_1d(ncells=200, iterations=60, order="vanleer")
+    g["tube1d_alphanull"] = cases.shock_tube_1d(ncells=120, iterations=40, alpha_floor=0.0, alpha_null=True,
+                                                name="tubeAlphaNull")
+    g["tube1d_nasg_o2"] = cases.shock_tube_1d(ncells=150, iterations=30, order="minmod", liquid=cases.WATER_NASG,
+                                              name="tubeNASG")
+    g["bubble2d_o2"] = cases.shock_bubble_2d(n=32, iterations=12)
+    c = cases.shock_bubble_2d(n=24, iterations=8, limiter="vanleer", name="bubbleLimiters")
+    c.interface_limiter, c.vf_limiter, c.interface_vf_limiter = "superbee", "minmod", "mc"
+    g["bubble2d_limiters"] = c
+    g["bubble2d_vanalbada"] = cases.shock_bubble_2d(n=20, iterations=6, limiter="vanalbada", name="bubbleVanAlbada")
+    g["bubble2d_o1"] = cases.shock_bubble_2d(n=24, iterations=8, limiter=None, name="bubbleO1")
+    g["cavity3d_o2"] = cases.cavity_collapse_3d(n=12, iterations=4, ninclusions=6, radius_cells=(2.0, 4.0))
+    g["cavity3d_o1"] = cases.cavity_collapse_3d(n=10, iterations=3, ninclusions=4, radius_cells=(2.0, 3.0),
+                                                limiter=None, name="cavityO1")
+    g["expansion2d_ptmu"] = cases.expansion_tube_2d(n=24, iterations=8)
+    g["euler1d_o1"] = cases.euler_shock_tube(ncells=200, iterations=40)
+    g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
+    return g
+
+
+def case_meta(c) -> dict:
+    return {"name": c.name, "cells": list(c.cells), "lengths": list(c.lengths), "nphases": c.nphases,
+            "model": c.model, "iterations": c.iterations, "total_time": c.total_time, "cfl": c.cfl,
+            "order": c.second_order, "limiters": [c.interface_limiter, c.vf_limiter, c.interface_vf_limiter]}
+
+
+def main():
+    if not refrun.available():
+        sys.exit("reference binary missing: run `make -C oracle ref` first")
+    work = os.path.join(ROOT, "_work", "runs", "golden")
+    for key, c in golden_cases().items():
+        w = os.path.join(work, key)
+        shutil.rmtree(w, ignore_errors=True)
+        d = c.write(w)
+        cases.write_ecogen_list(w, [d])
+        r = refrun.run(w)
+        if r.returncode != 0:
+            raise SystemExit(f"{key}: reference failed\n{r.stdout[-3000:]}")
+        files = refrun.result_files(w, c.name)
+        f0 = refrun.reference_prim(refrun.read_vtr(files[0]), c.nphases)
+        f1 = refrun.reference_prim(refrun.read_vtr(files[-1]), c.nphases)
+        it, t, dt = refrun.info(w, c.name)
+        arrays = {}
+        for tag, f in (("init", f0), ("final", f1)):
+            for name, v in f.items():
+                if v is not None:
+                    arrays[f"{tag}_{name}"] = np.asarray(v)
+        np.savez_compressed(os.path.join(OUT, f"{key}.npz"), **arrays)
+        meta = case_meta(c)
+        meta.update({"iterations_done": it, "time6": t, "dt6": dt})
+        with open(os.path.join(OUT, f"{key}.json"), "w") as fh:
+            json.dump(meta, fh, indent=1)
+        print(key, "iterations", it, "t", t)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,106 @@
+"""C ABI: the library loads without a GPU, exports every declared symbol, reads case inputs."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from ecogen_b200 import api, cases
+from oracle import oracle
+from tests.conftest import ROOT, display, load_golden
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "ecogen_b200.h")).read()
+    return sorted(set(re.findall(r"\b(ecg_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    assert len(declared_symbols()) >= 30
+
+
+@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "cavity3d_o2", "expansion2d_ptmu", "euler1d_o1"])
+def test_xml_input_fill_matches_reference_initial_state(key, golden_cases, tmp_path):
+    _, g = load_golden(key)
+    case = golden_cases[key]
+    d = case.write(str(tmp_path))
+    inp = api.Input(d, os.path.join(str(tmp_path), "libEOS"))
+    f = inp.fill()
+    k = case.nphases
+    if case.model.upper() == "EULER":
+        assert np.array_equal(f[0], g["init_rho"][0])
+        assert np.array_equal(f[1], g["init_p"])
+    else:
+        assert np.array_equal(display(np.stack(f[:k]), "alpha"), g["init_alpha"])
+        assert np.array_equal(np.stack(f[k:2 * k]), g["init_rho"])
+        # E is the total energy of Cell::completeFulfillState
+        assert np.array_equal(f[2 * k + 4], g["init_E"])
+    sim = oracle.Sim(case)
+    assert np.array_equal(f[-1], sim.fields()["E"])
+
+
+def test_case_record_from_xml(tmp_path):
+    case = cases.shock_bubble_2d(n=16, iterations=5)
+    case.interface_limiter = "superbee"
+    d = case.write(str(tmp_path))
+    inp = api.Input(d, os.path.join(str(tmp_path), "libEOS"))
+    c = inp.case
+    assert (c.model, c.nphases, c.order) == (api.MODEL_KAPILA, 2, 2)
+    assert list(c.limiter) == [2, 4, 2, 4]
+    assert list(c.ncells) == [16, 16, 1] and c.cfl == 0.6
+    assert c.time_iterations == 1 and c.max_iterations == 5
+    assert c.eos[0].type == 1 and c.eos[0].pinf == 6e8 and c.eos[1].type == 0
+    assert inp.run_name == "shockBubble2D"
+
+
+def _expect(status, fn):
+    with pytest.raises(api.EcgError) as ei:
+        fn()
+    assert ei.value.status == status
+
+
+def test_malformed_inputs_are_input_errors(tmp_path):
+    # reference non-regression error cases: a missing element and a missing attribute
+    case = cases.shock_tube_1d(ncells=50, iterations=3)
+    d = case.write(str(tmp_path))
+    eosdir = os.path.join(str(tmp_path), "libEOS")
+    main = open(os.path.join(d, "main.xml")).read()
+    open(os.path.join(d, "main.xml"), "w").write(main.replace("<run>shockTube1D</run>", ""))
+    _expect(4, lambda: api.Input(d, eosdir))
+    open(os.path.join(d, "main.xml"), "w").write(main)
+    mesh = open(os.path.join(d, "mesh.xml")).read()
+    open(os.path.join(d, "mesh.xml"), "w").write(mesh.replace(' y="1"', ""))
+    _expect(4, lambda: api.Input(d, eosdir))
+    open(os.path.join(d, "mesh.xml"), "w").write(mesh.replace("<numberCells", "<numberCells").replace("</mesh>", ""))
+    _expect(4, lambda: api.Input(d, eosdir))  # unterminated root
+
+
+def test_unsupported_inputs_are_refused(tmp_path):
+    case = cases.shock_tube_1d(ncells=50, iterations=3)
+    d = case.write(str(tmp_path))
+    eosdir = os.path.join(str(tmp_path), "libEOS")
+    mesh = open(os.path.join(d, "mesh.xml")).read()
+    open(os.path.join(d, "mesh.xml"), "w").write(
+        mesh.replace("</cartesianMesh>", '<AMR lvlMax="1" criteriaVar="0.1" varRho="true" varP="false" '
+                                          'varU="false" varAlpha="false" xiSplit="0.1" xiJoin="0.1"/></cartesianMesh>'))
+    _expect(2, lambda: api.Input(d, eosdir))
+    open(os.path.join(d, "mesh.xml"), "w").write(mesh)
+    ic = open(os.path.join(d, "initialConditions.xml")).read()
+    open(os.path.join(d, "initialConditions.xml"), "w").write(ic.replace('type="nonReflecting" number="1"',
+                                                                          'type="wall" number="1"'))
+    _expect(2, lambda: api.Input(d, eosdir))
+
+
+def test_create_rejects_bad_cases_without_gpu_work():
+    c = api.Case()
+    c.model, c.nphases, c.order = 0, 4, 1
+    c.ncells[0], c.ncells[1], c.ncells[2] = 10, 1, 1
+    c.length[0] = c.length[1] = c.length[2] = 1.0
+    h = api.C.c_void_p()
+    st = api.lib().ecg_create(api.C.byref(c), api.C.byref(h))
+    assert st == 2 and not h.value
+    c.nphases, c.ncells[0] = 2, 1
+    assert api.lib().ecg_create(api.C.byref(c), api.C.byref(h)) == 1
