@@ -548,6 +548,8 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
   h.done = (mode == 1 && h.it >= h.max_it) || (mode == 2 && h.t >= h.t_end);
   ECG_CUDA(cudaMemcpyAsync(x->scal, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
   ECG_CUDA(cudaMemsetAsync(x->stats, 0, sizeof(DevStats), x->stream));
+  const int cur0 = x->cur;  // a step that finds the stop flag set writes nothing, so the state that
+                            // holds the result is decided by the number of steps actually taken
   int64_t done_steps = 0;
   if (kernel_ms) {
     cudaEvent_t ev[4];
@@ -587,6 +589,7 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
   ECG_CUDA(cudaMemcpyAsync(&ds, x->stats, sizeof(ds), cudaMemcpyDeviceToHost, x->stream));
   ECG_CUDA(cudaStreamSynchronize(x->stream));
   done_steps = r.it - h.it;
+  x->cur = cur0 ^ (int)(done_steps & 1);
   *dt = r.dt;
   *t = r.t;
   if (iterations) *iterations = (int32_t)r.it;

@@ -1,0 +1,291 @@
+// Per-cell pieces of the Kapila step shared by the single-case kernels (ecg_step_kapila.cu) and
+// the batched kernel (ecg_batch.cu): face reconstruction, flux accumulation and the cell update
+// (U^n, time evolution, buildPrim, relaxations, energy correction, store).
+#pragma once
+#include "ecg_mlp_device.cuh"
+#include "ecg_step.cuh"
+
+namespace ecg {
+
+struct CellCounters {
+  unsigned int relax = 0, iters = 0, fallback = 0, seeded = 0, rejected = 0, nonfinite = 0, ptmu = 0;
+};
+
+// Reconstructs one side of an internal face (CellInterfaceO2Cartesian::solveRiemann
+// src/Order2/CellInterfaceO2Cartesian.cpp:101-160 with CellO2Cartesian::computeLocalSlopes
+// src/Order2/CellO2Cartesian.cpp:23-171 on a Cartesian mesh): the limited slope combines the slope
+// of this face (s1) and of the face on the opposite side of the cell along the same axis (s2, zero
+// when that face is a boundary); the interface detector decides between the global and interface
+// limiters; the state is extrapolated by `sign * slope * dist` and clamped.
+template <int NP, int DIM>
+__device__ __forceinline__ void reconstruct_side(const Model<NP>& M, const int lim[4], const double* sq, int RS, int rc,
+                                                 const double* ssl, int SS, int f1, int f2, double alphaCell,
+                                                 double alphaOther, double alphaAfter, double dist, double sign,
+                                                 Thermo<NP>& t, double u[3]) {
+  using FL = Fields<NP, DIM>;
+  const bool iface = (alphaCell >= 1.e-4) && (alphaCell <= 1. - 1.e-4) &&
+                     ((alphaOther - alphaCell) * (alphaCell - alphaAfter) >= 1.e-8);
+  const int lg = iface ? lim[1] : lim[0];
+  const int lv = iface ? lim[3] : lim[2];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double s1a = ssl[(k)*SS + f1], s1r = ssl[(NP + k) * SS + f1], s1p = ssl[(2 * NP + k) * SS + f1];
+    double s2a = 0., s2r = 0., s2p = 0.;
+    if (f2 >= 0) {
+      s2a = ssl[(k)*SS + f2];
+      s2r = ssl[(NP + k) * SS + f2];
+      s2p = ssl[(2 * NP + k) * SS + f2];
+    }
+    double la = limiter(lv, s1a, s2a), lr = limiter(lg, s1r, s2r), lp = limiter(lg, s1p, s2p);
+    double a = sq[(FL::A + k) * RS + rc], r = sq[(FL::R + k) * RS + rc];
+    double p = eos_fix_p(M.eos[k], sq[FL::P * RS + rc]);  // phase pressure of the cell
+    a += (sign * la) * dist;
+    r += (sign * lr) * dist;
+    p += (sign * lp) * dist;
+    phase_fix_ar(M.eps, a, r);
+    p = eos_fix_p(M.eos[k], p);
+    eos_rho_max(M.eos[k], r);
+    t.a[k] = a;
+    t.r[k] = r;
+    t.p[k] = p;
+  }
+  u[0] = u[1] = u[2] = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    double s1 = ssl[(3 * NP + d) * SS + f1];
+    double s2 = (f2 >= 0) ? ssl[(3 * NP + d) * SS + f2] : 0.;
+    double l = limiter(lg, s1, s2);
+    u[d] = sq[(FL::U + d) * RS + rc] + (sign * l) * dist;
+  }
+  fulfill<NP>(M, t);
+}
+
+template <int NP, int DIM>
+__device__ __forceinline__ void cell_thermo(const Model<NP>& M, const double* sq, int RS, int rc, Thermo<NP>& t,
+                                            double u[3]) {
+  using FL = Fields<NP, DIM>;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    t.a[k] = sq[(FL::A + k) * RS + rc];
+    t.r[k] = sq[(FL::R + k) * RS + rc];
+    t.p[k] = eos_fix_p(M.eos[k], sq[FL::P * RS + rc]);
+  }
+  u[0] = u[1] = u[2] = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) u[d] = sq[(FL::U + d) * RS + rc];
+  fulfill<NP>(M, t);
+}
+
+template <int NP, int DIM>
+__device__ __forceinline__ void acc_face(double cA, bool add, const Flux<NP>& F, const double an[NP],
+                                         const double pn[NP], double aa[NP], double am[NP], double ae[NP],
+                                         double amom[DIM], double& aE) {
+  // FluxUEq::addFlux/subtractFlux src/Models/UEq/FluxUEq.cpp:61,85 then
+  // FluxPUEq::addNonCons/subtractNonCons src/Models/PUEq/FluxPUEq.cpp:44,56 (time-n alpha_k, p_k).
+  if (add) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      aa[k] += cA * F.a[k];
+      am[k] += cA * F.m[k];
+      ae[k] += cA * F.en[k];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; d++) amom[d] += cA * F.mom[d];
+    aE += cA * F.E;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      aa[k] += -cA * an[k] * F.sM;
+      ae[k] += cA * an[k] * pn[k] * F.uStar;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      aa[k] -= cA * F.a[k];
+      am[k] -= cA * F.m[k];
+      ae[k] -= cA * F.en[k];
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; d++) amom[d] -= cA * F.mom[d];
+    aE -= cA * F.E;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      aa[k] -= -cA * an[k] * F.sM;
+      ae[k] -= cA * an[k] * pn[k] * F.uStar;
+    }
+  }
+}
+
+
+// Non-reflecting boundary face of a cell: HLLC(cell, cell) in the face frame, subtracted from the
+// cell (BoundCondNonReflecting::solveRiemannBoundary src/BoundConds/BoundCondNonReflecting.cpp:62,
+// BoundCond::computeFlux src/BoundConds/BoundCond.cpp:61; the buffer cell is fulfilled first, :84).
+template <int NP, int DIM>
+__device__ __forceinline__ void boundary_face(const Model<NP>& M, const double* q, int64_t nn, int64_t cell, int ax,
+                                              bool neg, double lcfl, double coefA, double& dtmax, const double an[NP],
+                                              const double pn[NP], double aa[NP], double am[NP], double ae[NP],
+                                              double amom[DIM], double& aE) {
+  using FL = Fields<NP, DIM>;
+  Thermo<NP> t;
+  double ug[3], ul[3], Fn[3];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    t.a[k] = q[(int64_t)(FL::A + k) * nn + cell];
+    t.r[k] = q[(int64_t)(FL::R + k) * nn + cell];
+    t.p[k] = eos_fix_p(M.eos[k], q[(int64_t)FL::P * nn + cell]);
+  }
+  ug[0] = ug[1] = ug[2] = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) ug[d] = q[(int64_t)(FL::U + d) * nn + cell];
+  fulfill<NP>(M, t);
+  to_local(ax, neg, ug, ul);
+  Flux<NP> F;
+  hllc<NP>(M, t, ul, t, ul, lcfl, lcfl, dtmax, Fn, F);
+  to_global(ax, neg, Fn, F.mom);
+  acc_face<NP, DIM>(coefA, false, F, an, pn, aa, am, ae, amom, aE);
+}
+
+// The cell update that follows the flux accumulation of one pass (everything after
+// "solveHyperbolic's face loop" for one cell).  aa/am/ae/amom/aE hold sum_faces coefA*F (+ the
+// non-conservative terms); an/rn/pn are the cell's time-n alpha_k, rho_k, p_k.
+template <int NP, int DIM, int PASS, bool PTMU>
+__device__ __forceinline__ void kapila_update(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
+                                              double dt, const double an[NP], const double rn[NP],
+                                              const double pn[NP], double aa[NP], double am[NP], double ae[NP],
+                                              double amom[DIM], double aE, CellCounters& cc) {
+  using FL = Fields<NP, DIM>;
+  // ---- U^n (FluxUEq::buildCons src/Models/UEq/FluxUEq.cpp:147) and time evolution
+  //      (Cell::timeEvolution src/Order1/Cell.cpp:286: m_cons*dt then + U^n)
+  const double scale = (PASS == PASS_PRED) ? 0.5 * dt : dt;
+  double rhon = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) rhon += an[k] * rn[k];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double Uk_m = an[k] * rn[k];
+    double Uk_e = an[k] * rn[k] * eos_e(M.eos[k], M.eps, rn[k], pn[k]);
+    aa[k] = aa[k] * scale + 1. * an[k];
+    am[k] = am[k] * scale + 1. * Uk_m;
+    ae[k] = ae[k] * scale + 1. * Uk_e;
+  }
+  double un[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    un[d] = P.sn[(int64_t)(FL::U + d) * nn + cell];
+    amom[d] = amom[d] * scale + 1. * (rhon * un[d]);
+  }
+  double En = P.sn[(int64_t)FL::E * nn + cell];
+  aE = aE * scale + 1. * (rhon * En);
+
+  // ---- buildPrim (FluxUEq::buildPrim src/Models/UEq/FluxUEq.cpp:161-209)
+  double un_sum = 0.;
+  if (M.eps > 1.e-20) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      if (aa[k] < 0.) aa[k] = 0.;
+      if (aa[k] > 1.) aa[k] = 1.;
+      un_sum += aa[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      if (aa[k] <= 1.e-15) aa[k] = 1e-15;
+      if (aa[k] >= 1. - 1.e-15) aa[k] = 1.0 - 1e-15;
+      un_sum += aa[k];
+    }
+  }
+  double a[NP], r[NP], pk[NP];
+  double rhoMel = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    aa[k] /= un_sum;
+    rhoMel += am[k];
+    a[k] = aa[k];
+    r[k] = am[k] / dmax(aa[k], M.eps);
+    if (M.eos[k].type == ECG_EOS_NASG && r[k] > 1. / M.eos[k].b - 1.) {  // verifyAndCorrectDensityMax(mass)
+      r[k] = 1. / M.eos[k].b - 1.;
+      a[k] = am[k] / r[k];
+    }
+    double ek = ae[k] / dmax(am[k], M.eps);
+    pk[k] = eos_p(M.eos[k], M.eps, r[k], ek);
+    phase_fix_ar(M.eps, a[k], r[k]);
+    pk[k] = eos_fix_p(M.eos[k], pk[k]);
+  }
+  double u[DIM], usq = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    u[d] = amom[d] / rhoMel;
+    if (fabs(u[d]) < 1.e-8) u[d] = 0.;
+    usq += u[d] * u[d];
+  }
+  double E = aE / rhoMel;
+  // mixture density (and internal energy for p-T-mu) of the rebuilt state
+  double rhomix = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
+
+  // ---- relaxations (Model::relaxations src/Models/Model.cpp:74): pressure, then p-T-mu
+  RelaxStats rs;
+  double seed = 0.;
+  bool use_seed = false;
+  if (P.mlp != nullptr) {
+    seed = mlp_seed<NP>(P.mlp, P.mlp_nin, a, r, pk);
+    use_seed = true;
+  }
+  double a0[NP], r0[NP], p0[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) { a0[k] = a[k]; r0[k] = r[k]; p0[k] = pk[k]; }
+  double pstar = 0.;
+  bool relaxed = relax_pinf<NP>(M, a, r, pk, pstar, rs, seed, use_seed, P.newton_cap);
+  if (relaxed) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) pk[k] = pstar;
+    if (P.rec_x != nullptr && !rs.fallback) record_pair<NP>(P.rec_x, P.rec_y, P.rec_count, P.rec_max, a0, r0, p0, pstar);
+  }
+  if (PTMU) {
+    // mixture internal energy of the rebuilt state (MixUEq::computeMixtureVariables :136), which
+    // RelaxationPTMu reads before any fulfillState
+    double emix = 0.;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      double Y = a0[k] * r0[k] / dmax(rhomix, M.eps);
+      emix += Y * eos_e(M.eos[k], M.eps, r0[k], p0[k]);
+    }
+    bool err = false;
+    if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err)) {
+      rhomix = 0.;
+#pragma unroll
+      for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
+    }
+    if (err) cc.ptmu = 1;
+  }
+
+  // ---- energy correction (FluxPUEq::correctionEnergy) and clamps
+  double p = correction_pressure<NP>(M, a, r, rhomix, E, usq);
+#pragma unroll
+  for (int k = 0; k < NP; k++) phase_fix_ar(M.eps, a[k], r[k]);
+
+  // ---- store
+  bool finite = isfinite(p) && isfinite(E);
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    P.out[(int64_t)(FL::A + k) * nn + cell] = a[k];
+    P.out[(int64_t)(FL::R + k) * nn + cell] = r[k];
+    finite = finite && isfinite(a[k]) && isfinite(r[k]);
+  }
+  P.out[(int64_t)FL::P * nn + cell] = p;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) P.out[(int64_t)(FL::U + d) * nn + cell] = u[d];
+  if (PASS != PASS_PRED) P.out[(int64_t)FL::E * nn + cell] = E;
+
+  // ---- counters
+  if (relaxed) {
+    cc.relax = 1;
+    cc.iters = (unsigned int)rs.iters;
+    cc.fallback = rs.fallback ? 1u : 0u;
+    cc.seeded = rs.seeded ? 1u : 0u;
+    cc.rejected = rs.rejected ? 1u : 0u;
+  }
+  cc.nonfinite = finite ? 0u : 1u;
+}
+
+}  // namespace ecg

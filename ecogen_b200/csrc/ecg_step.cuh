@@ -91,7 +91,8 @@ __device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, 
 // Every thread of the block must call it.
 __device__ __forceinline__ void block_counters(DevStats* st, unsigned int relax, unsigned int iters,
                                                unsigned int fallback, unsigned int seeded, unsigned int rejected,
-                                               unsigned int nonfinite, unsigned int ptmu) {
+                                               unsigned int nonfinite, unsigned int ptmu, unsigned int max_iters,
+                                               bool hist) {
   __shared__ unsigned int sc[24];
   const int tid = threadIdx.x;
   if (tid < 24) sc[tid] = 0u;
@@ -103,9 +104,9 @@ __device__ __forceinline__ void block_counters(DevStats* st, unsigned int relax,
     unsigned int w = __reduce_add_sync(full, v[i]);
     if ((tid & 31) == 0 && w) atomicAdd(&sc[i], w);
   }
-  unsigned int mx = __reduce_max_sync(full, iters);
+  unsigned int mx = __reduce_max_sync(full, max_iters);
   if ((tid & 31) == 0 && mx) atomicMax(&sc[7], mx);
-  if (relax) atomicAdd(&sc[8 + (iters < 16 ? (iters >= 1 ? iters - 1 : 0) : 15)], 1u);
+  if (hist && relax) atomicAdd(&sc[8 + (iters < 16 ? (iters >= 1 ? iters - 1 : 0) : 15)], 1u);
   __syncthreads();
   if (tid < 24 && sc[tid]) {
     unsigned long long x = sc[tid];
