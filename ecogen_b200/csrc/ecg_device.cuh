@@ -387,6 +387,71 @@ __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], dou
   return true;
 }
 
+
+// ------------------------------------------------------------------ correctly rounded log
+// The saturation temperature solve (Mixture::computeTsat) branches on tight tests (pure-phase
+// hypotheses, |f| > 1e-10), so a last-ulp difference between CUDA's log and the host libm's can
+// change a cell's path.  cr_log evaluates log(x) in double-double arithmetic (error-free sum and
+// product transformations; log(m) = 2 atanh((m-1)/(m+1)) for m in [1/sqrt2, sqrt2), k ln2 added
+// in double-double) to ~1e-30 relative accuracy and rounds once, i.e. it returns the correctly
+// rounded logarithm, as the host libm does in all but extremely rare cases.
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  double s = a + b, bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ DD dd_fast_sum(double a, double b) {
+  double s = a + b;
+  return {s, b - (s - a)};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD s = dd_two_sum(a.hi, b.hi), t = dd_two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = dd_fast_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return dd_fast_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+  double p = a.hi * b.hi;
+  double e = __fma_rn(a.hi, b.hi, -p);
+  e += a.hi * b.lo + a.lo * b.hi;
+  return dd_fast_sum(p, e);
+}
+__device__ __forceinline__ DD dd_div(DD a, DD b) {
+  double q1 = a.hi / b.hi;
+  DD r = dd_add(a, dd_mul(b, DD{-q1, 0.}));
+  double q2 = r.hi / b.hi;
+  r = dd_add(r, dd_mul(b, DD{-q2, 0.}));
+  double q3 = r.hi / b.hi;
+  return dd_add(dd_fast_sum(q1, q2), DD{q3, 0.});
+}
+__device__ __noinline__ double cr_log(double x) {
+  if (!(x > 0.) || isinf(x)) return log(x);
+  int k;
+  double m = frexp(x, &k);
+  if (m < 0.70710678118654752440) {
+    m *= 2.;
+    k -= 1;
+  }
+  DD num{m - 1., 0.};                 // exact (Sterbenz)
+  DD den = dd_two_sum(m, 1.);
+  DD s = dd_div(num, den);
+  DD s2 = dd_mul(s, s);
+  double t = 1. / 45.;                // tail sum_{i>=3} s^(2(i-3)) / (2i+1), i = 3..22, in double
+  for (int i = 21; i >= 3; i--) t = t * s2.hi + 1. / (2. * i + 1.);
+  DD P = dd_add(dd_div(DD{1., 0.}, DD{5., 0.}), dd_mul(s2, DD{t, 0.}));
+  P = dd_add(dd_div(DD{1., 0.}, DD{3., 0.}), dd_mul(s2, P));
+  P = dd_add(DD{1., 0.}, dd_mul(s2, P));
+  DD lm = dd_mul(s, P);
+  lm.hi *= 2.;
+  lm.lo *= 2.;
+  const DD ln2{0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56};
+  DD r = dd_add(dd_mul(ln2, DD{(double)k, 0.}), lm);
+  return r.hi + r.lo;
+}
+
 // ------------------------------------------------------------------ relaxation (p-T-mu, 2 phases)
 
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
@@ -407,7 +472,7 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
       err = true;
       break;
     }
-    f = A + B / Tsat + C * log(Tsat) - log(p + piV) + D * log(p + piL);
+    f = A + B / Tsat + C * cr_log(Tsat) - cr_log(p + piV) + D * cr_log(p + piL);
     df = C / Tsat - B / (Tsat * Tsat);
   } while (fabs(f) > 1e-10);
   double dfdp = -1. / (p + piV) + D / (p + piL);
