@@ -427,7 +427,7 @@ __device__ __forceinline__ DD dd_div(DD a, DD b) {
   double q3 = r.hi / b.hi;
   return dd_add(dd_fast_sum(q1, q2), DD{q3, 0.});
 }
-__device__ __noinline__ double cr_log(double x) {
+static __device__ __noinline__ double cr_log(double x) {
   if (!(x > 0.) || isinf(x)) return log(x);
   int k;
   double m = frexp(x, &k);
