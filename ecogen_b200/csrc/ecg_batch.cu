@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
   double* sa0 = sq + (size_t)FL::NQ * RS;
   double* ssl = sq + (size_t)K::NQ * RS;
   double* sfl = ssl + (O2 ? (size_t)FL::NSL * SS : 0);
+  MlpSmem* smlp = reinterpret_cast<MlpSmem*>(sfl + (size_t)FL::NFL * FS);  // present when a seed model is set
   __shared__ int s_item;
   __shared__ double red[32];
   const StepParams& P = B.P;
@@ -72,6 +73,10 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
   const int tid = threadIdx.x;
   CellCounters total;
   unsigned int max_iters = 0;
+  if (P.mlp != nullptr) {
+    mlp_load(smlp, P.mlp, P.mlp_nin);
+    __syncthreads();
+  }
 
   for (;;) {
     if (tid == 0) s_item = (int)atomicAdd(B.queue, 1u);
@@ -153,6 +158,7 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
     }
     __syncthreads();
     const int g = org + tid;
+    CellPrim<NP, 1> cp;
     if (g < n) {
       const int64_t cell = C.off + g;
       double an[NP], rn[NP], pn[NP], aa[NP], am[NP], ae[NP], amom[1] = {0.}, aE = 0.;
@@ -185,8 +191,14 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
       if (g == 0) boundary_face<NP, 1>(M, P.q, nn, cell, 0, true, C.lcfl, C.coefA, dtmax, an, pn, aa, am, ae, amom, aE);
       if (g == n - 1)
         boundary_face<NP, 1>(M, P.q, nn, cell, 0, false, C.lcfl, C.coefA, dtmax, an, pn, aa, am, ae, amom, aE);
+      kapila_rebuild<NP, 1, PASS>(P, M, nn, cell, B.scal[c].dt, an, rn, pn, aa, am, ae, amom, aE, cp);
+    }
+    double seed = 0.;
+    if (P.mlp != nullptr) seed = mlp_seed_warp<NP>(smlp, g < n, cp.a, cp.r, cp.pk);
+    if (g < n) {
+      const int64_t cell = C.off + g;
       CellCounters cc;
-      kapila_update<NP, 1, PASS, false>(P, M, nn, cell, B.scal[c].dt, an, rn, pn, aa, am, ae, amom, aE, cc);
+      kapila_finish<NP, 1, PASS, false>(P, M, nn, cell, cp, seed, P.mlp != nullptr, cc);
       total.relax += cc.relax;
       total.iters += cc.iters;
       total.fallback += cc.fallback;
@@ -231,11 +243,12 @@ template <int NP, int TB, int PASS>
 static cudaError_t batch_one(const BatchParams& B, const ecg_eos* eos, double eps, int grid, cudaStream_t s,
                              bool prepare, int* max_blocks) {
   auto kern = k_batch<NP, TB, PASS>;
-  const size_t sm = BatchTile<NP, TB, PASS>::smem_bytes();
+  const size_t base = BatchTile<NP, TB, PASS>::smem_bytes();
+  const size_t sm = base + (B.P.mlp != nullptr ? sizeof(MlpSmem) : 0);
   if (prepare) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(base + sizeof(MlpSmem)));
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks, kern, TB, sm);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks, kern, TB, base + sizeof(MlpSmem));
   }
   Model<NP> M;
   for (int k = 0; k < NP; k++) M.eos[k] = {eos[k].type, eos[k].gamma, eos[k].pinf, eos[k].b, eos[k].cv, eos[k].eref, eos[k].sref};

@@ -144,14 +144,23 @@ __device__ __forceinline__ void boundary_face(const Model<NP>& M, const double* 
   acc_face<NP, DIM>(coefA, false, F, an, pn, aa, am, ae, amom, aE);
 }
 
-// The cell update that follows the flux accumulation of one pass (everything after
-// "solveHyperbolic's face loop" for one cell).  aa/am/ae/amom/aE hold sum_faces coefA*F (+ the
-// non-conservative terms); an/rn/pn are the cell's time-n alpha_k, rho_k, p_k.
-template <int NP, int DIM, int PASS, bool PTMU>
-__device__ __forceinline__ void kapila_update(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
-                                              double dt, const double an[NP], const double rn[NP],
-                                              const double pn[NP], double aa[NP], double am[NP], double ae[NP],
-                                              double amom[DIM], double aE, CellCounters& cc) {
+// State of a cell after buildPrim, handed from kapila_rebuild to kapila_finish (the learned seed, when
+// installed, is evaluated between the two by the whole warp).
+template <int NP, int DIM>
+struct CellPrim {
+  double a[NP], r[NP], pk[NP];
+  double u[DIM];
+  double usq, E, rhomix;
+};
+
+// The cell update that follows the flux accumulation of one pass (everything after the face loop
+// of solveHyperbolic for one cell), first half: U^n, time evolution and buildPrim.  aa/am/ae/amom/aE
+// hold sum_faces coefA*F (+ the non-conservative terms); an/rn/pn are the time-n alpha_k, rho_k, p_k.
+template <int NP, int DIM, int PASS>
+__device__ __forceinline__ void kapila_rebuild(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
+                                               double dt, const double an[NP], const double rn[NP],
+                                               const double pn[NP], double aa[NP], double am[NP], double ae[NP],
+                                               double amom[DIM], double aE, CellPrim<NP, DIM>& cp) {
   using FL = Fields<NP, DIM>;
   // ---- U^n (FluxUEq::buildCons src/Models/UEq/FluxUEq.cpp:147) and time evolution
   //      (Cell::timeEvolution src/Order1/Cell.cpp:286: m_cons*dt then + U^n)
@@ -193,7 +202,9 @@ __device__ __forceinline__ void kapila_update(const StepParams& P, const Model<N
       un_sum += aa[k];
     }
   }
-  double a[NP], r[NP], pk[NP];
+  double* a = cp.a;
+  double* r = cp.r;
+  double* pk = cp.pk;
   double rhoMel = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
@@ -210,27 +221,38 @@ __device__ __forceinline__ void kapila_update(const StepParams& P, const Model<N
     phase_fix_ar(M.eps, a[k], r[k]);
     pk[k] = eos_fix_p(M.eos[k], pk[k]);
   }
-  double u[DIM], usq = 0.;
+  double* u = cp.u;
+  double usq = 0.;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     u[d] = amom[d] / rhoMel;
     if (fabs(u[d]) < 1.e-8) u[d] = 0.;
     usq += u[d] * u[d];
   }
-  double E = aE / rhoMel;
+  cp.usq = usq;
+  cp.E = aE / rhoMel;
   // mixture density (and internal energy for p-T-mu) of the rebuilt state
   double rhomix = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
+  cp.rhomix = rhomix;
+}
 
+
+// Relaxations, energy correction, clamps and store of one rebuilt cell.  seed / use_seed: learned
+// initial guess of the pressure relaxation (see ecg_mlp_device.cuh).
+template <int NP, int DIM, int PASS, bool PTMU>
+__device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
+                                              CellPrim<NP, DIM>& cp, double seed, bool use_seed, CellCounters& cc) {
+  using FL = Fields<NP, DIM>;
+  double* a = cp.a;
+  double* r = cp.r;
+  double* pk = cp.pk;
+  const double* u = cp.u;
+  const double usq = cp.usq, E = cp.E;
+  double rhomix = cp.rhomix;
   // ---- relaxations (Model::relaxations src/Models/Model.cpp:74): pressure, then p-T-mu
   RelaxStats rs;
-  double seed = 0.;
-  bool use_seed = false;
-  if (P.mlp != nullptr) {
-    seed = mlp_seed<NP>(P.mlp, P.mlp_nin, a, r, pk);
-    use_seed = true;
-  }
   double a0[NP], r0[NP], p0[NP];
 #pragma unroll
   for (int k = 0; k < NP; k++) { a0[k] = a[k]; r0[k] = r[k]; p0[k] = pk[k]; }

@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH)
   double* sa0 = sq + (size_t)FL::NQ * RS;                  // [NA0][RS]
   double* ssl = sa0 + (size_t)K::NA0 * RS;                 // [NSL][SS]
   double* sfl = ssl + (K::O2 ? (size_t)FL::NSL * SS : 0);  // [NFL][FS]
+  MlpSmem* smlp = reinterpret_cast<MlpSmem*>(sfl + (size_t)FL::NFL * FS);  // present when a seed model is set
 
   if (*P.done) return;  // stop condition reached earlier in a captured step sequence
   const int tid = threadIdx.x;
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH)
     }
   }
   double dtmax = 1.e10;
+  if (P.mlp != nullptr) mlp_load(smlp, P.mlp, P.mlp_nin);  // visible after the first barrier below
 
 #pragma unroll 1
   for (int ax = 0; ax < DIM; ax++) {
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH)
 
   // per-thread counters, reduced per block at the end
   CellCounters cc;
+  CellPrim<NP, DIM> cp;
   if (active) {
     // ---- boundary faces (non-reflecting: HLLC(cell, cell), BoundCondNonReflecting::solveRiemannBoundary
     //      src/BoundConds/BoundCondNonReflecting.cpp:62), subtracted from the cell (BoundCond::computeFlux :61)
@@ -210,8 +213,12 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH)
       boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE);
     }
 
-    kapila_update<NP, DIM, PASS, PTMU>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cc);
+    kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
   }
+  // learned seed of the pressure relaxation: one warp-wide tensor-core evaluation (all lanes)
+  double seed = 0.;
+  if (P.mlp != nullptr) seed = mlp_seed_warp<NP>(smlp, active, cp.a, cp.r, cp.pk);
+  if (active) kapila_finish<NP, DIM, PASS, PTMU>(P, M, nn, cell, cp, seed, P.mlp != nullptr, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
 
   // ---- dtMax: block min, one atomic per block
@@ -240,8 +247,9 @@ static cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_
   using K = KapilaStep<NP, DIM, PASS>;
   using TS = TileShape<DIM>;
   auto kern = k_kapila_step<NP, DIM, PASS, PTMU>;
-  const size_t sm = K::smem_bytes();
-  if (prepare) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const size_t sm = K::smem_bytes() + (P.mlp != nullptr ? sizeof(MlpSmem) : 0);
+  if (prepare)
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(K::smem_bytes() + sizeof(MlpSmem)));
   Model<NP> M;
   for (int k = 0; k < NP; k++) {
     M.eos[k].type = eos[k].type;

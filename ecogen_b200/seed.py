@@ -1,0 +1,180 @@
+"""Learned initial guess of the pressure-relaxation Newton iteration: record, train, install.
+
+1. ``record``: run the plain solver on training cases and let the step kernels record, for every
+   converged relaxation, the features (alpha_k, log rho_k, asinh(p_k/1e5) per phase) and the
+   position of the relaxed pressure inside the bracket of the phase pressures.
+2. ``train``: fit the 3N -> 64 -> 64 -> 1 GELU MLP with the library's own CUDA training kernels
+   (forward, backward and AdamW in ecg_mlp_train.cu).
+3. ``SeedModel.install(ctx)``: copy the weights into a context; the step kernels then evaluate the
+   network with BF16 tensor-core MMA inside the fused update and start Newton from its output.
+   Newton still iterates to |f| <= 1e-10, so the plain iteration stays the judge of convergence.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from . import api
+
+
+class SeedModel:
+    def __init__(self, mlp: api.Mlp, arrays):
+        self.mlp = mlp
+        self._arrays = arrays  # keep the weight buffers alive
+
+    def install(self, ctx: api.Context):
+        ctx.set_seed_model(self.mlp)
+
+    def install_batch(self, batch_handle):
+        api.check(api.lib().ecg_batch_set_seed_model(batch_handle, C.byref(self.mlp)), "ecg_batch_set_seed_model")
+
+    def save(self, path: str):
+        w1, b1, w2, b2, w3 = self._arrays
+        m = self.mlp
+        np.savez(path, w1=w1, b1=b1, w2=w2, b2=b2, w3=w3, b3=np.float32(m.b3),
+                 in_shift=np.array(m.in_shift[:m.n_in], dtype=np.float32),
+                 in_scale=np.array(m.in_scale[:m.n_in], dtype=np.float32),
+                 out_shift=np.float32(m.out_shift), out_scale=np.float32(m.out_scale))
+
+    @staticmethod
+    def load(path: str) -> "SeedModel":
+        d = np.load(path)
+        return make_model(d["w1"], d["b1"], d["w2"], d["b2"], d["w3"], float(d["b3"]), d["in_shift"], d["in_scale"],
+                          float(d["out_shift"]), float(d["out_scale"]))
+
+
+def make_model(w1, b1, w2, b2, w3, b3, in_shift, in_scale, out_shift, out_scale) -> SeedModel:
+    arrays = [np.ascontiguousarray(a, dtype=np.float32) for a in (w1, b1, w2, b2, w3)]
+    m = api.Mlp()
+    m.n_in = int(len(in_shift))
+    m.hidden = api.MLP_HIDDEN
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    m.w1, m.b1, m.w2, m.b2, m.w3 = (fp(a) for a in arrays)
+    m.b3 = float(b3)
+    for i in range(m.n_in):
+        m.in_shift[i] = float(in_shift[i])
+        m.in_scale[i] = float(in_scale[i])
+    m.out_shift = float(out_shift)
+    m.out_scale = float(out_scale)
+    return SeedModel(m, arrays)
+
+
+def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000) -> Tuple[np.ndarray, np.ndarray]:
+    """Run each case on the GPU for `steps` steps and collect (features, target) pairs."""
+    xs, ys = [], []
+    budget = max_pairs
+    for spec in case_specs:
+        if budget <= 0:
+            break
+        with tempfile.TemporaryDirectory() as tmp:
+            d = spec.write(tmp)
+            inp = api.Input(d, os.path.join(tmp, "libEOS"))
+            ctx = api.Context(inp.case)
+            ctx.upload(inp.fill())
+            ctx.record_pairs(budget)
+            ctx.step(steps)
+            x, y = ctx.fetch_pairs()
+            ctx.close()
+        xs.append(x)
+        ys.append(y)
+        budget -= len(y)
+    if not xs:
+        return np.zeros((0, 0), np.float32), np.zeros(0, np.float32)
+    return np.concatenate(xs), np.concatenate(ys)
+
+
+class Trainer:
+    """The library's GPU trainer (ecg_trainer_*)."""
+
+    def __init__(self, n_in: int, seed: int = 0):
+        h = C.c_void_p()
+        api.check(api.lib().ecg_trainer_create(n_in, api.MLP_HIDDEN, seed, C.byref(h)), "ecg_trainer_create")
+        self.h = h
+        self.n_in = n_in
+
+    def set_norm(self, in_shift, in_scale, out_shift, out_scale):
+        a = np.ascontiguousarray(in_shift, dtype=np.float32)
+        b = np.ascontiguousarray(in_scale, dtype=np.float32)
+        api.check(api.lib().ecg_trainer_set_norm(self.h, a.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 b.ctypes.data_as(C.POINTER(C.c_float)), out_shift, out_scale),
+                  "ecg_trainer_set_norm")
+
+    def epoch(self, x: np.ndarray, y: np.ndarray, batch: int = 4096, lr: float = 1e-3, wd: float = 1e-5) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        loss = C.c_float()
+        api.check(api.lib().ecg_trainer_epoch(self.h, x.ctypes.data_as(C.POINTER(C.c_float)),
+                                              y.ctypes.data_as(C.POINTER(C.c_float)), len(y), batch, lr, wd,
+                                              C.byref(loss)), "ecg_trainer_epoch")
+        return loss.value
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros(len(x), dtype=np.float32)
+        api.check(api.lib().ecg_trainer_forward(self.h, x.ctypes.data_as(C.POINTER(C.c_float)), len(x),
+                                                out.ctypes.data_as(C.POINTER(C.c_float))), "ecg_trainer_forward")
+        return out
+
+    def grad(self, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        H, I = api.MLP_HIDDEN, self.n_in
+        g = {"w1": np.zeros((H, I), np.float32), "b1": np.zeros(H, np.float32), "w2": np.zeros((H, H), np.float32),
+             "b2": np.zeros(H, np.float32), "w3": np.zeros(H, np.float32)}
+        gb3 = C.c_float()
+        loss = C.c_float()
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        api.check(api.lib().ecg_trainer_grad(self.h, fp(x), fp(y), len(y), C.byref(loss), fp(g["w1"]), fp(g["b1"]),
+                                             fp(g["w2"]), fp(g["b2"]), fp(g["w3"]), C.byref(gb3)), "ecg_trainer_grad")
+        g["b3"] = gb3.value
+        return loss.value, g
+
+    def params(self):
+        m = api.Mlp()
+        api.check(api.lib().ecg_trainer_export(self.h, C.byref(m)), "ecg_trainer_export")
+        H, I = api.MLP_HIDDEN, m.n_in
+        arr = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy()
+        return {"w1": arr(m.w1, H * I).reshape(H, I), "b1": arr(m.b1, H), "w2": arr(m.w2, H * H).reshape(H, H),
+                "b2": arr(m.b2, H), "w3": arr(m.w3, H), "b3": m.b3,
+                "in_shift": np.array(m.in_shift[:I]), "in_scale": np.array(m.in_scale[:I]),
+                "out_shift": m.out_shift, "out_scale": m.out_scale}
+
+    def model(self) -> SeedModel:
+        p = self.params()
+        return make_model(p["w1"], p["b1"], p["w2"], p["b2"], p["w3"], p["b3"], p["in_shift"], p["in_scale"],
+                          p["out_shift"], p["out_scale"])
+
+    def close(self):
+        if getattr(self, "h", None):
+            api.lib().ecg_trainer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def train(x: np.ndarray, y: np.ndarray, epochs: int = 20, batch: int = 4096, lr: float = 2e-3, seed: int = 0,
+          log=None) -> Tuple[SeedModel, List[float]]:
+    """Normalise the features and the target, then fit the MLP on the GPU."""
+    shift = x.mean(axis=0)
+    scale = 1.0 / np.maximum(x.std(axis=0), 1e-6)
+    xn = ((x - shift) * scale).astype(np.float32)
+    ysh, ysc = float(y.mean()), float(max(y.std(), 1e-6))
+    yn = ((y - ysh) / ysc).astype(np.float32)
+    tr = Trainer(x.shape[1], seed=seed)
+    tr.set_norm(shift, scale, ysh, ysc)
+    rng = np.random.default_rng(seed)
+    losses = []
+    for ep in range(epochs):
+        perm = rng.permutation(len(yn))
+        l = tr.epoch(xn[perm], yn[perm], batch=batch, lr=lr * (0.5 ** (ep // max(1, epochs // 3))))
+        losses.append(l)
+        if log:
+            log(f"epoch {ep}: loss {l:.4e}")
+    m = tr.model()
+    tr.close()
+    return m, losses
