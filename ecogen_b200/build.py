@@ -23,7 +23,7 @@ DRIVER = os.path.join(HERE, "ecogen-b200")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-           "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+           "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")] + os.environ.get("ECG_NVCC_EXTRA", "").split()
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
 

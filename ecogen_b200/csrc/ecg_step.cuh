@@ -20,18 +20,28 @@
 #pragma once
 #include "ecg_device.cuh"
 
+// Minimum resident blocks per SM asked of the compiler for the step kernels (caps registers at
+// 65536 / (256 x this)): 2 -> 128 registers without spills on the 2D two-phase kernels.
+#ifndef ECG_KAPILA_MIN_BLOCKS
+#define ECG_KAPILA_MIN_BLOCKS 2
+#endif
+
 namespace ecg {
 
 enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
 
+// Cells of a block's tile and threads of the block.  Face fluxes are computed one per thread, so
+// the tiles are shaped for every axis to have at most THREADS faces ((X+1)*Y*Z, X*(Y+1)*Z,
+// X*Y*(Z+1)): each face pass then takes a single round and no warp waits at the following barrier
+// for a partial second round.
 template <int DIM>
 struct TileShape;
 template <>
-struct TileShape<1> { static constexpr int X = 256, Y = 1, Z = 1; };
+struct TileShape<1> { static constexpr int X = 255, Y = 1, Z = 1, THREADS = 256; };
 template <>
-struct TileShape<2> { static constexpr int X = 32, Y = 8, Z = 1; };
+struct TileShape<2> { static constexpr int X = 16, Y = 15, Z = 1, THREADS = 256; };
 template <>
-struct TileShape<3> { static constexpr int X = 16, Y = 4, Z = 4; };
+struct TileShape<3> { static constexpr int X = 6, Y = 6, Z = 6, THREADS = 256; };
 
 // Field indices of a state array (stride = ncells):
 //   alpha_k [0,NP), rho_k [NP,2NP), p 2NP, u_d 2NP+1+d, E 2NP+1+DIM

@@ -16,13 +16,14 @@ template <int DIM, int PASS>
 struct EulerStep {
   using TS = TileShape<DIM>;
   static constexpr int H = (PASS == PASS_O1) ? 1 : 2;
-  static constexpr int NTH = TS::X * TS::Y * TS::Z;
+  static constexpr int NTH = TS::THREADS;
+  static constexpr int NCELL = TS::X * TS::Y * TS::Z;
   static constexpr bool O2 = (PASS != PASS_O1);
   static constexpr int NQ = 3 + DIM;      // rho, p, u_d, E
   static constexpr int NSL = 2 + DIM;     // rho, p, u_d
   static constexpr int NFL = 2 + DIM;     // mass, mom_d, E
   __host__ __device__ static constexpr int ext(int a) { return a == 0 ? TS::X : (a == 1 ? TS::Y : TS::Z); }
-  __host__ __device__ static constexpr int lines(int a) { return NTH / ext(a); }
+  __host__ __device__ static constexpr int lines(int a) { return NCELL / ext(a); }
   __host__ __device__ static constexpr int rlen(int a) { return ext(a) + 2 * H; }
   __host__ __device__ static constexpr int region(int a) { return rlen(a) * lines(a); }
   __host__ __device__ static constexpr int nslope(int a) { return O2 ? (ext(a) + 3) * lines(a) : 0; }
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
   const int org[3] = {(int)blockIdx.x * TS::X, (int)blockIdx.y * TS::Y, (int)blockIdx.z * TS::Z};
   const int lc[3] = {tid % TS::X, (tid / TS::X) % TS::Y, tid / (TS::X * TS::Y)};
   const int gc[3] = {org[0] + lc[0], org[1] + lc[1], org[2] + lc[2]};
-  const bool active = gc[0] < G.n[0] && gc[1] < G.n[1] && gc[2] < G.n[2];
+  const bool active = tid < K::NCELL && gc[0] < G.n[0] && gc[1] < G.n[1] && gc[2] < G.n[2];
   const int64_t nn = P.n;
   const int64_t cell = (int64_t)gc[0] + (int64_t)gc[1] * G.n[0] + (int64_t)gc[2] * G.n[0] * G.n[1];
   double am = 0., amom[DIM], aE = 0.;

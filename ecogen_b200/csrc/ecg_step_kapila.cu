@@ -1,280 +1,11 @@
-// Kapila (PUEq) step kernels: first-order step, MUSCL predictor and MUSCL corrector.
-// See ecg_step.cuh for the work decomposition.
-#include <cuda_runtime.h>
-
-#include "ecg_kapila_cell.cuh"
+// Dispatch of the Kapila step kernels over (phases, dimension, p-T-mu) variants.
+#include "ecg_step.cuh"
 
 namespace ecg {
-
-template <int NP, int DIM, int PASS>
-struct KapilaStep {
-  using FL = Fields<NP, DIM>;
-  using TS = TileShape<DIM>;
-  static constexpr int H = (PASS == PASS_O1) ? 1 : 2;
-  static constexpr int NTH = TS::X * TS::Y * TS::Z;
-  static constexpr bool O2 = (PASS != PASS_O1);
-
-  __host__ __device__ static constexpr int ext(int a) { return a == 0 ? TS::X : (a == 1 ? TS::Y : TS::Z); }
-  __host__ __device__ static constexpr int lines(int a) { return NTH / ext(a); }
-  __host__ __device__ static constexpr int rlen(int a) { return ext(a) + 2 * H; }
-  __host__ __device__ static constexpr int region(int a) { return rlen(a) * lines(a); }
-  __host__ __device__ static constexpr int nslope(int a) { return O2 ? (ext(a) + 3) * lines(a) : 0; }
-  __host__ __device__ static constexpr int nface(int a) { return (ext(a) + 1) * lines(a); }
-  __host__ __device__ static constexpr int cmax(int a, int b) { return a > b ? a : b; }
-  __host__ __device__ static constexpr int RMAX() {
-    return cmax(region(0), cmax(DIM > 1 ? region(1) : 0, DIM > 2 ? region(2) : 0));
-  }
-  __host__ __device__ static constexpr int SMAX() {
-    return cmax(nslope(0), cmax(DIM > 1 ? nslope(1) : 0, DIM > 2 ? nslope(2) : 0));
-  }
-  __host__ __device__ static constexpr int FMAX() {
-    return cmax(nface(0), cmax(DIM > 1 ? nface(1) : 0, DIM > 2 ? nface(2) : 0));
-  }
-  static constexpr int NA0 = (PASS == PASS_CORR) ? 1 : 0;  // separate time-n alpha_0 plane
-  static constexpr size_t smem_bytes() {
-    return sizeof(double) * ((size_t)RMAX() * (FL::NQ + NA0) + (size_t)SMAX() * FL::NSL + (size_t)FMAX() * FL::NFL);
-  }
-};
-
-template <int NP, int DIM, int PASS, bool PTMU>
-__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH)
-    k_kapila_step(StepParams P, Geometry G, Model<NP> M) {
-  using K = KapilaStep<NP, DIM, PASS>;
-  using FL = Fields<NP, DIM>;
-  using TS = TileShape<DIM>;
-  extern __shared__ double smem[];
-  constexpr int RS = K::RMAX();
-  constexpr int SS = (K::SMAX() > 0) ? K::SMAX() : 1;
-  constexpr int FS = K::FMAX();
-  double* sq = smem;                                       // [NQ][RS]
-  double* sa0 = sq + (size_t)FL::NQ * RS;                  // [NA0][RS]
-  double* ssl = sa0 + (size_t)K::NA0 * RS;                 // [NSL][SS]
-  double* sfl = ssl + (K::O2 ? (size_t)FL::NSL * SS : 0);  // [NFL][FS]
-  MlpSmem* smlp = reinterpret_cast<MlpSmem*>(sfl + (size_t)FL::NFL * FS);  // present when a seed model is set
-
-  if (*P.done) return;  // stop condition reached earlier in a captured step sequence
-  const int tid = threadIdx.x;
-  const int org[3] = {(int)blockIdx.x * TS::X, (int)blockIdx.y * TS::Y, (int)blockIdx.z * TS::Z};
-  const int lc[3] = {tid % TS::X, (tid / TS::X) % TS::Y, tid / (TS::X * TS::Y)};
-  const int gc[3] = {org[0] + lc[0], org[1] + lc[1], org[2] + lc[2]};
-  const bool active = gc[0] < G.n[0] && gc[1] < G.n[1] && gc[2] < G.n[2];
-  const int64_t nn = P.n;
-  const int64_t cell = (int64_t)gc[0] + (int64_t)gc[1] * G.n[0] + (int64_t)gc[2] * G.n[0] * G.n[1];
-
-  // time-n state of the own cell: non-conservative terms and U^n
-  double an[NP], rn[NP], pn[NP];
-  double aa[NP], am[NP], ae[NP], amom[DIM], aE = 0.;
-#pragma unroll
-  for (int k = 0; k < NP; k++) {
-    an[k] = rn[k] = pn[k] = 0.;
-    aa[k] = am[k] = ae[k] = 0.;
-  }
-#pragma unroll
-  for (int d = 0; d < DIM; d++) amom[d] = 0.;
-  if (active) {
-    double p0 = P.sn[(int64_t)FL::P * nn + cell];
-#pragma unroll
-    for (int k = 0; k < NP; k++) {
-      an[k] = P.sn[(int64_t)(FL::A + k) * nn + cell];
-      rn[k] = P.sn[(int64_t)(FL::R + k) * nn + cell];
-      pn[k] = eos_fix_p(M.eos[k], p0);
-    }
-  }
-  double dtmax = 1.e10;
-  if (P.mlp != nullptr) mlp_load(smlp, P.mlp, P.mlp_nin);  // visible after the first barrier below
-
-#pragma unroll 1
-  for (int ax = 0; ax < DIM; ax++) {
-    const int T = K::ext(ax), RL = K::rlen(ax), NL = K::lines(ax);
-    const int b1 = (ax == 0) ? 1 : 0, b2 = (ax == 2) ? 1 : 2;  // the two other axes
-    const int e1 = K::ext(b1);
-    const int nax = G.n[ax];
-    // ---- stage tile + halo along ax
-    for (int e = tid; e < K::region(ax); e += K::NTH) {
-      int la = e % RL - K::H, line = e / RL;
-      int l1 = line % e1, l2 = line / e1;
-      int g[3];
-      g[ax] = org[ax] + la;
-      g[b1] = org[b1] + l1;
-      g[b2] = org[b2] + l2;
-      bool in = g[ax] >= 0 && g[ax] < nax && g[b1] < G.n[b1] && g[b2] < G.n[b2];
-      if (in) {
-        int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
-#pragma unroll
-        for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
-        if (K::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
-      }
-    }
-    __syncthreads();
-    // ---- face slopes (MUSCL): face j between local cells j-1 and j, j in [-1, T+1]
-    if (K::O2) {
-      for (int e = tid; e < K::nslope(ax); e += K::NTH) {
-        int j = e % (T + 3) - 1, line = e / (T + 3);
-        int gl = org[ax] + j - 1;
-        if (gl < 0 || gl + 1 >= nax) continue;  // not an internal face
-        int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
-        double d = G.dcc[ax][gl];
-#pragma unroll
-        for (int k = 0; k < NP; k++) {
-          ssl[k * SS + e] = (sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl]) / d;
-          ssl[(NP + k) * SS + e] = (sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl]) / d;
-          double pr = eos_fix_p(M.eos[k], sq[FL::P * RS + rr]), pl = eos_fix_p(M.eos[k], sq[FL::P * RS + rl]);
-          ssl[(2 * NP + k) * SS + e] = (pr - pl) / d;
-        }
-#pragma unroll
-        for (int dd = 0; dd < DIM; dd++)
-          ssl[(3 * NP + dd) * SS + e] = (sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl]) / d;
-      }
-      __syncthreads();
-    }
-    // ---- face fluxes: face j between local cells j-1 and j, j in [0, T]
-    for (int e = tid; e < K::nface(ax); e += K::NTH) {
-      int j = e % (T + 1), line = e / (T + 1);
-      int l1 = line % e1, l2 = line / e1;
-      int gl = org[ax] + j - 1;
-      if (gl < 0 || gl + 1 >= nax || org[b1] + l1 >= G.n[b1] || org[b2] + l2 >= G.n[b2]) continue;
-      int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
-      Thermo<NP> tl, tr;
-      double ug[3], vg[3];
-      if (!K::O2) {
-        cell_thermo<NP, DIM>(M, sq, RS, rl, tl, ug);
-        cell_thermo<NP, DIM>(M, sq, RS, rr, tr, vg);
-      } else {
-        const int fs = line * (T + 3);
-        const int f1 = fs + j + 1;                         // this face
-        const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
-        const int f2l = hasL ? fs + j : -1;                // face (j-2, j-1)
-        const int f2r = hasR ? fs + j + 2 : -1;            // face (j, j+1)
-        const double* a0 = K::NA0 ? sa0 : sq;              // time-n alpha_0 planes
-        double aL = sq[FL::A * RS + rl], aR = sq[FL::A * RS + rr];
-        double aLL = hasL ? a0[rl - 1] : 0., aRR = hasR ? a0[rr + 1] : 0.;
-        reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl, ug);
-        reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr, vg);
-      }
-      double ul[3], ur[3], Fn[3];
-      to_local(ax, false, ug, ul);
-      to_local(ax, false, vg, ur);
-      Flux<NP> F;
-      hllc<NP>(M, tl, ul, tr, ur, G.lcfl, G.lcfl, dtmax, Fn, F);
-      to_global(ax, false, Fn, F.mom);
-#pragma unroll
-      for (int k = 0; k < NP; k++) {
-        sfl[k * FS + e] = F.a[k];
-        sfl[(NP + k) * FS + e] = F.m[k];
-        sfl[(2 * NP + k) * FS + e] = F.en[k];
-      }
-#pragma unroll
-      for (int d = 0; d < DIM; d++) sfl[(3 * NP + d) * FS + e] = F.mom[d];
-      sfl[(3 * NP + DIM) * FS + e] = F.E;
-      sfl[(3 * NP + DIM + 1) * FS + e] = F.sM;
-      sfl[(3 * NP + DIM + 2) * FS + e] = F.uStar;
-    }
-    __syncthreads();
-    // ---- accumulate the two faces of this axis into the own cell (left +, right -)
-    if (active) {
-      int la = lc[ax];
-      int line = lc[b1] + lc[b2] * e1;
-      const double cA = G.coefA[ax];
-#pragma unroll
-      for (int side = 0; side < 2; side++) {
-        int j = la + side;
-        int gl = org[ax] + j - 1;
-        if (gl < 0 || gl + 1 >= nax) continue;  // boundary face: handled below
-        int e = line * (T + 1) + j;
-        Flux<NP> F;
-#pragma unroll
-        for (int k = 0; k < NP; k++) {
-          F.a[k] = sfl[k * FS + e];
-          F.m[k] = sfl[(NP + k) * FS + e];
-          F.en[k] = sfl[(2 * NP + k) * FS + e];
-        }
-#pragma unroll
-        for (int d = 0; d < DIM; d++) F.mom[d] = sfl[(3 * NP + d) * FS + e];
-        F.E = sfl[(3 * NP + DIM) * FS + e];
-        F.sM = sfl[(3 * NP + DIM + 1) * FS + e];
-        F.uStar = sfl[(3 * NP + DIM + 2) * FS + e];
-        acc_face<NP, DIM>(cA, side == 0, F, an, pn, aa, am, ae, amom, aE);
-      }
-    }
-    __syncthreads();
-  }
-
-  // per-thread counters, reduced per block at the end
-  CellCounters cc;
-  CellPrim<NP, DIM> cp;
-  if (active) {
-    // ---- boundary faces (non-reflecting: HLLC(cell, cell), BoundCondNonReflecting::solveRiemannBoundary
-    //      src/BoundConds/BoundCondNonReflecting.cpp:62), subtracted from the cell (BoundCond::computeFlux :61)
-#pragma unroll 1
-    for (int bf = 0; bf < 2 * DIM; bf++) {
-      int ax = bf >> 1;
-      bool neg = (bf & 1) == 0;
-      if (neg ? (gc[ax] != 0) : (gc[ax] != G.n[ax] - 1)) continue;
-      boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE);
-    }
-
-    kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
-  }
-  // learned seed of the pressure relaxation: one warp-wide tensor-core evaluation (all lanes)
-  double seed = 0.;
-  if (P.mlp != nullptr) seed = mlp_seed_warp<NP>(smlp, active, cp.a, cp.r, cp.pk);
-  if (active) kapila_finish<NP, DIM, PASS, PTMU>(P, M, nn, cell, cp, seed, P.mlp != nullptr, cc);
-  block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
-
-  // ---- dtMax: block min, one atomic per block
-  __shared__ double red[32];
-  double v = dtmax;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((tid & 31) == 0) red[tid >> 5] = v;
-  __syncthreads();
-  if (tid < 32) {
-    v = (tid < K::NTH / 32) ? red[tid] : 1.e10;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (tid == 0) atomic_min_pos_double(P.dtmax_bits, v);
-  }
-}
-
-}  // namespace ecg
-
-// ------------------------------------------------------------------------------- host launchers
-namespace ecg {
-
-template <int NP, int DIM, int PASS, bool PTMU>
-static cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps, cudaStream_t s,
-                              bool prepare) {
-  using K = KapilaStep<NP, DIM, PASS>;
-  using TS = TileShape<DIM>;
-  auto kern = k_kapila_step<NP, DIM, PASS, PTMU>;
-  const size_t sm = K::smem_bytes() + (P.mlp != nullptr ? sizeof(MlpSmem) : 0);
-  if (prepare)
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(K::smem_bytes() + sizeof(MlpSmem)));
-  Model<NP> M;
-  for (int k = 0; k < NP; k++) {
-    M.eos[k].type = eos[k].type;
-    M.eos[k].gamma = eos[k].gamma;
-    M.eos[k].pinf = eos[k].pinf;
-    M.eos[k].b = eos[k].b;
-    M.eos[k].cv = eos[k].cv;
-    M.eos[k].eref = eos[k].eref;
-    M.eos[k].sref = eos[k].sref;
-  }
-  M.eps = eps;
-  dim3 grid((G.n[0] + TS::X - 1) / TS::X, (G.n[1] + TS::Y - 1) / TS::Y, (G.n[2] + TS::Z - 1) / TS::Z);
-  kern<<<grid, K::NTH, sm, s>>>(P, G, M);
-  return cudaGetLastError();
-}
 
 template <int NP, int DIM, bool PTMU>
-static cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
-                               cudaStream_t s, bool prepare) {
-  switch (pass) {
-    case PASS_O1: return launch_one<NP, DIM, PASS_O1, PTMU>(P, G, eos, eps, s, prepare);
-    case PASS_PRED: return launch_one<NP, DIM, PASS_PRED, PTMU>(P, G, eos, eps, s, prepare);
-    default: return launch_one<NP, DIM, PASS_CORR, PTMU>(P, G, eos, eps, s, prepare);
-  }
-}
+cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
+                        cudaStream_t s, bool prepare);
 
 // Launches (or, with prepare, configures) one pass of the Kapila step for a case shape.
 cudaError_t kapila_launch(int np, int dim, bool ptmu, int pass, const StepParams& P, const Geometry& G,
@@ -295,18 +26,6 @@ cudaError_t kapila_launch(int np, int dim, bool ptmu, int pass, const StepParams
     return launch_pass<3, 3, false>(pass, P, G, eos, eps, s, prepare);
   }
   return cudaErrorNotSupported;
-}
-
-size_t kapila_smem_bytes(int np, int dim, int pass) {
-#define ECG_SM(NPV, DV)                                                         \
-  if (np == NPV && dim == DV) {                                                 \
-    if (pass == PASS_O1) return KapilaStep<NPV, DV, PASS_O1>::smem_bytes();     \
-    if (pass == PASS_PRED) return KapilaStep<NPV, DV, PASS_PRED>::smem_bytes(); \
-    return KapilaStep<NPV, DV, PASS_CORR>::smem_bytes();                        \
-  }
-  ECG_SM(2, 1) ECG_SM(2, 2) ECG_SM(2, 3) ECG_SM(3, 1) ECG_SM(3, 2) ECG_SM(3, 3)
-#undef ECG_SM
-  return 0;
 }
 
 }  // namespace ecg
