@@ -97,6 +97,7 @@ def lib():
     L.ecg_step.argtypes = [vp, C.c_int32, dp, dp, P(StepStats)]
     L.ecg_run.argtypes = [vp, dp, dp, P(C.c_int32), P(StepStats)]
     L.ecg_step_profiled.argtypes = [vp, C.c_int32, dp, dp, P(StepStats), dp]
+    L.ecg_step_noalloc.argtypes = [P(Case), vp, vp, C.c_double, dp, P(StepStats), vp]
     L.ecg_ncells.restype = C.c_int64
     L.ecg_ncells.argtypes = [vp]
     L.ecg_stream.restype = vp

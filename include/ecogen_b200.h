@@ -144,6 +144,27 @@ ecg_status ecg_set_newton_cap(ecg_ctx* ctx, int32_t cap);
 ecg_status ecg_upload_prim_device(ecg_ctx* ctx, const double* const* dfields, int64_t ncells);
 ecg_status ecg_download_prim_device(ecg_ctx* ctx, double* const* dfields, int64_t ncells);
 
+/* One time step on device buffers the caller owns, allocating no device memory.  This entry point
+ * has no counterpart in the reference (whose CPU run loop owns its memory): it is for callers that
+ * cannot call cudaMalloc, e.g. codes whose device memory all comes from their own allocator or pool,
+ * or that must not allocate inside their time loop.  Instead of a context it uses one fixed
+ * __device__ scratch array of the library (about 10 MB per GPU that loads the library, held until
+ * the process exits) for the MUSCL half-step state, distance tables, dt scalars and counters.
+ *   - At most ECG_NOALLOC_MAX_CELLS cells; larger cases return ECG_ERR_TOO_LARGE.
+ *   - state_in / state_out: device arrays in the library's device layout, fields of ncells doubles
+ *     back to back: alpha_0..alpha_{N-1}, rho_0..rho_{N-1}, p, u_0..u_{dim-1}, E (Kapila) or
+ *     rho, p, u_0..u_{dim-1}, E (Euler), where dim counts the axes with more than one cell; this is
+ *     what ecg_upload_prim stores.  They must not alias.
+ *   - dt: the step to take; *dt_next (optional) receives cfl * dtMax.  stats may be NULL.
+ *   - stream: a cudaStream_t (NULL = legacy default stream); the call returns after the step ran.
+ *   - The first call on a device looks up the scratch's device address; make it before any stream
+ *     capture.  All calls share the scratch and the last call's contents stay in it; every call
+ *     re-initialises what must start at zero.  Calls that overlap on the GPU (other streams, other
+ *     host threads) race on the scratch and must be serialised by the caller. */
+#define ECG_NOALLOC_MAX_CELLS 65536
+ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in, double* state_out, double dt, double* dt_next,
+                            ecg_step_stats* stats, void* stream);
+
 /* ------------------------------------------------------------------ learned relaxation seed */
 /* A 9 -> 64 -> 64 -> 1 (or nin -> h -> h -> 1) GELU MLP whose output seeds the pressure-relaxation
  * Newton iteration (RelaxationP::NewtonRaphson start, src/Relaxations/RelaxationPInfinite.cpp:58-63).
