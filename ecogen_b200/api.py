@@ -12,7 +12,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libecg.so")
+LIB_PATH = os.environ.get("ECG_LIB", os.path.join(HERE, "libecg.so"))
 
 ECG_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported case", 3: "CUDA error", 4: "case input error",

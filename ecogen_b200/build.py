@@ -17,8 +17,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libecg.so")
+BUILD = os.environ.get("ECG_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("ECG_LIB_OUT", os.path.join(HERE, "libecg.so"))
 DRIVER = os.path.join(HERE, "ecogen-b200")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

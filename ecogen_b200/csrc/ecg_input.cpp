@@ -34,6 +34,8 @@ struct StateIC {
 
 struct ecg_input {
   ecg_case c;
+  int iter_freq = 0;
+  double time_freq = 0.;
   std::string run_name;
   std::string output_format;
   std::vector<std::string> eos_names;
@@ -139,10 +141,12 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
     const Node* it = tc->child("iterations");
     int nb = 0;
     if (!it || !it->get_int("number", &nb)) return bail(ECG_ERR_XML, "main.xml: <iterations number> missing");
+    if (!it->get_int("iterFreq", &in->iter_freq)) return bail(ECG_ERR_XML, "main.xml: <iterations iterFreq> missing");
     c.max_iterations = nb;
   } else {
     const Node* pt = tc->child("physicalTime");
     if (!pt || !pt->get_double("totalTime", &c.total_time)) return bail(ECG_ERR_XML, "main.xml: <physicalTime totalTime> missing");
+    if (!pt->get_double("timeFreq", &in->time_freq)) return bail(ECG_ERR_XML, "main.xml: <physicalTime timeFreq> missing");
   }
   const Node* cc = mainx->child("computationControl");
   if (!cc || !cc->get_double("CFL", &c.cfl)) return bail(ECG_ERR_XML, "main.xml: <computationControl CFL> missing");
@@ -422,6 +426,18 @@ extern "C" ecg_status ecg_input_case(const ecg_input* in, ecg_case* out) {
 }
 
 extern "C" const char* ecg_input_run_name(const ecg_input* in) { return in ? in->run_name.c_str() : ""; }
+
+extern "C" ecg_status ecg_input_print_control(const ecg_input* in, int32_t* iter_freq, double* time_freq) {
+  if (!in) return fail(ECG_ERR_INVALID, "null input");
+  if (iter_freq) *iter_freq = in->iter_freq;
+  if (time_freq) *time_freq = in->time_freq;
+  return ECG_OK;
+}
+
+extern "C" const char* ecg_input_eos_name(const ecg_input* in, int32_t k) {
+  if (!in || k < 0 || k >= (int)in->eos_names.size()) return "";
+  return in->eos_names[k].c_str();
+}
 
 namespace {
 

@@ -104,6 +104,10 @@ void ecg_input_free(ecg_input* in);
 ecg_status ecg_input_case(const ecg_input* in, ecg_case* out);
 /* Run name (main.xml <run>) and output format; strings are owned by the input. */
 const char* ecg_input_run_name(const ecg_input* in);
+/* Print control of main.xml: iterFreq (iteration mode) or timeFreq (physical-time mode). */
+ecg_status ecg_input_print_control(const ecg_input* in, int32_t* iter_freq, double* time_freq);
+/* EOS file name of phase k (model.xml <EOS name>), used for output field names. */
+const char* ecg_input_eos_name(const ecg_input* in, int32_t k);
 /* Fills the initial primitive fields on the host, domain by domain in document order
  * (GeometricalDomain::fillIn src/Geometries/GeometricalDomain.cpp:64).  Field layout as above. */
 ecg_status ecg_input_fill(const ecg_input* in, double* const* fields, int64_t ncells);

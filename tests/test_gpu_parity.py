@@ -79,3 +79,29 @@ def test_newton_stats_match_oracle(tmp_path):
     assert out["stats"]["relax_calls"] == sim.stats.relax_calls
     assert out["stats"]["newton_evals"] == sim.stats.newton_evals
     assert sum(out["stats"]["newton_hist"]) == sim.stats.relax_calls
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "euler1d_o2"])
+def test_driver_writes_reference_results(key, golden_cases, tmp_path):
+    """ecogen-b200 <work> runs ECOGEN.xml's cases and writes reference-format VTK results."""
+    import subprocess
+    import os
+    from ecogen_b200 import cases
+    from oracle import refrun
+    from tests.helpers import ROOT
+    meta, g = load_golden(key)
+    case = golden_cases[key]
+    d = case.write(str(tmp_path))
+    cases.write_ecogen_list(str(tmp_path), [d])
+    exe = os.path.join(ROOT, "ecogen_b200", "ecogen-b200")
+    r = subprocess.run([exe, str(tmp_path) + "/"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    files = refrun.result_files(str(tmp_path), case.name)
+    assert len(files) >= 2
+    got = refrun.reference_prim(refrun.read_vtr(files[-1]), case.nphases)
+    for name in ("alpha", "rho", "p", "u", "E"):
+        ref = g.get("final_" + name)
+        if ref is None or got.get(name) is None:
+            continue
+        assert rel_l1(got[name], ref) <= TOL, name
