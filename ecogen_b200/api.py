@@ -19,6 +19,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported case", 3: "CUDA error"
           5: "physics check failed", 6: "out of memory", 7: "size above the stated maximum", 8: "device wait timed out"}
 MODEL_KAPILA, MODEL_EULER = 0, 1
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
+BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
 
 
@@ -38,7 +39,7 @@ class Case(C.Structure):
                 ("limiter", C.c_int32 * 4), ("ncells", C.c_int32 * 3), ("length", C.c_double * 3),
                 ("cfl", C.c_double), ("time_iterations", C.c_int32), ("max_iterations", C.c_int32),
                 ("total_time", C.c_double), ("ptmu", C.c_int32), ("ptmu_liquid", C.c_int32),
-                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3)]
+                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6)]
 
 
 class StepStats(C.Structure):
@@ -130,6 +131,8 @@ def lib():
     L.ecg_batch_autotune.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
     L.ecg_batch_total_cells.restype = C.c_int64
     L.ecg_batch_total_cells.argtypes = [vp]
+    L.ecg_batch_stream.restype = vp
+    L.ecg_batch_stream.argtypes = [vp]
     _lib = L
     return L
 
@@ -175,6 +178,8 @@ def case_from_spec(spec) -> Case:
         c.ptmu, c.ptmu_liquid, c.ptmu_vapor = 1, spec.ptmu[0], spec.ptmu[1]
     for k, e in enumerate(spec.eos):
         c.eos[k] = Eos(EOS_CODE[e.kind], e.gamma, e.pinf, e.b, e.cv, e.eref, e.sref)
+    for i, b in enumerate(spec.boundary_types()):
+        c.bc[i] = BC_CODE[b.upper()]
     return c
 
 

@@ -152,9 +152,15 @@ class Case:
     vf_limiter: Optional[str] = None
     interface_vf_limiter: Optional[str] = None
     ptmu: Optional[Tuple[int, int]] = None  # (liquid phase, vapour phase)
+    boundaries: Optional[List[str]] = None  # boundCond types Xm, Xp, Ym, Yp, Zm, Zp (default nonReflecting)
     output_format: str = "XML"
     output_binary: bool = True
     extra: Dict[str, object] = field(default_factory=dict)
+
+    def boundary_types(self) -> List[str]:
+        """boundCond type of each side Xm, Xp, Ym, Yp, Zm, Zp (sides of unused axes included)."""
+        b = list(self.boundaries or [])
+        return b + ["nonReflecting"] * (6 - len(b))
 
     @property
     def ncells(self) -> int:
@@ -224,9 +230,9 @@ class Case:
             s += "    " + d.xml() + "\n"
         s += "  </physicalDomains>\n  <boundaryConditions>\n"
         names = ["CLXm", "CLXp", "CLYm", "CLYp", "CLZm", "CLZp"]
-        nb = 2 * self.dim
-        for i in range(nb):
-            s += f'    <boundCond name="{names[i]}" type="nonReflecting" number="{i + 1}"/>\n'
+        types = self.boundary_types()
+        for i in range(2 * self.dim):
+            s += f'    <boundCond name="{names[i]}" type="{types[i]}" number="{i + 1}"/>\n'
         s += "  </boundaryConditions>\n"
         euler = self.model.upper() == "EULER"
         for st in self.states:

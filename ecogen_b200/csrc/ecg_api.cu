@@ -134,6 +134,8 @@ ecg_status validate_case(const ecg_case* c) {
     set_error("THINC volume-fraction reconstruction is not supported");
     return ECG_ERR_UNSUPPORTED;
   }
+  for (int i = 0; i < 6; i++)
+    if (c->bc[i] != ECG_BC_NONREFLECTING && c->bc[i] != ECG_BC_SYMMETRY) { set_error("bad boundary condition"); return ECG_ERR_INVALID; }
   if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
   int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
   if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
@@ -341,6 +343,7 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
     x->geo.dfr[a] = x->dist + (size_t)(3 * a + 2) * nmax;
   }
   x->geo.dim = x->dim;
+  side_geometry(*c, x->geo);
   // MeshCartesian::initializeGeometrieMonoCpu :228-236 and face surfaces :287, :320, :353
   double dX = c->length[0] / (double)c->ncells[0], dY = c->length[1] / (double)c->ncells[1],
          dZ = c->length[2] / (double)c->ncells[2];

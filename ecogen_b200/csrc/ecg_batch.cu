@@ -251,7 +251,7 @@ static cudaError_t batch_one(const BatchParams& B, const ecg_eos* eos, double ep
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks, kern, TB, base + sizeof(MlpSmem));
   }
   Model<NP> M;
-  for (int k = 0; k < NP; k++) M.eos[k] = {eos[k].type, eos[k].gamma, eos[k].pinf, eos[k].b, eos[k].cv, eos[k].eref, eos[k].sref};
+  for (int k = 0; k < NP; k++) M.eos[k] = make_eos_params(eos[k]);
   M.eps = eps;
   kern<<<grid, TB, sm, s>>>(B, M);
   return cudaGetLastError();
@@ -449,6 +449,10 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
       set_error("batched mode runs 1D cases");
       return ECG_ERR_UNSUPPORTED;
     }
+    if (x.bc[0] != ECG_BC_NONREFLECTING || x.bc[1] != ECG_BC_NONREFLECTING) {
+      set_error("batched mode runs non-reflecting sides only");
+      return ECG_ERR_UNSUPPORTED;
+    }
     if (x.model != c0.model || x.nphases != c0.nphases || x.order != c0.order || x.alpha_null != c0.alpha_null ||
         std::memcmp(x.limiter, c0.limiter, sizeof(x.limiter)) != 0 || std::memcmp(x.eos, c0.eos, sizeof(x.eos)) != 0) {
       set_error("all cases of a batch share model, phases, EOS, order, limiters and alphaNull");
@@ -545,6 +549,7 @@ extern "C" void ecg_batch_destroy(ecg_batch* b) {
 }
 
 extern "C" int64_t ecg_batch_total_cells(const ecg_batch* b) { return b ? b->total : 0; }
+extern "C" void* ecg_batch_stream(const ecg_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 extern "C" ecg_status ecg_batch_upload_prim(ecg_batch* b, const double* const* f, int64_t total) {
   if (!b || !f || total != b->total) {

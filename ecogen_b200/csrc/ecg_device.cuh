@@ -124,20 +124,20 @@ __device__ __forceinline__ void phase_fix_ar(double eps, double& a, double& r) {
 // Thermodynamic closure of one side of a face or of a cell: what fulfillState computes
 // (ModUEq::fulfillState src/Models/UEq/ModUEq.cpp:99 -> PhaseUEq::extendedCalculusPhase :97,
 // MixUEq::computeMixtureVariables src/Models/UEq/MixUEq.cpp:136).
+// The phase internal energies e_k and the mixture energy sum_k Y_k e_k are needed only on the side
+// the HLLC solution is sampled from, so hllc() evaluates them once the side is known
+// (hllc_side_energy); the values are the ones fulfillState would have produced.
 template <int NP>
 struct Thermo {
-  double a[NP], r[NP], p[NP], e[NP];
-  double rho, pm, cF, em;
+  double a[NP], r[NP], p[NP], Y[NP];
+  double rho, pm, cF;
 };
 
 template <int NP>
 __device__ __forceinline__ void fulfill(const Model<NP>& M, Thermo<NP>& t) {
   double c[NP];
 #pragma unroll
-  for (int k = 0; k < NP; k++) {
-    t.e[k] = eos_e(M.eos[k], M.eps, t.r[k], t.p[k]);
-    c[k] = eos_c(M.eos[k], M.eps, t.r[k], t.p[k]);
-  }
+  for (int k = 0; k < NP; k++) c[k] = eos_c(M.eos[k], M.eps, t.r[k], t.p[k]);
   t.rho = 0.;
   t.pm = 0.;
 #pragma unroll
@@ -145,15 +145,25 @@ __device__ __forceinline__ void fulfill(const Model<NP>& M, Thermo<NP>& t) {
     t.rho += t.a[k] * t.r[k];
     t.pm += t.a[k] * t.p[k];
   }
-  double em = 0., cF = 0.;
+  double cF = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
-    double Y = t.a[k] * t.r[k] / dmax(t.rho, M.eps);
-    em += Y * t.e[k];
-    cF += Y * c[k] * c[k];
+    t.Y[k] = t.a[k] * t.r[k] / dmax(t.rho, M.eps);
+    cF += t.Y[k] * c[k] * c[k];
   }
-  t.em = em;
   t.cF = sqrt(cF);
+}
+
+// PhaseUEq::extendedCalculusPhase energies and MixUEq::computeMixtureVariables' e = sum_k Y_k e_k.
+template <int NP>
+__device__ __forceinline__ double side_energy(const Model<NP>& M, const Thermo<NP>& t, double e[NP]) {
+  double em = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    e[k] = eos_e(M.eos[k], M.eps, t.r[k], t.p[k]);
+    em += t.Y[k] * e[k];
+  }
+  return em;
 }
 
 // Face-frame projection of a Cartesian face (src/Maths/Coord.cpp:133-151 with the frames of
@@ -213,13 +223,15 @@ __device__ __forceinline__ void hllc(const Model<NP>& M, const Thermo<NP>& L, co
     const Thermo<NP>& S = left ? L : R;
     const double* us = left ? ul : ur;
     double un = us[0], rhoS = S.rho, pS = S.pm;
+    double e[NP];
+    const double em = side_energy<NP>(M, S, e);
 #pragma unroll
     for (int k = 0; k < NP; k++) {
       F.a[k] = S.a[k] * sM;
       F.m[k] = S.a[k] * S.r[k] * un;
-      F.en[k] = S.a[k] * S.r[k] * S.e[k] * un;
+      F.en[k] = S.a[k] * S.r[k] * e[k] * un;
     }
-    double Et = S.em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
+    double Et = em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
     Fn[0] = rhoS * un * un + pS;
     Fn[1] = rhoS * us[1] * un;
     Fn[2] = rhoS * us[2] * un;
@@ -232,7 +244,9 @@ __device__ __forceinline__ void hllc(const Model<NP>& M, const Thermo<NP>& L, co
     double sK = left ? sL : sR;
     double mK = left ? mL : mR;
     double uK = us[0], pK = S.pm;
-    double Et = S.em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
+    double e[NP];
+    const double em = side_energy<NP>(M, S, e);
+    double Et = em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
     double rhoStar = mK / (sK - sM);
     double EStar = Et + (sM - uK) * (sM + pK / mK);
     double pStar = mK * (sM - uK) + pK;
@@ -596,8 +610,7 @@ __device__ __forceinline__ double correction_pressure(const Model<NP>& M, const 
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     const EosParams& q = M.eos[k];
-    double gpi = (q.type == ECG_EOS_IG) ? 0. : q.gamma * q.pinf / (q.gamma - 1.);
-    double ig = 1. / (q.gamma - 1.);
+    const double gpi = q.gpi, ig = q.ig;  // sendSpecialMixtureEos constants, computed on the host
     double cov = (q.type == ECG_EOS_NASG) ? q.b : 0.;
     pp -= a[k] * (gpi * (1. - r[k] * cov) + r[k] * q.eref);
     denom += a[k] * ig * (1. - r[k] * cov);

@@ -406,12 +406,23 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   if (in->domains.empty()) return bail(ECG_ERR_XML, "initialConditions.xml: no domain");
   const Node* bcs = icx->child("boundaryConditions");
   if (!bcs) return bail(ECG_ERR_XML, "initialConditions.xml: <boundaryConditions> missing");
+  // The i-th <boundCond> in reading order is side i (Xm, Xp, Ym, Yp, Zm, Zp), whatever its "number"
+  // (Input::readInputXML src/InputOutput/Input.cpp:1120-1190, MeshCartesian::assignLimits
+  // src/Meshes/MeshCartesian.cpp:86); sides without one are non-reflecting.  Without viscosity
+  // (out of scope here) a "wall" is a symmetry side.
+  int side = 0;
   for (const Node* b : bcs->all("boundCond")) {
     int num = 0;
     if (b->attr("name").empty() || b->attr("type").empty() || !b->get_int("number", &num))
       return bail(ECG_ERR_XML, "boundCond name/type/number missing");
-    if (upper(b->attr("type")) != "NONREFLECTING")
-      return bail(ECG_ERR_UNSUPPORTED, "boundary condition " + b->attr("type") + " is not supported (nonReflecting)");
+    if (side >= 6) return bail(ECG_ERR_XML, "more than six boundCond");
+    std::string t = upper(b->attr("type"));
+    if (t == "NONREFLECTING") in->c.bc[side] = ECG_BC_NONREFLECTING;
+    else if (t == "SYMMETRY" || t == "WALL") in->c.bc[side] = ECG_BC_SYMMETRY;
+    else
+      return bail(ECG_ERR_UNSUPPORTED,
+                  "boundary condition " + b->attr("type") + " is not supported (nonReflecting, symmetry, wall)");
+    side++;
   }
   *out = in;
   return ECG_OK;

@@ -144,6 +144,65 @@ __device__ __forceinline__ void boundary_face(const Model<NP>& M, const double* 
   acc_face<NP, DIM>(coefA, false, F, an, pn, aa, am, ae, amom, aE);
 }
 
+// Buffer cell of a symmetry side in a MUSCL pass (BoundCondWallO2Cartesian::solveRiemann
+// src/BoundConds/BoundCondWallO2Cartesian.cpp:111-141 with CellO2Cartesian::computeLocalSlopesLimite
+// src/Order2/CellO2Cartesian.cpp:173-272): slope 1 is the side's own slope (fw), slope 2 the slope of the
+// internal face on the opposite side (fo); the interface detector only tests the cell's time-n alpha;
+// the state is extrapolated by slope * dist (dist signed) without the clamps of the internal faces.
+template <int NP, int DIM>
+__device__ __forceinline__ void wall_side(const Model<NP>& M, const int lim[4], const double* sq, int RS, int rc,
+                                          const double* ssl, int SS, int fw, int fo, double alphaN, double dist,
+                                          Thermo<NP>& t, double u[3]) {
+  using FL = Fields<NP, DIM>;
+  const bool iface = (alphaN >= 1.e-4) && (alphaN <= 1. - 1.e-4);
+  const int lg = iface ? lim[1] : lim[0];
+  const int lv = iface ? lim[3] : lim[2];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double la = limiter(lv, ssl[k * SS + fw], ssl[k * SS + fo]);
+    double lr = limiter(lg, ssl[(NP + k) * SS + fw], ssl[(NP + k) * SS + fo]);
+    double lp = limiter(lg, ssl[(2 * NP + k) * SS + fw], ssl[(2 * NP + k) * SS + fo]);
+    t.a[k] = sq[(FL::A + k) * RS + rc] + la * dist;
+    t.r[k] = sq[(FL::R + k) * RS + rc] + lr * dist;
+    t.p[k] = eos_fix_p(M.eos[k], sq[FL::P * RS + rc]) + lp * dist;
+  }
+  u[0] = u[1] = u[2] = 0.;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    double l = limiter(lg, ssl[(3 * NP + d) * SS + fw], ssl[(3 * NP + d) * SS + fo]);
+    u[d] = sq[(FL::U + d) * RS + rc] + l * dist;
+  }
+  fulfill<NP>(M, t);
+}
+
+// Symmetry side (also an inviscid wall): ModUEq::solveRiemannWall src/Models/UEq/ModUEq.cpp:452-492 on the
+// fulfilled buffer cell t with face-frame velocity ul.  Returns the normal momentum flux pStar; every other
+// flux component, sM and uStar are zero.
+template <int NP>
+__device__ __forceinline__ double wall_pstar(const Thermo<NP>& t, const double ul[3], double lcfl, double& dtmax) {
+  const double uL = ul[0], cL = t.cF, pL = t.pm, rhoL = t.rho;
+  const double sL = dmin(uL - cL, -uL - cL);
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * lcfl / fabs(sL));
+  return rhoL * (uL - sL) * uL + pL;
+}
+
+// Subtracts a symmetry side's flux (zero but for the normal momentum pStar) from the cell
+// (BoundCond::computeFlux src/BoundConds/BoundCond.cpp:61).
+template <int NP, int DIM>
+__device__ __forceinline__ void wall_acc(int ax, bool neg, double pstar, double coefA, const double an[NP],
+                                         const double pn[NP], double aa[NP], double am[NP], double ae[NP],
+                                         double amom[DIM], double& aE) {
+  Flux<NP> F;
+#pragma unroll
+  for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
+  F.E = 0.;
+  F.sM = 0.;
+  F.uStar = 0.;
+  const double Fn[3] = {pstar, 0., 0.};
+  to_global(ax, neg, Fn, F.mom);
+  acc_face<NP, DIM>(coefA, false, F, an, pn, aa, am, ae, amom, aE);
+}
+
 // State of a cell after buildPrim, handed from kapila_rebuild to kapila_finish (the learned seed, when
 // installed, is evaluated between the two by the whole warp).
 template <int NP, int DIM>

@@ -39,7 +39,7 @@ struct KapilaStep {
 };
 
 template <int NP, int DIM, int PASS, bool PTMU, bool SEED>
-__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN_BLOCKS)
+__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>::MINB)
     k_kapila_step(StepParams P, Geometry G, Model<NP> M) {
   using K = KapilaStep<NP, DIM, PASS>;
   using FL = Fields<NP, DIM>;
@@ -83,6 +83,9 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN
     }
   }
   double dtmax = 1.e10;
+  double wallp[DIM];  // normal momentum flux of the cell's symmetry sides, per axis
+#pragma unroll
+  for (int d = 0; d < DIM; d++) wallp[d] = 0.;
   if (SEED) mlp_load(smlp, P.mlp, P.mlp_nin);  // visible after the first barrier below
 
 #pragma unroll
@@ -113,8 +116,19 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN
       for (int e = tid; e < K::nslope(ax); e += K::NTH) {
         int j = e % (T + 3) - 1, line = e / (T + 3);
         int gl = org[ax] + j - 1;
-        if (gl < 0 || gl + 1 >= nax) continue;  // not an internal face
         int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
+        if (gl < 0 || gl + 1 >= nax) {
+          // a side of the domain: slopes only on a symmetry side, the velocity along the axis over the
+          // centre-to-face coordinate (BoundCondWallO2Cartesian::computeSlopes :84-108)
+          const int sd = (gl == -1) ? 0 : ((gl == nax - 1) ? 1 : -1);
+          if (sd < 0 || G.bc[2 * ax + sd] != ECG_BC_SYMMETRY) continue;
+          if (org[b1] + line % e1 >= G.n[b1] || org[b2] + line / e1 >= G.n[b2]) continue;
+#pragma unroll
+          for (int f = 0; f < FL::NSL; f++) ssl[f * SS + e] = 0.;
+          const double wd = G.wslope[2 * ax + sd];
+          if (fabs(wd) > 1.e-8) ssl[(3 * NP + ax) * SS + e] = sq[(FL::U + ax) * RS + (sd ? rl : rr)] / wd;
+          continue;
+        }
         double d = G.dcc[ax][gl];
 #pragma unroll
         for (int k = 0; k < NP; k++) {
@@ -145,11 +159,16 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN
         const int fs = line * (T + 3);
         const int f1 = fs + j + 1;                         // this face
         const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
-        const int f2l = hasL ? fs + j : -1;                // face (j-2, j-1)
-        const int f2r = hasR ? fs + j + 2 : -1;            // face (j, j+1)
+        // beyond a symmetry side the opposite slope is the side's and alphaCellAfterOppositeSide is
+        // the cell's own time-n alpha (CellO2Cartesian::computeLocalSlopes :68-71); a non-reflecting
+        // side has neither
+        const bool wL = !hasL && G.bc[2 * ax] == ECG_BC_SYMMETRY;
+        const bool wR = !hasR && G.bc[2 * ax + 1] == ECG_BC_SYMMETRY;
+        const int f2l = (hasL || wL) ? fs + j : -1;        // face (j-2, j-1)
+        const int f2r = (hasR || wR) ? fs + j + 2 : -1;    // face (j, j+1)
         const double* a0 = K::NA0 ? sa0 : sq;              // time-n alpha_0 planes
         double aL = sq[FL::A * RS + rl], aR = sq[FL::A * RS + rr];
-        double aLL = hasL ? a0[rl - 1] : 0., aRR = hasR ? a0[rr + 1] : 0.;
+        double aLL = hasL ? a0[rl - 1] : (wL ? a0[rl] : 0.), aRR = hasR ? a0[rr + 1] : (wR ? a0[rr] : 0.);
         reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl, ug);
         reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr, vg);
       }
@@ -197,6 +216,23 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN
         F.uStar = sfl[(3 * NP + DIM + 2) * FS + e];
         acc_face<NP, DIM>(cA, side == 0, F, an, pn, aa, am, ae, amom, aE);
       }
+      // a symmetry side of this cell along ax: its flux is computed now, while the slopes of this axis
+      // are staged, and subtracted with the other boundary faces below (reference face order)
+      const int sd = (gc[ax] == 0) ? 0 : ((gc[ax] == nax - 1) ? 1 : -1);
+      if (sd >= 0 && G.bc[2 * ax + sd] == ECG_BC_SYMMETRY) {
+        const int rc = line * RL + la + K::H;
+        Thermo<NP> t;
+        double ug[3], ul[3];
+        if (K::O2) {
+          const int fs = line * (T + 3);
+          wall_side<NP, DIM>(M, P.lim, sq, RS, rc, ssl, SS, fs + la + 1 + sd, fs + la + 2 - sd, an[0],
+                             G.wdist[2 * ax + sd], t, ug);
+        } else {
+          cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
+        }
+        to_local(ax, sd == 0, ug, ul);
+        wallp[ax] = wall_pstar<NP>(t, ul, G.lcfl, dtmax);
+      }
     }
     __syncthreads();
   }
@@ -206,13 +242,17 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, ECG_KAPILA_MIN
   CellPrim<NP, DIM> cp;
   if (active) {
     // ---- boundary faces (non-reflecting: HLLC(cell, cell), BoundCondNonReflecting::solveRiemannBoundary
-    //      src/BoundConds/BoundCondNonReflecting.cpp:62), subtracted from the cell (BoundCond::computeFlux :61)
+    //      src/BoundConds/BoundCondNonReflecting.cpp:62; symmetry: the flux computed in the axis pass),
+    //      subtracted from the cell (BoundCond::computeFlux :61)
 #pragma unroll
     for (int bf = 0; bf < 2 * DIM; bf++) {
       int ax = bf >> 1;
       bool neg = (bf & 1) == 0;
       if (neg ? (gc[ax] != 0) : (gc[ax] != G.n[ax] - 1)) continue;
-      boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE);
+      if (G.bc[bf] == ECG_BC_SYMMETRY)
+        wall_acc<NP, DIM>(ax, neg, wallp[ax], G.coefA[ax], an, pn, aa, am, ae, amom, aE);
+      else
+        boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE);
     }
 
     kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);

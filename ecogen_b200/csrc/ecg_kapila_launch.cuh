@@ -18,15 +18,7 @@ cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eo
     return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   }
   Model<NP> M;
-  for (int k = 0; k < NP; k++) {
-    M.eos[k].type = eos[k].type;
-    M.eos[k].gamma = eos[k].gamma;
-    M.eos[k].pinf = eos[k].pinf;
-    M.eos[k].b = eos[k].b;
-    M.eos[k].cv = eos[k].cv;
-    M.eos[k].eref = eos[k].eref;
-    M.eos[k].sref = eos[k].sref;
-  }
+  for (int k = 0; k < NP; k++) M.eos[k] = make_eos_params(eos[k]);
   M.eps = eps;
   dim3 grid((G.n[0] + TS::X - 1) / TS::X, (G.n[1] + TS::Y - 1) / TS::Y, (G.n[2] + TS::Z - 1) / TS::Z);
   kern<<<grid, K::NTH, sm, s>>>(P, G, M);

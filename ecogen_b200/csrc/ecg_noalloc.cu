@@ -154,6 +154,7 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
     G.dfr[a] = S->dist + (size_t)(3 * a + 2) * nmax;
   }
   G.dim = dim;
+  side_geometry(*c, G);
   double dX = c->length[0] / (double)c->ncells[0], dY = c->length[1] / (double)c->ncells[1],
          dZ = c->length[2] / (double)c->ncells[2];
   double vol = dX * dY * dZ;

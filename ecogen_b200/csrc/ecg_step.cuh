@@ -20,11 +20,6 @@
 #pragma once
 #include "ecg_device.cuh"
 
-// Minimum resident blocks per SM asked of the compiler for the step kernels (caps registers at
-// 65536 / (256 x this)): 2 -> 128 registers without spills on the 2D two-phase kernels.
-#ifndef ECG_KAPILA_MIN_BLOCKS
-#define ECG_KAPILA_MIN_BLOCKS 2
-#endif
 
 namespace ecg {
 
@@ -33,15 +28,34 @@ enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
 // Cells of a block's tile and threads of the block.  Face fluxes are computed one per thread, so
 // the tiles are shaped for every axis to have at most THREADS faces ((X+1)*Y*Z, X*(Y+1)*Z,
 // X*Y*(Z+1)): each face pass then takes a single round and no warp waits at the following barrier
-// for a partial second round.
+// for a partial second round.  MINB is the number of resident blocks per SM asked of the compiler
+// (__launch_bounds__), which caps registers at 65536 / (THREADS * MINB): the kernels are bound by
+// FP64 latency, and more resident warps beat the spills this costs (measured: 2D two-phase MUSCL
+// step 28 % faster at 80 registers / 24 warps than at 128 registers / 16 warps).
+#ifndef ECG_TILE1D_MINB
+#define ECG_TILE1D_MINB 3
+#endif
+#ifndef ECG_TILE2D_X
+#define ECG_TILE2D_X 16
+#define ECG_TILE2D_Y 15
+#define ECG_TILE2D_THREADS 256
+#endif
+#ifndef ECG_TILE2D_MINB
+#define ECG_TILE2D_MINB 3
+#endif
+#ifndef ECG_TILE3D_MINB
+#define ECG_TILE3D_MINB 2
+#endif
 template <int DIM>
 struct TileShape;
 template <>
-struct TileShape<1> { static constexpr int X = 255, Y = 1, Z = 1, THREADS = 256; };
+struct TileShape<1> { static constexpr int X = 255, Y = 1, Z = 1, THREADS = 256, MINB = ECG_TILE1D_MINB; };
 template <>
-struct TileShape<2> { static constexpr int X = 16, Y = 15, Z = 1, THREADS = 256; };
+struct TileShape<2> {
+  static constexpr int X = ECG_TILE2D_X, Y = ECG_TILE2D_Y, Z = 1, THREADS = ECG_TILE2D_THREADS, MINB = ECG_TILE2D_MINB;
+};
 template <>
-struct TileShape<3> { static constexpr int X = 6, Y = 6, Z = 6, THREADS = 256; };
+struct TileShape<3> { static constexpr int X = 6, Y = 6, Z = 6, THREADS = 256, MINB = ECG_TILE3D_MINB; };
 
 // Field indices of a state array (stride = ncells):
 //   alpha_k [0,NP), rho_k [NP,2NP), p 2NP, u_d 2NP+1+d, E 2NP+1+DIM

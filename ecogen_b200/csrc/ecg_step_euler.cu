@@ -120,8 +120,11 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
 #pragma unroll
   for (int d = 0; d < DIM; d++) amom[d] = 0.;
   double dtmax = 1.e10;
+  double wallp[DIM];  // normal momentum flux of the cell's symmetry sides, per axis
+#pragma unroll
+  for (int d = 0; d < DIM; d++) wallp[d] = 0.;
 
-#pragma unroll 1
+#pragma unroll
   for (int ax = 0; ax < DIM; ax++) {
     const int T = K::ext(ax), RL = K::rlen(ax);
     const int b1 = (ax == 0) ? 1 : 0, b2 = (ax == 2) ? 1 : 2;
@@ -144,8 +147,19 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
       for (int e = tid; e < K::nslope(ax); e += K::NTH) {
         int j = e % (T + 3) - 1, line = e / (T + 3);
         int gl = org[ax] + j - 1;
-        if (gl < 0 || gl + 1 >= nax) continue;
         int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
+        if (gl < 0 || gl + 1 >= nax) {
+          // symmetry side: velocity slope along the axis (BoundCondWallO2Cartesian::computeSlopes :84-108,
+          // PhaseEuler::setU)
+          const int sd = (gl == -1) ? 0 : ((gl == nax - 1) ? 1 : -1);
+          if (sd < 0 || G.bc[2 * ax + sd] != ECG_BC_SYMMETRY) continue;
+          if (org[b1] + line % e1 >= G.n[b1] || org[b2] + line / e1 >= G.n[b2]) continue;
+#pragma unroll
+          for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = 0.;
+          const double wd = G.wslope[2 * ax + sd];
+          if (fabs(wd) > 1.e-8) ssl[(2 + ax) * SS + e] = sq[(2 + ax) * RS + (sd ? rl : rr)] / wd;
+          continue;
+        }
         double d = G.dcc[ax][gl];
 #pragma unroll
         for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = (sq[f * RS + rr] - sq[f * RS + rl]) / d;
@@ -174,7 +188,8 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
         } else {
           const int fs = line * (T + 3), f1 = fs + j + 1;
           const bool has = side ? (gl + 2 < nax) : (gl - 1 >= 0);
-          const int f2 = has ? (side ? fs + j + 2 : fs + j) : -1;
+          const bool wall = !has && G.bc[2 * ax + side] == ECG_BC_SYMMETRY;  // opposite slope of a symmetry side
+          const int f2 = (has || wall) ? (side ? fs + j + 2 : fs + j) : -1;
           const double sign = side ? -1. : 1.;
           const double dist = side ? G.dfr[ax][gl] : G.dfl[ax][gl];
           // PhaseEuler::limitSlopes (global limiter: the interface detector never fires for Euler),
@@ -228,16 +243,57 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
           aE -= cA * FE;
         }
       }
+      // symmetry side along ax: flux now (slopes of this axis staged), subtracted below in face order
+      const int sd = (gc[ax] == 0) ? 0 : ((gc[ax] == nax - 1) ? 1 : -1);
+      if (sd >= 0 && G.bc[2 * ax + sd] == ECG_BC_SYMMETRY) {
+        const int rc = line * RL + la + K::H;
+        EulerSide S;
+        S.rho = sq[0 * RS + rc];
+        S.p = sq[1 * RS + rc];
+        S.u[0] = S.u[1] = S.u[2] = 0.;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) S.u[d] = sq[(2 + d) * RS + rc];
+        if (K::O2) {
+          // BoundCondWallO2Cartesian::solveRiemann :111-141: limited slopes (global limiter), extrapolation
+          // by the signed distance without clamps
+          const int fs = line * (T + 3), fw = fs + la + 1 + sd, fo = fs + la + 2 - sd;
+          const double dist = G.wdist[2 * ax + sd];
+          S.rho = S.rho + limiter(P.lim[0], ssl[0 * SS + fw], ssl[0 * SS + fo]) * dist;
+          S.p = S.p + limiter(P.lim[0], ssl[1 * SS + fw], ssl[1 * SS + fo]) * dist;
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+            S.u[d] = S.u[d] + limiter(P.lim[0], ssl[(2 + d) * SS + fw], ssl[(2 + d) * SS + fo]) * dist;
+        }
+        euler_complete(q, eps, S);
+        double ul[3];
+        to_local(ax, sd == 0, S.u, ul);
+        // ModEuler::solveRiemannWall src/Models/Euler/ModEuler.cpp:368-409
+        const double uL = ul[0], cL = S.c, pL = S.p, rhoL = S.rho;
+        const double sL = dmin(uL - cL, -uL - cL);
+        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * G.lcfl / fabs(sL));
+        wallp[ax] = rhoL * uL * (uL - sL) + pL;
+      }
     }
     __syncthreads();
   }
 
   if (active) {
-#pragma unroll 1
+#pragma unroll
     for (int bf = 0; bf < 2 * DIM; bf++) {
       int ax = bf >> 1;
       bool neg = (bf & 1) == 0;
       if (neg ? (gc[ax] != 0) : (gc[ax] != G.n[ax] - 1)) continue;
+      if (G.bc[bf] == ECG_BC_SYMMETRY) {
+        const double Fn[3] = {wallp[ax], 0., 0.};
+        double Fg[3];
+        to_global(ax, neg, Fn, Fg);
+        const double cA = G.coefA[ax];
+        am -= cA * 0.;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) amom[d] -= cA * Fg[d];
+        aE -= cA * 0.;
+        continue;
+      }
       EulerSide S;
       S.rho = P.q[cell];
       S.p = P.q[nn + cell];

@@ -1,5 +1,6 @@
 // Types shared by the host code and the kernels.
 #pragma once
+#include <cmath>
 #include <cstdint>
 
 #include "../../include/ecogen_b200.h"
@@ -10,7 +11,17 @@ namespace ecg {
 struct EosParams {
   int type;
   double gamma, pinf, b, cv, eref, sref;
+  // sendSpecialMixtureEos constants (src/Eos/EosSG.cpp:196): gamma*pInf/(gamma-1) (0 for IG) and
+  // 1/(gamma-1), evaluated once on the host (IEEE division, the same value as in the kernels).
+  double gpi, ig;
 };
+
+inline EosParams make_eos_params(const ecg_eos& e) {
+  EosParams q{e.type, e.gamma, e.pinf, e.b, e.cv, e.eref, e.sref, 0., 0.};
+  q.gpi = (e.type == ECG_EOS_IG) ? 0. : e.gamma * e.pinf / (e.gamma - 1.);
+  q.ig = 1. / (e.gamma - 1.);
+  return q;
+}
 
 // Geometry of a uniform Cartesian mesh, precomputed on the host with the reference's formulas
 // (MeshCartesian::meshStretching src/Meshes/MeshCartesian.cpp:168 and
@@ -25,7 +36,33 @@ struct Geometry {
   const double* dcc[3];
   const double* dfl[3];
   const double* dfr[3];
+  // Sides Xm, Xp, Ym, Yp, Zm, Zp (index 2*axis + plus): boundary condition, centre-minus-face
+  // coordinate along the axis (Element::distanceX(Face*), divisor of a symmetry side's velocity
+  // slope) and the signed centre-to-face distance of the MUSCL extrapolation towards that side
+  // (negative on the minus sides, BoundCondWallO2Cartesian::solveRiemann).
+  int bc[6];
+  double wslope[6];
+  double wdist[6];
 };
+
+// Fills the side fields of a Geometry with the reference's mesh arithmetic (cell centres
+// (i + 0.5) * d, minus faces at 0, plus faces at the last centre + d / 2, src/Meshes/MeshCartesian.cpp:168,
+// :402, :426).
+inline void side_geometry(const ecg_case& c, Geometry& g) {
+  for (int a = 0; a < 3; a++) {
+    double d = c.length[a] / (double)c.ncells[a];
+    double p0 = (0 + 0.5) * d, pn = (c.ncells[a] - 1 + 0.5) * d;
+    double fm = 0., fp = pn + 0.5 * d;
+    for (int side = 0; side < 2; side++) {
+      double cen = side ? pn : p0, face = side ? fp : fm;
+      double x = face - cen;
+      double dist = std::sqrt(x * x + 0. * 0. + 0. * 0.);
+      g.bc[2 * a + side] = c.bc[2 * a + side];
+      g.wslope[2 * a + side] = cen - face;
+      g.wdist[2 * a + side] = side ? dist : -dist;
+    }
+  }
+}
 
 // Device counters filled by the step kernels.
 struct DevStats {

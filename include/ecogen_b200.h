@@ -46,6 +46,10 @@ enum {
   ECG_LIM_NONE = 0, ECG_LIM_MINMOD = 1, ECG_LIM_VANLEER = 2, ECG_LIM_VANALBADA = 3,
   ECG_LIM_SUPERBEE = 4, ECG_LIM_MC = 5, ECG_LIM_THINC = 6
 };
+/* Boundary condition of one side of the domain (initialConditions.xml <boundCond type=...>):
+ * nonReflecting (BoundCondNonReflecting), or symmetry -- also what an inviscid "wall" is
+ * (BoundCondSymmetry / BoundCondSymmetryO2Cartesian, src/InputOutput/Input.cpp:1146-1180). */
+enum { ECG_BC_NONREFLECTING = 0, ECG_BC_SYMMETRY = 1 };
 #define ECG_MAX_PHASES 3
 
 /* One EOS (src/Eos/EosIG.h, EosSG.h, EosNASG.h parameters). */
@@ -70,6 +74,7 @@ typedef struct {
   int32_t ptmu;                 /* p-T-mu relaxation (model.xml <relaxation type="PTMu">) */
   int32_t ptmu_liquid, ptmu_vapor;
   ecg_eos eos[ECG_MAX_PHASES];
+  int32_t bc[6];                /* ECG_BC_* of the sides Xm, Xp, Ym, Yp, Zm, Zp (MeshCartesian::assignLimits) */
 } ecg_case;
 
 /* Counters of one ecg_step call (replace the reference's errors / warnings vectors). */
@@ -231,6 +236,8 @@ ecg_status ecg_batch_set_seed_model(ecg_batch* b, const ecg_mlp* mlp);
 ecg_status ecg_batch_set_shape(ecg_batch* b, int32_t tile, int32_t threads);
 ecg_status ecg_batch_autotune(ecg_batch* b, int32_t* tile, int32_t* threads);
 int64_t ecg_batch_total_cells(const ecg_batch* b);
+/* The cudaStream_t every batch operation is ordered on (for events around ecg_batch_step). */
+void* ecg_batch_stream(const ecg_batch* b);
 
 #ifdef __cplusplus
 }

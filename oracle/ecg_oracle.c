@@ -50,6 +50,7 @@ typedef struct {
 typedef struct {
   int L, R;           /* R < 0 for a boundary face */
   int axis;           /* 0,1,2 */
+  int bc;             /* -1 internal face, else ECGO_BC_* of its side */
   double n[3], t[3], b[3];
   double surface;
   double pos[3];
@@ -850,7 +851,7 @@ static void build_mesh(ecgo_sim* S) {
     for (int iy = 0; iy < ny; iy++)
       for (int iz = 0; iz < nz; iz++) {
         OFace* F = &S->faces[f];
-        F->L = IDX(ix, iy, iz); F->R = IDX(ix + 1, iy, iz); F->axis = 0;
+        F->L = IDX(ix, iy, iz); F->R = IDX(ix + 1, iy, iz); F->axis = 0; F->bc = -1;
         SETV(F->n, 1., 0., 0.); SETV(F->t, 0., 1., 0.); SETV(F->b, 0., 0., 1.);
         F->surface = dY * dZ;
         SETV(F->pos, S->pos[3 * F->L] + 0.5 * dX, S->pos[3 * F->L + 1], S->pos[3 * F->L + 2]);
@@ -861,7 +862,7 @@ static void build_mesh(ecgo_sim* S) {
     for (int iy = 0; iy < ny - 1; iy++)
       for (int iz = 0; iz < nz; iz++) {
         OFace* F = &S->faces[f];
-        F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy + 1, iz); F->axis = 1;
+        F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy + 1, iz); F->axis = 1; F->bc = -1;
         SETV(F->n, 0., 1., 0.); SETV(F->t, -1., 0., 0.); SETV(F->b, 0., 0., 1.);
         F->surface = dX * dZ;
         SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1] + 0.5 * dY, S->pos[3 * F->L + 2]);
@@ -872,7 +873,7 @@ static void build_mesh(ecgo_sim* S) {
     for (int iy = 0; iy < ny; iy++)
       for (int iz = 0; iz < nz - 1; iz++) {
         OFace* F = &S->faces[f];
-        F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy, iz + 1); F->axis = 2;
+        F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy, iz + 1); F->axis = 2; F->bc = -1;
         SETV(F->n, 0., 0., 1.); SETV(F->t, 1., 0., 0.); SETV(F->b, 0., 1., 0.);
         F->surface = dX * dY;
         SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1], S->pos[3 * F->L + 2] + 0.5 * dZ);
@@ -880,54 +881,34 @@ static void build_mesh(ecgo_sim* S) {
         f++;
       }
   S->ninner = f;
-  /* boundary faces: Xm, Xp, Ym, Yp, Zm, Zp (src/Meshes/MeshCartesian.cpp:384-557) */
-  if (nx != 1) {
-    for (int iy = 0; iy < ny; iy++)
-      for (int iz = 0; iz < nz; iz++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(0, iy, iz); F->R = -1; F->axis = 0;
-        SETV(F->n, -1., 0., 0.); SETV(F->t, 0., -1., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dY * dZ;
-      }
-    for (int iy = 0; iy < ny; iy++)
-      for (int iz = 0; iz < nz; iz++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(nx - 1, iy, iz); F->R = -1; F->axis = 0;
-        SETV(F->n, 1., 0., 0.); SETV(F->t, 0., 1., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dY * dZ;
-      }
-  }
-  if (ny != 1) {
-    for (int ix = 0; ix < nx; ix++)
-      for (int iz = 0; iz < nz; iz++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(ix, 0, iz); F->R = -1; F->axis = 1;
-        SETV(F->n, 0., -1., 0.); SETV(F->t, 1., 0., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dX * dZ;
-      }
-    for (int ix = 0; ix < nx; ix++)
-      for (int iz = 0; iz < nz; iz++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(ix, ny - 1, iz); F->R = -1; F->axis = 1;
-        SETV(F->n, 0., 1., 0.); SETV(F->t, -1., 0., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dX * dZ;
-      }
-  }
-  if (nz != 1) {
-    for (int ix = 0; ix < nx; ix++)
-      for (int iy = 0; iy < ny; iy++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(ix, iy, 0); F->R = -1; F->axis = 2;
-        SETV(F->n, 0., 0., -1.); SETV(F->t, -1., 0., 0.); SETV(F->b, 0., 1., 0.);
-        F->surface = dX * dY;
-      }
-    for (int ix = 0; ix < nx; ix++)
-      for (int iy = 0; iy < ny; iy++) {
-        OFace* F = &S->faces[f++];
-        F->L = IDX(ix, iy, nz - 1); F->R = -1; F->axis = 2;
-        SETV(F->n, 0., 0., 1.); SETV(F->t, 1., 0., 0.); SETV(F->b, 0., 1., 0.);
-        F->surface = dX * dY;
-      }
+  /* boundary faces: Xm, Xp, Ym, Yp, Zm, Zp (src/Meshes/MeshCartesian.cpp:384-557); positions 0 on the
+   * minus sides and last centre + half size on the plus sides; each side takes the boundary condition
+   * of its index in the case file (MeshCartesian::assignLimits :86) */
+  const int nn3[3] = {nx, ny, nz};
+  for (int ax = 0; ax < 3; ax++) {
+    if (nn3[ax] == 1) continue;
+    int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
+    for (int side = 0; side < 2; side++) {
+      for (int a = 0; a < nn3[o1]; a++)
+        for (int b2 = 0; b2 < nn3[o2]; b2++) {
+          int ijk[3];
+          ijk[ax] = side ? nn3[ax] - 1 : 0;
+          ijk[o1] = a;
+          ijk[o2] = b2;
+          OFace* F = &S->faces[f];
+          F->L = IDX(ijk[0], ijk[1], ijk[2]); F->R = -1; F->axis = ax;
+          F->bc = c->bc[2 * ax + side];
+          double sg = side ? 1. : -1.;
+          if (ax == 0) { SETV(F->n, sg, 0., 0.); SETV(F->t, 0., sg, 0.); SETV(F->b, 0., 0., 1.); F->surface = dY * dZ; }
+          if (ax == 1) { SETV(F->n, 0., sg, 0.); SETV(F->t, -sg, 0., 0.); SETV(F->b, 0., 0., 1.); F->surface = dX * dZ; }
+          if (ax == 2) { SETV(F->n, 0., 0., sg); SETV(F->t, sg, 0., 0.); SETV(F->b, 0., 1., 0.); F->surface = dX * dY; }
+          const double dd[3] = {dX, dY, dZ};
+          for (int d = 0; d < 3; d++) F->pos[d] = S->pos[3 * F->L + d];
+          F->pos[ax] = side ? S->pos[3 * F->L + ax] + 0.5 * dd[ax] : 0.;
+          S->cellface[6 * F->L + 2 * ax + side] = f;
+          f++;
+        }
+    }
   }
 #undef IDX
 #undef SETV
@@ -972,6 +953,20 @@ static void compute_slopes(ecgo_sim* S, OSt* st) {
     }
     for (int d = 0; d < 3; d++) sl->u[d] = (R->m.u[d] - L->m.u[d]) / dist;
   }
+  /* symmetry sides: BoundCondWallO2Cartesian::computeSlopes src/BoundConds/BoundCondWallO2Cartesian.cpp:84-108.
+   * Only the velocity slope along each axis whose centre-to-face distance exceeds 1e-8 is set (the phase
+   * slopes of PUEq have no velocity and stay zero). */
+  for (int f = S->ninner; f < S->nfaces; f++) {
+    OFace* F = &S->faces[f];
+    if (F->bc != ECGO_BC_SYMMETRY) continue;
+    OSlope* sl = &S->slopes[f];
+    memset(sl, 0, sizeof(*sl));
+    const double* u = (S->c.model == ECGO_MODEL_EULER) ? st[F->L].ph[0].u : st[F->L].m.u;
+    for (int d = 0; d < 3; d++) {
+      double dd = S->pos[3 * F->L + d] - F->pos[d]; /* Element::distanceX(Face*) src/Meshes/Element.cpp:117 */
+      if (fabs(dd) > 1.e-8) sl->u[d] = u[d] / dd;
+    }
+  }
 }
 
 /* CellO2Cartesian::computeLocalSlopes src/Order2/CellO2Cartesian.cpp:23-171 for a Cartesian mesh without
@@ -985,10 +980,12 @@ static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, doub
   OSlope s1 = S->slopes[face], s2;
   double alphaAfter = 0.;
   memset(&s2, 0, sizeof(s2));
-  if (opp >= 0) {
+  if (opp >= 0 && S->faces[opp].bc != ECGO_BC_NONREFLECTING) {
+    /* a non-reflecting side has no slopes and is skipped; a symmetry side gives its slopes and, as
+     * alphaCellAfterOppositeSide, the cell's own alpha (its left cell, CellO2Cartesian.cpp:68-71) */
     s2 = S->slopes[opp];
     const OFace* G = &S->faces[opp];
-    int nb = (G->L == cell) ? G->R : G->L;
+    int nb = (G->R < 0) ? cell : ((G->L == cell) ? G->R : G->L);
     alphaAfter = (S->c.model == ECGO_MODEL_EULER) ? 0. : S->s[nb].ph[0].alpha;
   }
   int np = S->np;
@@ -1009,6 +1006,74 @@ static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, doub
     out->p[k] = ecgo_limiter(lim, s1.p[k], s2.p[k]);
   }
   for (int d = 0; d < 3; d++) out->u[d] = ecgo_limiter(lim, s1.u[d], s2.u[d]);
+}
+
+/* CellO2Cartesian::computeLocalSlopesLimite src/Order2/CellO2Cartesian.cpp:173-272 for a symmetry side:
+ * slope 1 is the side's own slope, slope 2 the slope of the internal face on the opposite side; the
+ * interface detector only tests the cell's time-n alpha against 1e-4. */
+static void local_slopes_side(ecgo_sim* S, int cell, int face, OSlope* out) {
+  const OFace* F = &S->faces[face];
+  int plus = (S->cellface[6 * cell + 2 * F->axis + 1] == face);
+  int opp = S->cellface[6 * cell + 2 * F->axis + (plus ? 0 : 1)];
+  OSlope s1 = S->slopes[face], s2;
+  memset(&s2, 0, sizeof(s2));
+  if (opp >= 0 && S->faces[opp].bc != ECGO_BC_NONREFLECTING) s2 = S->slopes[opp];
+  double eps = 1.e-4;
+  int interface = 0;
+  if (S->c.model != ECGO_MODEL_EULER) {
+    double a = S->s[cell].ph[0].alpha;
+    interface = (a >= eps) && (a <= 1. - eps);
+  }
+  int lim = interface ? S->c.lim[1] : S->c.lim[0];
+  int limv = interface ? S->c.lim[3] : S->c.lim[2];
+  if (S->c.model == ECGO_MODEL_EULER) {
+    out->rho[0] = ecgo_limiter(lim, s1.rho[0], s2.rho[0]);
+    out->p[0] = ecgo_limiter(lim, s1.p[0], s2.p[0]);
+    for (int d = 0; d < 3; d++) out->u[d] = ecgo_limiter(lim, s1.u[d], s2.u[d]);
+    return;
+  }
+  for (int k = 0; k < S->np; k++) {
+    out->alpha[k] = ecgo_limiter(limv, s1.alpha[k], s2.alpha[k]);
+    out->rho[k] = ecgo_limiter(lim, s1.rho[k], s2.rho[k]);
+    out->p[k] = ecgo_limiter(lim, s1.p[k], s2.p[k]);
+  }
+  for (int d = 0; d < 3; d++) out->u[d] = ecgo_limiter(lim, s1.u[d], s2.u[d]);
+}
+
+/* Reflecting boundary: ModUEq::solveRiemannWall src/Models/UEq/ModUEq.cpp:452-492 and
+ * ModEuler::solveRiemannWall src/Models/Euler/ModEuler.cpp:368-409 on the face-frame state. */
+static void riemann_wall(ecgo_sim* S, const OSt* b, double dxL, double* dtMax, OFlux* out) {
+  double uL, cL, pL, rhoL;
+  int euler = (S->c.model == ECGO_MODEL_EULER);
+  if (euler) {
+    uL = b->ph[0].u[0]; pL = b->ph[0].p; rhoL = b->ph[0].rho; cL = b->ph[0].c;
+  } else {
+    uL = b->m.u[0]; cL = b->m.cF; pL = b->m.p; rhoL = b->m.rho;
+  }
+  double sL = omin(uL - cL, -uL - cL);
+  if (fabs(sL) > 1.e-3) *dtMax = omin(*dtMax, 1. * dxL / fabs(sL));
+  double pStar = euler ? rhoL * uL * (uL - sL) + pL : rhoL * (uL - sL) * uL + pL;
+  memset(out, 0, sizeof(*out));
+  out->mom[0] = pStar;
+}
+
+static void extrapolate_side(ecgo_sim* S, OSt* b, const OSlope* sl, double dist) {
+  /* Phase::extrapolate / MixUEq::extrapolate without the clamps of the internal faces
+   * (BoundCondWallO2Cartesian::solveRiemann src/BoundConds/BoundCondWallO2Cartesian.cpp:120-131) */
+  if (S->c.model == ECGO_MODEL_EULER) {
+    OPh* ph = &b->ph[0];
+    ph->rho += sl->rho[0] * dist;
+    ph->p += sl->p[0] * dist;
+    for (int d = 0; d < 3; d++) ph->u[d] = ph->u[d] + sl->u[d] * dist;
+    return;
+  }
+  for (int k = 0; k < S->np; k++) {
+    OPh* ph = &b->ph[k];
+    ph->alpha += sl->alpha[k] * dist;
+    ph->rho += sl->rho[k] * dist;
+    ph->p += sl->p[k] * dist;
+  }
+  for (int d = 0; d < 3; d++) b->m.u[d] = b->m.u[d] + sl->u[d] * dist;
 }
 
 static void extrapolate(ecgo_sim* S, OSt* b, const OSlope* sl, double dist, double sign) {
@@ -1043,8 +1108,24 @@ static void flux_pass(ecgo_sim* S, OSt* prim, int o2, double* dtMax) {
     if (F->R < 0) {
       /* BoundCond::computeFlux / solveRiemann src/BoundConds/BoundCond.cpp:61-98 */
       OSt b = prim[F->L];
-      fulfill(S, &b);
-      riemann(S, &b, &b, F, S->lcfl[F->L], S->lcfl[F->L], dtMax, &fl);
+      if (F->bc == ECGO_BC_SYMMETRY) {
+        if (o2) {
+          /* BoundCondWallO2Cartesian::solveRiemann :111-141: extrapolate by the signed distance */
+          double dG = vnorm_diff(F->pos, &S->pos[3 * F->L]);
+          if (F->n[0] < 0. || F->n[1] < 0. || F->n[2] < 0.) dG = -dG;
+          OSlope sl;
+          memset(&sl, 0, sizeof(sl));
+          local_slopes_side(S, F->L, f, &sl);
+          extrapolate_side(S, &b, &sl, dG);
+        }
+        fulfill(S, &b);
+        proj_local(vel_of(S, &b), F->n, F->t, F->b);
+        riemann_wall(S, &b, S->lcfl[F->L], dtMax, &fl);
+        proj_reverse(fl.mom, F->n, F->t, F->b);
+      } else {
+        fulfill(S, &b);
+        riemann(S, &b, &b, F, S->lcfl[F->L], S->lcfl[F->L], dtMax, &fl);
+      }
       double cA = F->surface / S->vol[F->L];
       acc_sub(S, &S->cons[F->L], &fl, cA, &S->s[F->L]);
       continue;
@@ -1141,7 +1222,7 @@ ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho
   S->s = (OSt*)calloc((size_t)n, sizeof(OSt));
   S->s2 = (OSt*)calloc((size_t)n, sizeof(OSt));
   S->cons = (OFlux*)calloc((size_t)n, sizeof(OFlux));
-  S->slopes = (OSlope*)calloc((size_t)(S->ninner > 0 ? S->ninner : 1), sizeof(OSlope));
+  S->slopes = (OSlope*)calloc((size_t)(S->nfaces > 0 ? S->nfaces : 1), sizeof(OSlope));
   for (int i = 0; i < n; i++) {
     OSt* st = &S->s[i];
     if (c->model == ECGO_MODEL_EULER) {

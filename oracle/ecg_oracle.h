@@ -23,6 +23,9 @@ enum { ECGO_EOS_IG = 0, ECGO_EOS_SG = 1, ECGO_EOS_NASG = 2 };
 enum { ECGO_LIM_NONE = 0, ECGO_LIM_MINMOD = 1, ECGO_LIM_VANLEER = 2, ECGO_LIM_VANALBADA = 3,
        ECGO_LIM_SUPERBEE = 4, ECGO_LIM_MC = 5, ECGO_LIM_THINC = 6 };
 enum { ECGO_MODEL_KAPILA = 0, ECGO_MODEL_EULER = 1 };
+/* Boundary conditions per side Xm, Xp, Ym, Yp, Zm, Zp: non-reflecting, or symmetry (also an
+ * inviscid "wall", src/InputOutput/Input.cpp:1146-1180). */
+enum { ECGO_BC_NONREFLECTING = 0, ECGO_BC_SYMMETRY = 1 };
 
 typedef struct {
   int type;
@@ -40,6 +43,7 @@ typedef struct {
   int lim[4];      /* global, interface, global volume-fraction, interface volume-fraction */
   int ptmu, ptmu_liq, ptmu_vap;
   ecgo_eos eos[3];
+  int bc[6];       /* ECGO_BC_* per side */
 } ecgo_case;
 
 typedef struct {

@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libecg_oracle.so")
 
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
+BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
 
 
@@ -33,7 +34,7 @@ class Case(C.Structure):
                 ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("cfl", C.c_double),
                 ("lim", C.c_int * 4), ("ptmu", C.c_int), ("ptmu_liq", C.c_int), ("ptmu_vap", C.c_int),
-                ("eos", Eos * 3)]
+                ("eos", Eos * 3), ("bc", C.c_int * 6)]
 
 
 class Stats(C.Structure):
@@ -100,6 +101,8 @@ def make_case(case) -> Case:
         c.ptmu, c.ptmu_liq, c.ptmu_vap = 1, case.ptmu[0], case.ptmu[1]
     for k, e in enumerate(case.eos):
         c.eos[k] = Eos(EOS_CODE[e.kind], e.gamma, e.pinf, e.b, e.cv, e.eref, e.sref)
+    for i, b in enumerate(case.boundary_types()):
+        c.bc[i] = BC_CODE[b.upper()]
     return c
 
 

@@ -5,7 +5,7 @@ The reference is built from its own sources by ``make -C oracle ref`` (single-ra
 read back exactly by oracle/refrun.py) for one small case from ecogen_b200/cases.py, plus the
 initial state (result file 0).  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [key ...]
 """
 from __future__ import annotations
 
@@ -45,6 +45,25 @@ def golden_cases():
                                                 limiter=None, name="cavityO1")
     g["expansion2d_ptmu"] = cases.expansion_tube_2d(n=24, iterations=8)
     g["euler1d_o1"] = cases.euler_shock_tube(ncells=200, iterations=40)
+    # symmetry / wall sides (reflecting boundaries)
+    c = cases.shock_tube_1d(ncells=120, iterations=120, x_interface=0.75, name="tubeWallO1")
+    c.boundaries = ["symmetry", "wall"]
+    g["tube1d_wall_o1"] = c
+    c = cases.shock_tube_1d(ncells=120, iterations=120, x_interface=0.75, order="vanleer", name="tubeWallO2")
+    c.boundaries = ["wall", "symmetry"]
+    g["tube1d_wall_o2"] = c
+    c = cases.shock_bubble_2d(n=24, iterations=10, name="bubbleSym")
+    c.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry"]
+    g["bubble2d_sym_o2"] = c
+    c = cases.shock_bubble_2d(n=20, iterations=8, limiter=None, name="bubbleSymO1")
+    c.boundaries = ["symmetry", "nonReflecting", "symmetry", "wall"]
+    g["bubble2d_sym_o1"] = c
+    c = cases.cavity_collapse_3d(n=10, iterations=4, ninclusions=5, radius_cells=(2.0, 3.0), name="cavityWall")
+    c.boundaries = ["wall"] * 6
+    g["cavity3d_wall_o2"] = c
+    c = cases.euler_shock_tube(ncells=100, iterations=80, order="vanleer", name="eulerWall")
+    c.boundaries = ["wall", "symmetry"]
+    g["euler1d_wall_o2"] = c
     g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
     return g
 
@@ -59,7 +78,10 @@ def main():
     if not refrun.available():
         sys.exit("reference binary missing: run `make -C oracle ref` first")
     work = os.path.join(ROOT, "_work", "runs", "golden")
+    only = set(sys.argv[1:])
     for key, c in golden_cases().items():
+        if only and key not in only:
+            continue
         w = os.path.join(work, key)
         shutil.rmtree(w, ignore_errors=True)
         d = c.write(w)

@@ -90,8 +90,18 @@ def test_unsupported_inputs_are_refused(tmp_path):
     open(os.path.join(d, "mesh.xml"), "w").write(mesh)
     ic = open(os.path.join(d, "initialConditions.xml")).read()
     open(os.path.join(d, "initialConditions.xml"), "w").write(ic.replace('type="nonReflecting" number="1"',
-                                                                          'type="wall" number="1"'))
+                                                                          'type="outletPressure" number="1"'))
     _expect(2, lambda: api.Input(d, eosdir))
+
+
+def test_boundary_sides_read_in_order(tmp_path):
+    """The i-th boundCond is side i (Xm, Xp, Ym, Yp, ...); wall and symmetry are the same side type."""
+    case = cases.shock_bubble_2d(n=8, iterations=2)
+    case.boundaries = ["wall", "nonReflecting", "symmetry", "wall"]
+    d = case.write(str(tmp_path))
+    inp = api.Input(d, os.path.join(str(tmp_path), "libEOS"))
+    assert list(inp.case.bc) == [1, 0, 1, 1, 0, 0]
+    assert list(api.case_from_spec(case).bc) == [1, 0, 1, 1, 0, 0]
 
 
 def test_create_rejects_bad_cases_without_gpu_work():

@@ -14,8 +14,9 @@ from tests.helpers import gpu_run
 TOL = 1e-12
 KAPILA_KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_o2", "bubble2d_o2",
                "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
-               "expansion2d_ptmu"]
-EULER_KEYS = ["euler1d_o1", "euler1d_o2"]
+               "expansion2d_ptmu", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2", "bubble2d_sym_o1",
+               "cavity3d_wall_o2"]
+EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2"]
 
 
 def _compare(key, got, g):
@@ -56,17 +57,35 @@ def test_gpu_matches_oracle_2d(size, tmp_path):
 
 
 @pytest.mark.gpu
-def test_gpu_matches_oracle_3d_ragged(tmp_path):
+@pytest.mark.parametrize("sides", [None, ["wall", "nonReflecting", "symmetry", "symmetry", "nonReflecting", "wall"]])
+def test_gpu_matches_oracle_3d_ragged(sides, tmp_path):
     # non-multiple-of-tile sizes in every direction
     from ecogen_b200 import cases
     case = cases.cavity_collapse_3d(n=19, iterations=3, ninclusions=5, radius_cells=(2.0, 4.0))
     case.cells = (19, 7, 5)
+    case.boundaries = sides
     out = gpu_run(case, tmp_path)
     sim = oracle.Sim(case)
     sim.step(3)
     o = sim.fields()
     for name in ("alpha", "rho", "p", "u", "E"):
         assert rel_l1(out[name], o[name]) <= TOL, name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [None, "vanleer", "minmod"])
+def test_gpu_symmetry_sides_match_oracle_2d(order, tmp_path):
+    """Symmetry / wall sides on a mesh of several tiles per axis (tile edges next to the sides)."""
+    from ecogen_b200 import cases
+    case = cases.shock_bubble_2d(n=70, iterations=30, limiter=order, shock_x=6e-3, name="bubbleWalls")
+    case.boundaries = ["wall", "symmetry", "symmetry", "wall"]
+    out = gpu_run(case, tmp_path)
+    sim = oracle.Sim(case)
+    sim.step(30)
+    o = sim.fields()
+    for name in ("alpha", "rho", "p", "u", "E"):
+        assert rel_l1(out[name], o[name]) <= TOL, name
+    assert out["dt"] == pytest.approx(sim.dt.value, rel=1e-12)
 
 
 @pytest.mark.gpu
@@ -82,7 +101,7 @@ def test_newton_stats_match_oracle(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "euler1d_o2"])
+@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "euler1d_o2", "bubble2d_sym_o2"])
 def test_driver_writes_reference_results(key, golden_cases, tmp_path):
     """ecogen-b200 <work> runs ECOGEN.xml's cases and writes reference-format VTK results."""
     import subprocess

@@ -11,7 +11,8 @@ from oracle import oracle
 
 KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_o2", "bubble2d_o2",
         "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
-        "expansion2d_ptmu", "euler1d_o1", "euler1d_o2"]
+        "expansion2d_ptmu", "euler1d_o1", "euler1d_o2", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2",
+        "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2"]
 
 
 @pytest.mark.parametrize("key", KEYS)
