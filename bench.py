@@ -46,12 +46,39 @@ def make_case(config: str, size: int | None):
         return cases.cavity_collapse_3d(n=size or 256, iterations=10 ** 6)
     if config == "c5":
         return cases.expansion_tube_2d(n=size or 1024, iterations=10 ** 6)
+    if config == "c4":
+        # one case of the batched workload (its per-case reference timing)
+        return cases.shock_tube_1d(ncells=1000, iterations=10 ** 6, order="vanleer")
     return cases.shock_bubble_2d(n=size or 2048, iterations=10 ** 6)
 
 
+def state_fields(case) -> int:
+    """Doubles per cell of the stored state: (alpha_k, rho_k)_k, p, u (d components), E."""
+    per_phase = 1 if case.model.upper() == "EULER" else 2
+    return per_phase * case.nphases + 2 + case.dim
+
+
 def bytes_per_cell_update(case) -> int:
-    """Algorithmic bytes: read + write of (alpha_k, rho_k)_k, p, u (d components), E."""
-    return 16 * (2 * case.nphases + 2 + case.dim)
+    """Minimal algorithmic bytes of one step: read and write the state once."""
+    return 16 * state_fields(case)
+
+
+def pass_bytes_per_cell(case) -> dict:
+    """Algorithmic bytes per cell of each step kernel.
+
+    MUSCL predictor: reads S^n (NS doubles), writes S^{n+1/2} without E (NS - 1).
+    MUSCL corrector: reads S^{n+1/2} (NS - 1) and S^n (NS), writes S^{n+1} (NS).
+    First order: reads S^n, writes S^{n+1}.
+    """
+    ns = state_fields(case)
+    if case.second_order:
+        return {"pass1": 8 * (2 * ns - 1), "pass2": 8 * (3 * ns - 1)}
+    return {"pass1": 16 * ns}
+
+
+# DRAM bytes per cell of the corrector kernel measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, 2D two-phase MUSCL; profiles/k_kapila_step_shock_bubble_1536.md).
+NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 176.3, ("kapila", 2, 2, True, "pass1"): 109.8}
 
 
 class ClockSampler:
@@ -72,6 +99,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)  # the timed region starts once sampling runs
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -109,6 +139,17 @@ def measured_peak():
         return float(d["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def max_over_ranks(value: float, device: str) -> float:
+    """Max of a per-rank device time over all ranks of the default process group (if any)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 # ----------------------------------------------------------------------------------- reference arm
@@ -164,16 +205,74 @@ def reference_sample(steps: int, warmup: int, size: int = 256, iters: int = 4, p
                       f"(time of an {iters}-iteration run minus a 1-iteration run)", "samples": samples}
 
 
+# ------------------------------------------------------------------------------------ batched mode
+
+
+def bench_batch(args, rank, world, local):
+    """Batched independent 1D shock tubes (persistent work-queue kernel, per-case dt)."""
+    import ctypes as C
+
+    import torch
+    from ecogen_b200 import api, cases
+    torch.cuda.set_device(local if world > 1 else 0)
+    ncases = args.size or 4096
+    specs = cases.batch_shock_tubes(ncases=ncases, seed=2024 + rank, iterations=1000)
+    work = tempfile.mkdtemp(prefix=f"ecg_batch_{rank}_")
+    recs, fields = [], []
+    for i, c in enumerate(specs):
+        d = c.write(work, subdir=f"c{i}")
+        inp = api.Input(d, os.path.join(work, "libEOS"))
+        recs.append(inp.case)
+        fields.append(inp.fill())
+    shutil.rmtree(work, ignore_errors=True)
+    arr = (api.Case * len(recs))(*recs)
+    cat = [np.ascontiguousarray(np.concatenate([f[k] for f in fields])) for k in range(len(fields[0]))]
+    h = C.c_void_p()
+    api.check(api.lib().ecg_batch_create(arr, len(recs), C.byref(h)), "ecg_batch_create")
+    total = int(api.lib().ecg_batch_total_cells(h))
+    api.check(api.lib().ecg_batch_upload_prim(h, api._field_ptrs(cat), total), "upload")
+    tile, th = C.c_int32(), C.c_int32()
+    api.check(api.lib().ecg_batch_autotune(h, C.byref(tile), C.byref(th)), "autotune")
+    st = api.StepStats()
+    api.check(api.lib().ecg_batch_step(h, args.warmup, None, None, C.byref(st)), "warmup")
+    stream = torch.cuda.ExternalStream(api.lib().ecg_batch_stream(h))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        api.check(api.lib().ecg_batch_step(h, args.steps, None, None, C.byref(st)), "step")
+        e1.record(stream)
+        e1.synchronize()
+    dt_s = max_over_ranks(e0.elapsed_time(e1), "cuda") * 1e-3
+    value = total * args.steps / dt_s
+    api.lib().ecg_batch_destroy(h)
+    if rank == 0:
+        peak, kind = measured_peak()
+        B = 16 * (2 * 2 + 2 + 1)
+        line = {"metric": METRIC, "value": value * world, "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt_s * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": f"batched 1D shock tubes, Kapila 2-phase, MUSCL + van Leer, {len(recs)} cases",
+                           "cells": total, "tile": tile.value, "parallelism": f"replicas{world}"},
+                "roofline": {"bound": "hbm", "achieved": B * value / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": B * value / 1e9 / peak, "traffic": None, "peak_kind": kind},
+                "gpu_launches": args.steps * 3, "clocks": clk.summary(),
+                "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max}}
+        print(json.dumps(line))
+
+
 # ------------------------------------------------------------------------------------------- main
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--no-seeded", action="store_true", help="skip the learned-seed measurement")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -212,6 +311,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     else:
         torch.cuda.set_device(0)
+    if args.config == "c4":
+        bench_batch(args, rank, world, local)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     from ecogen_b200 import api
 
     work = tempfile.mkdtemp(prefix=f"ecg_bench_{rank}_")
@@ -235,12 +339,41 @@ def main():
         e1.synchronize()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, "cuda")
     value = case.ncells * args.steps * world / (ms_max * 1e-3)
+
+    # ---- learned seed: same workload, relaxation Newton started from the installed MLP
+    seeded = None
+    model_path = os.path.join(ROOT, "ecogen_b200", "models", f"seed_np{case.nphases}.npz")
+    if not args.no_seeded and os.path.exists(model_path):
+        from ecogen_b200 import seed as seedmod
+        model = seedmod.SeedModel.load(model_path)
+        ref_ctx = api.Context(inp.case)
+        ref_ctx.upload(fields0)
+        ctx3 = api.Context(inp.case)
+        ctx3.upload(fields0)
+        model.install(ctx3)
+        ref_ctx.step(args.warmup)
+        ctx3.step(args.warmup)
+        stream3 = torch.cuda.ExternalStream(api.lib().ecg_stream(ctx3.h))
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream3)
+        st3 = ctx3.step(args.steps)
+        s1.record(stream3)
+        s1.synchronize()
+        ms3 = s0.elapsed_time(s1)
+        st_ref = ref_ctx.step(args.steps)
+        a, b = ref_ctx.download_dict(), ctx3.download_dict()
+        diff = max(float(np.abs(a[k] - b[k]).sum() / max(np.abs(a[k]).sum(), 1e-300)) for k in ("alpha", "rho", "p", "E"))
+        seeded = {"value": case.ncells * args.steps / (ms3 * 1e-3), "unit": "cell-updates/s",
+                  "speedup_vs_plain": ms_max / ms3,
+                  "newton_evals_per_relaxation": st3.newton_evals / max(1, st3.relax_calls),
+                  "plain_newton_evals_per_relaxation": st_ref.newton_evals / max(1, st_ref.relax_calls),
+                  "seeded": st3.seeded, "seed_rejected": st3.seed_rejected, "fallback": st3.newton_fallback,
+                  "field_rel_l1_vs_plain": diff, "model": os.path.relpath(model_path, ROOT)}
+        ref_ctx.close()
+        ctx3.close()
 
     # ---- per-kernel attribution (separate launches, events between kernels)
     st_p, kms = ctx.step_profiled(max(2, min(args.steps, 10)))
@@ -281,7 +414,15 @@ def main():
     if rank == 0:
         peak, peak_kind = measured_peak()
         B = bytes_per_cell_update(case)
-        achieved = B * case.ncells / (step_ms * 1e-3) / 1e9
+        pb = pass_bytes_per_cell(case)
+        top = max(pb, key=lambda k: pass_ms[0 if k == "pass1" else 1])
+        top_ms = pass_ms[0 if top == "pass1" else 1]
+        achieved = pb[top] * case.ncells / (top_ms * 1e-3) / 1e9
+        tkey = ("euler" if case.model.upper() == "EULER" else "kapila", case.nphases, case.dim,
+                bool(case.second_order), top)
+        traffic = NCU_TRAFFIC_PER_CELL.get(tkey)
+        kname = {"pass1": "MUSCL predictor" if case.second_order else "first-order step",
+                 "pass2": "MUSCL corrector"}[top]
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = reference_sample(steps=2, warmup=0, config=args.config)
@@ -296,15 +437,20 @@ def main():
                     "note": "state uploaded from pinned host memory once and downloaded once per timed run; "
                             "one ecg_step call per step"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "one full step (predictor + corrector + dt update)",
-                         "bytes_per_cell_update": B},
+                         "frac": achieved / peak,
+                         "traffic": traffic * case.ncells if traffic is not None else None,
+                         "peak_kind": peak_kind, "kernel": f"{'k_euler_step' if tkey[0] == 'euler' else 'k_kapila_step'} ({kname})",
+                         "algorithmic_bytes_per_cell": pb[top], "launch_ms": top_ms,
+                         "step_bytes_per_cell_update": B,
+                         "step_frac": B * case.ncells / (step_ms * 1e-3) / 1e9 / peak},
             "kernels_ms": {"pass1": pass_ms[0], "pass2": pass_ms[1], "update": pass_ms[2]},
             "gpu_launches": args.steps * (3 if case.second_order else 2),
             "clocks": clk.summary(),
             "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max,
                        "fallback": st.newton_fallback, "hist": list(st.newton_hist)},
         }
+        if seeded is not None:
+            line["mlp_seeded"] = seeded
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "cell-updates/s", "cores": cpu["cores"],
                                     "kind": "reference", "sample": cpu["sample"]}

@@ -63,25 +63,29 @@ def make_model(w1, b1, w2, b2, w3, b3, in_shift, in_scale, out_shift, out_scale)
     return SeedModel(m, arrays)
 
 
-def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000) -> Tuple[np.ndarray, np.ndarray]:
-    """Run each case on the GPU for `steps` steps and collect (features, target) pairs."""
+def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000, warm: int = 0
+           ) -> Tuple[np.ndarray, np.ndarray]:
+    """Run each case on the GPU and collect (features, target) pairs of its relaxations.
+
+    Each case first runs `warm` steps unrecorded, then records during `steps` steps; the pair
+    budget is shared evenly between the cases.
+    """
     xs, ys = [], []
-    budget = max_pairs
+    per_case = max(1, max_pairs // max(1, len(case_specs)))
     for spec in case_specs:
-        if budget <= 0:
-            break
         with tempfile.TemporaryDirectory() as tmp:
             d = spec.write(tmp)
             inp = api.Input(d, os.path.join(tmp, "libEOS"))
             ctx = api.Context(inp.case)
             ctx.upload(inp.fill())
-            ctx.record_pairs(budget)
+            if warm:
+                ctx.step(warm)
+            ctx.record_pairs(per_case)
             ctx.step(steps)
             x, y = ctx.fetch_pairs()
             ctx.close()
         xs.append(x)
         ys.append(y)
-        budget -= len(y)
     if not xs:
         return np.zeros((0, 0), np.float32), np.zeros(0, np.float32)
     return np.concatenate(xs), np.concatenate(ys)
