@@ -278,7 +278,8 @@ def main():
     args = ap.parse_args()
     rank, world, local = env_rank()
     case = make_case(args.config, args.size)
-    workload = {"c1": "1D water/air shock tube, Kapila, first order",
+    workload = {"c4": "1D water/air shock tube, Kapila, MUSCL + van Leer (one case of the batched workload)",
+                "c1": "1D water/air shock tube, Kapila, first order",
                 "c2": "2D shock-bubble, Kapila 2-phase, MUSCL + van Leer",
                 "c3": "3D three-phase cavity collapse, Kapila, MUSCL + minmod",
                 "c5": "2D liquid/vapour expansion, Kapila + p-T-mu relaxation, MUSCL + van Leer"}[args.config]

@@ -131,6 +131,8 @@ def lib():
     L.ecg_batch_autotune.argtypes = [vp, P(C.c_int32), P(C.c_int32)]
     L.ecg_batch_total_cells.restype = C.c_int64
     L.ecg_batch_total_cells.argtypes = [vp]
+    L.ecg_input_output_control.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.ecg_restart_fill.argtypes = [C.POINTER(Case), C.POINTER(C.POINTER(C.c_double)), C.c_int64]
     L.ecg_batch_stream.restype = vp
     L.ecg_batch_stream.argtypes = [vp]
     _lib = L

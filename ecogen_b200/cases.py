@@ -155,6 +155,9 @@ class Case:
     boundaries: Optional[List[str]] = None  # boundCond types Xm, Xp, Ym, Yp, Zm, Zp (default nonReflecting)
     output_format: str = "XML"
     output_binary: bool = True
+    output_precision: Optional[int] = None  # outputMode precision (ASCII values, infoCalcul.out)
+    print_freq: Optional[int] = None        # iterFreq (iteration mode; default: print at the end only)
+    restart_file: Optional[int] = None      # restartSimulation restartFileNumber
     extra: Dict[str, object] = field(default_factory=dict)
 
     def boundary_types(self) -> List[str]:
@@ -178,7 +181,7 @@ class Case:
     def main_xml(self) -> str:
         if self.iterations is not None:
             tc = (f'<timeControlMode iterations="true">\n    <iterations number="{self.iterations}" '
-                  f'iterFreq="{self.iterations}"/>\n  </timeControlMode>')
+                  f'iterFreq="{self.print_freq or self.iterations}"/>\n  </timeControlMode>')
         else:
             tc = (f'<timeControlMode iterations="false">\n    <physicalTime totalTime="{self.total_time!r}" '
                   f'timeFreq="{self.total_time!r}"/>\n  </timeControlMode>')
@@ -195,10 +198,15 @@ class Case:
             so += "  </secondOrder>\n"
         binary = "true" if self.output_binary else "false"
         prec = ' precision="17"' if self.output_format == "GNU" else ""
+        if self.output_precision is not None:
+            prec = f' precision="{self.output_precision}"'
+        rs = ""
+        if self.restart_file is not None:
+            rs = f'  <restartSimulation restartFileNumber="{self.restart_file}" AMRsaveFreq="0"/>\n'
         return ('<?xml version = "1.0" encoding = "UTF-8" standalone = "yes"?>\n<computationParam>\n'
                 f'  <run>{self.name}</run>\n'
                 f'  <outputMode format="{self.output_format}" binary="{binary}"{prec}/>\n'
-                f'  {tc}\n  <computationControl CFL="{self.cfl!r}"/>\n{so}</computationParam>\n')
+                f'  {tc}\n  <computationControl CFL="{self.cfl!r}"/>\n{so}{rs}</computationParam>\n')
 
     def mesh_xml(self) -> str:
         lx, ly, lz = self.lengths

@@ -36,6 +36,7 @@ struct ecg_input {
   ecg_case c;
   int iter_freq = 0;
   double time_freq = 0.;
+  int binary = 1, precision = 0, restart_file = 0;
   std::string run_name;
   std::string output_format;
   std::vector<std::string> eos_names;
@@ -133,6 +134,13 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   const Node* om = mainx->child("outputMode");
   if (!om || om->attr("format").empty()) return bail(ECG_ERR_XML, "main.xml: <outputMode format> missing");
   in->output_format = upper(om->attr("format"));
+  {  // Output::Output src/InputOutput/Output.cpp:73-80: precision optional, binary required
+    bool bin = true;
+    if (!om->get_bool("binary", &bin)) return bail(ECG_ERR_XML, "main.xml: <outputMode binary> missing");
+    in->binary = bin ? 1 : 0;
+    int prec = 0;
+    if (om->get_int("precision", &prec)) in->precision = prec;
+  }
   const Node* tc = mainx->child("timeControlMode");
   bool iters = false;
   if (!tc || !tc->get_bool("iterations", &iters)) return bail(ECG_ERR_XML, "main.xml: <timeControlMode iterations> missing");
@@ -176,10 +184,12 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
     c.limiter[2] = gv;
     c.limiter[3] = iv;
   }
-  if (mainx->child("restartSimulation")) {
-    int rn = 0;
-    mainx->child("restartSimulation")->get_int("restartFileNumber", &rn);
-    if (rn > 0) return bail(ECG_ERR_UNSUPPORTED, "restart from result files: upload the fields with ecg_upload_prim");
+  if (const Node* rs = mainx->child("restartSimulation")) {  // Input::inputMain :305-311
+    int rn = 0, freq = 0;
+    if (!rs->get_int("restartFileNumber", &rn)) return bail(ECG_ERR_XML, "main.xml: <restartSimulation restartFileNumber> missing");
+    if (!rs->get_int("AMRsaveFreq", &freq)) return bail(ECG_ERR_XML, "main.xml: <restartSimulation AMRsaveFreq> missing");
+    if (rn < 0) return bail(ECG_ERR_XML, "main.xml: negative restartFileNumber");
+    in->restart_file = rn;
   }
 
   // ---------------------------------------------------------------- mesh.xml (Input::inputMesh :319)
@@ -442,6 +452,55 @@ extern "C" ecg_status ecg_input_print_control(const ecg_input* in, int32_t* iter
   if (!in) return fail(ECG_ERR_INVALID, "null input");
   if (iter_freq) *iter_freq = in->iter_freq;
   if (time_freq) *time_freq = in->time_freq;
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_input_output_control(const ecg_input* in, int32_t* binary, int32_t* precision,
+                                               int32_t* restart_file) {
+  if (!in) return fail(ECG_ERR_INVALID, "null input");
+  if (binary) *binary = in->binary;
+  if (precision) *precision = in->precision;
+  if (restart_file) *restart_file = in->restart_file;
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_restart_fill(const ecg_case* cp, double* const* fields, int64_t ncells) {
+  if (!cp || !fields) return fail(ECG_ERR_INVALID, "ecg_restart_fill: null argument");
+  const ecg_case& c = *cp;
+  int64_t n = (int64_t)c.ncells[0] * c.ncells[1] * c.ncells[2];
+  if (ncells != n) return fail(ECG_ERR_INVALID, "ecg_restart_fill: ncells does not match the mesh");
+  const int nf = ecg::abi_nfields(c);
+  for (int f = 0; f < nf; f++)
+    if (!fields[f]) return fail(ECG_ERR_INVALID, "ecg_restart_fill: null field pointer");
+  const double eps = c.alpha_null ? 1.e-15 : 0.;
+  const int np = c.nphases;
+  for (int64_t i = 0; i < n; i++) {
+    if (c.model == ECG_MODEL_EULER) {
+      const double u0 = fields[2][i], u1 = fields[3][i], u2 = fields[4][i];
+      fields[5][i] = ecg::host_eos_e(c.eos[0], eps, fields[0][i], fields[1][i]) + 0.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+      continue;
+    }
+    const double p = fields[2 * np][i];
+    double rho = 0., e = 0., ek[ECG_MAX_PHASES];
+    for (int k = 0; k < np; k++) {
+      double& a = fields[k][i];
+      double& r = fields[np + k][i];
+      if (eps > 1.e-20) {  // PhaseUEq::verifyAndCorrectPhase src/Models/UEq/PhaseUEq.cpp:355
+        if (a < 0.) a = 0.;
+        if (a > 1.) a = 1.;
+        if (r <= 1.e-15) r = 1.e-15;
+      } else {
+        if (a < 1e-15) a = 1e-14;
+        if (a > 1. - 1e-15) a = 1. - 1e-14;
+        if (r < 1.e-15) r = 1.e-14;
+      }
+      ek[k] = ecg::host_eos_e(c.eos[k], eps, r, ecg::host_eos_fix_p(c.eos[k], p));
+    }
+    for (int k = 0; k < np; k++) rho += fields[k][i] * fields[np + k][i];
+    for (int k = 0; k < np; k++) e += fields[k][i] * fields[np + k][i] / std::max(rho, eps) * ek[k];
+    const double u0 = fields[2 * np + 1][i], u1 = fields[2 * np + 2][i], u2 = fields[2 * np + 3][i];
+    fields[2 * np + 4][i] = e + 0.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+  }
   return ECG_OK;
 }
 

@@ -19,4 +19,11 @@ inline double host_eos_e(const ecg_eos& q, double eps, double rho, double p) {
   return (p + q.gamma * q.pinf) * std::max(1. - rho * q.b, eps) / (q.gamma - 1.) / std::max(rho, eps) + q.eref;
 }
 
+// Eos::verifyAndModifyPressure (EosIG.cpp, EosSG.cpp, EosNASG.cpp): pressure floors.
+inline double host_eos_fix_p(const ecg_eos& q, double p) {
+  if (q.type == ECG_EOS_IG) return (p < 1.e-8) ? 1.e-8 : p;
+  double floor = -(1. - 1.e-15) * q.pinf + 1.e-15;
+  return (p <= floor) ? floor : p;
+}
+
 }  // namespace ecg

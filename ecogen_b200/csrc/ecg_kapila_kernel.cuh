@@ -15,6 +15,8 @@ struct KapilaStep {
   static constexpr int NTH = TS::THREADS;
   static constexpr int NCELL = TS::X * TS::Y * TS::Z;
   static constexpr bool O2 = (PASS != PASS_O1);
+  static_assert(NCELL <= NTH, "one thread per cell of the tile");
+  static_assert(NTH % 32 == 0 && NTH <= 1024, "whole warps");
 
   __host__ __device__ static constexpr int ext(int a) { return a == 0 ? TS::X : (a == 1 ? TS::Y : TS::Z); }
   __host__ __device__ static constexpr int lines(int a) { return NCELL / ext(a); }

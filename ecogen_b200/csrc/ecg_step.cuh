@@ -30,18 +30,26 @@ enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
 // X*Y*(Z+1)): each face pass then takes a single round and no warp waits at the following barrier
 // for a partial second round.  MINB is the number of resident blocks per SM asked of the compiler
 // (__launch_bounds__), which caps registers at 65536 / (THREADS * MINB): the kernels are bound by
-// FP64 latency, and more resident warps beat the spills this costs (measured: 2D two-phase MUSCL
-// step 28 % faster at 80 registers / 24 warps than at 128 registers / 16 warps).
+// FP64 latency, and more resident warps beat the spills this costs.  Measured on the 2048^2
+// two-phase MUSCL step (cell-updates/s): 16x15 / 256 threads / 2 blocks (128 registers) 652 M;
+// 16x15 / 256 / 3 (80) 825 M; 16x15 / 256 / 4 (64) 790 M; 8x14 / 128 / 6 (80) 849 M;
+// 8x14 / 128 / 7 (72) 949 M; 8x14 / 128 / 8 (64) 883 M; 16x7 / 128 / 7 868 M; 8x7 / 64 / 14 719 M.
 #ifndef ECG_TILE1D_MINB
 #define ECG_TILE1D_MINB 3
 #endif
 #ifndef ECG_TILE2D_X
-#define ECG_TILE2D_X 16
-#define ECG_TILE2D_Y 15
-#define ECG_TILE2D_THREADS 256
+#define ECG_TILE2D_X 8
+#define ECG_TILE2D_Y 14
+#define ECG_TILE2D_THREADS 128
 #endif
 #ifndef ECG_TILE2D_MINB
-#define ECG_TILE2D_MINB 3
+#define ECG_TILE2D_MINB 7
+#endif
+#ifndef ECG_TILE3D_X
+#define ECG_TILE3D_X 6
+#define ECG_TILE3D_Y 6
+#define ECG_TILE3D_Z 6
+#define ECG_TILE3D_THREADS 256
 #endif
 #ifndef ECG_TILE3D_MINB
 #define ECG_TILE3D_MINB 2
@@ -55,7 +63,10 @@ struct TileShape<2> {
   static constexpr int X = ECG_TILE2D_X, Y = ECG_TILE2D_Y, Z = 1, THREADS = ECG_TILE2D_THREADS, MINB = ECG_TILE2D_MINB;
 };
 template <>
-struct TileShape<3> { static constexpr int X = 6, Y = 6, Z = 6, THREADS = 256, MINB = ECG_TILE3D_MINB; };
+struct TileShape<3> {
+  static constexpr int X = ECG_TILE3D_X, Y = ECG_TILE3D_Y, Z = ECG_TILE3D_Z, THREADS = ECG_TILE3D_THREADS,
+                       MINB = ECG_TILE3D_MINB;
+};
 
 // Field indices of a state array (stride = ncells):
 //   alpha_k [0,NP), rho_k [NP,2NP), p 2NP, u_d 2NP+1+d, E 2NP+1+DIM

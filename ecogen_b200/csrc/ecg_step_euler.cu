@@ -19,6 +19,8 @@ struct EulerStep {
   static constexpr int NTH = TS::THREADS;
   static constexpr int NCELL = TS::X * TS::Y * TS::Z;
   static constexpr bool O2 = (PASS != PASS_O1);
+  static_assert(NCELL <= NTH, "one thread per cell of the tile");
+  static_assert(NTH % 32 == 0 && NTH <= 1024, "whole warps");
   static constexpr int NQ = 3 + DIM;      // rho, p, u_d, E
   static constexpr int NSL = 2 + DIM;     // rho, p, u_d
   static constexpr int NFL = 2 + DIM;     // mass, mom_d, E

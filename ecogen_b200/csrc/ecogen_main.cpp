@@ -4,18 +4,24 @@
 //
 // Like the reference's main (src/main.cpp:44-133) it reads <work>/ECOGEN.xml, runs each <testCase>
 // folder in turn with the EOS files of <work>/libEOS, and writes results to
-// <work>/results/<run>/: infoCalcul.out (iteration, time, dt per print) and, at every print time,
-// datasets/resultB64_CPU0_TIME<k>.vtr — a VTK rectilinear grid with base64 Float64 cell arrays named
-// like the reference's writer (src/InputOutput/OutputXML.cpp:320-470).  Print control follows
-// Run::solver (src/Run.cpp:417-428): every iterFreq iterations, or every timeFreq of physical time
-// and at the end.  A case the library does not run is reported and skipped; the exit code is the
-// number of failed cases.
+// <work>/results/<run>/: infoCalcul.out (CPU count, then file number, iteration, time, next dt and
+// computation seconds per print, src/InputOutput/Output.cpp:491) and, at every print time,
+// datasets/result[B64]_CPU0_TIME<k>.vtr — a VTK rectilinear grid with Float64 cell arrays named and
+// ordered like the reference's writer (src/InputOutput/OutputXML.cpp:320-470), base64 or ASCII with
+// the outputMode precision.  Print control follows Run::solver (src/Run.cpp:417-428): every iterFreq
+// iterations, or every timeFreq of physical time and at the end.  <restartSimulation
+// restartFileNumber="N"> restarts from result file N and its infoCalcul.out line (Run::restartSimulation
+// src/Run.cpp:345, Output::readInfos src/InputOutput/Output.cpp:524): ASCII files as the reference
+// reads them, and base64 files too.  A case the library does not run is reported and skipped; the
+// exit code is the number of failed cases.
 #include <sys/stat.h>
 
 #include <cerrno>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -50,16 +56,113 @@ std::string b64(const unsigned char* d, size_t n) {
   return out;
 }
 
-// VTK "binary" inline array: base64 of a 4-byte length header, then base64 of the data
-void write_array(std::ostream& f, const std::string& name, const std::vector<double>& v, int ncomp) {
+// VTK inline array.  "binary": base64 of a 4-byte length header, then base64 of the data
+// (IO::writeb64Chaine src/InputOutput/IO.cpp:40); "ascii": every value streamed with the stream's
+// precision and a space (Output::writeDataset src/InputOutput/Output.cpp:372).
+void write_array(std::ostream& f, const std::string& name, const std::vector<double>& v, int ncomp, bool binary) {
   f << "        <DataArray type=\"Float64\"";
   if (!name.empty()) f << " Name=\"" << name << "\"";
   if (ncomp > 1) f << " NumberOfComponents=\"" << ncomp << "\"";
-  f << " format=\"binary\">\n";
-  int32_t nb = (int32_t)(v.size() * sizeof(double));
-  f << b64(reinterpret_cast<const unsigned char*>(&nb), 4)
-    << b64(reinterpret_cast<const unsigned char*>(v.data()), v.size() * sizeof(double)) << "\n";
+  f << " format=\"" << (binary ? "binary" : "ascii") << "\">\n";
+  if (binary) {
+    int32_t nb = (int32_t)(v.size() * sizeof(double));
+    f << b64(reinterpret_cast<const unsigned char*>(&nb), 4)
+      << b64(reinterpret_cast<const unsigned char*>(v.data()), v.size() * sizeof(double)) << "\n";
+  } else {
+    for (double x : v) f << x << " ";
+    f << "\n";
+  }
   f << "        </DataArray>\n";
+}
+
+int b64val(char ch) {
+  if (ch >= 'A' && ch <= 'Z') return ch - 'A';
+  if (ch >= 'a' && ch <= 'z') return ch - 'a' + 26;
+  if (ch >= '0' && ch <= '9') return ch - '0' + 52;
+  if (ch == '+') return 62;
+  if (ch == '/') return 63;
+  return -1;
+}
+
+// Decodes one base64 group sequence (stops at padding); returns false on a bad character.
+bool unb64(const std::string& s, size_t pos, size_t len, std::vector<unsigned char>& out) {
+  unsigned acc = 0;
+  int bits = 0;
+  for (size_t i = pos; i < pos + len && i < s.size(); i++) {
+    char ch = s[i];
+    if (ch == '=') break;
+    int v = b64val(ch);
+    if (v < 0) return false;
+    acc = (acc << 6) | (unsigned)v;
+    bits += 6;
+    if (bits >= 8) {
+      bits -= 8;
+      out.push_back((unsigned char)((acc >> bits) & 0xFF));
+    }
+  }
+  return true;
+}
+
+// The Float64 cell arrays of a result file, in document order (OutputXML::ReadPhysicalDataXML
+// src/InputOutput/OutputXML.cpp:194 reads them by position, not by name).
+bool read_cell_arrays(const std::string& path, std::vector<std::vector<double>>& arrays, std::string* err) {
+  std::ifstream f(path);
+  if (!f) {
+    *err = "cannot open " + path;
+    return false;
+  }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string txt = ss.str();
+  size_t pos = txt.find("<CellData>");
+  if (pos == std::string::npos) {
+    *err = path + ": <CellData> missing";
+    return false;
+  }
+  const size_t end = txt.find("</CellData>", pos);
+  while (true) {
+    size_t a = txt.find("<DataArray", pos);
+    if (a == std::string::npos || (end != std::string::npos && a > end)) break;
+    size_t gt = txt.find('>', a);
+    size_t close = txt.find("</DataArray>", gt);
+    if (gt == std::string::npos || close == std::string::npos) {
+      *err = path + ": unterminated DataArray";
+      return false;
+    }
+    const std::string head = txt.substr(a, gt - a);
+    std::vector<double> v;
+    if (head.find("format=\"binary\"") != std::string::npos) {
+      size_t p0 = txt.find_first_not_of(" \t\r\n", gt + 1);
+      std::vector<unsigned char> h;
+      if (p0 == std::string::npos || !unb64(txt, p0, 8, h) || h.size() < 4) {
+        *err = path + ": bad base64 header";
+        return false;
+      }
+      int32_t nb;
+      std::memcpy(&nb, h.data(), 4);
+      std::vector<unsigned char> d;
+      size_t p1 = p0 + 8, p2 = txt.find_last_not_of(" \t\r\n", close - 1);
+      if (!unb64(txt, p1, p2 + 1 - p1, d) || nb < 0 || d.size() < (size_t)nb) {
+        *err = path + ": bad base64 data";
+        return false;
+      }
+      v.resize((size_t)nb / sizeof(double));
+      std::memcpy(v.data(), d.data(), v.size() * sizeof(double));
+    } else {
+      const char* q = txt.c_str() + gt + 1;
+      const char* qe = txt.c_str() + close;
+      while (q < qe) {
+        char* nx = nullptr;
+        double x = std::strtod(q, &nx);
+        if (nx == q) break;
+        v.push_back(x);
+        q = nx;
+      }
+    }
+    arrays.push_back(std::move(v));
+    pos = close + 12;
+  }
+  return true;
 }
 
 bool mkdirs(const std::string& p) {
@@ -79,12 +182,18 @@ std::string strip_xml(const std::string& s) {  // "SG_water.xml" -> "SG_water" (
   return s.size() > 4 ? s.substr(0, s.size() - 4) : s;
 }
 
+std::string result_name(bool binary, int file) {  // OutputXML::createFilenameXML :271
+  return std::string("result") + (binary ? "B64" : "") + "_CPU0_TIME" + std::to_string(file) + ".vtr";
+}
+
 struct Output {
   std::string dir;
   const ecg_input* in;
   ecg_case c;
   int64_t n;
   int file = 0;
+  bool binary = true;
+  int precision = 0;
 
   bool write(ecg_ctx* ctx) {
     const int np = c.nphases;
@@ -96,10 +205,9 @@ struct Output {
     if (ecg_download_prim(ctx, ptr.data(), n) != ECG_OK) return false;
     std::vector<double> T((size_t)np * n), Y((size_t)np * n);
     if (ecg_download_derived(ctx, T.data(), Y.data(), n) != ECG_OK) return false;
-    char name[64];
-    std::snprintf(name, sizeof(name), "resultB64_CPU0_TIME%d.vtr", file++);
-    std::ofstream o(dir + "datasets/" + name, std::ios::trunc);
+    std::ofstream o(dir + "datasets/" + result_name(binary, file++), std::ios::trunc);
     if (!o) return false;
+    if (precision != 0) o.precision(precision);
     int nx = c.ncells[0], ny = c.ncells[1], nz = c.ncells[2];
     o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"RectilinearGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
     o << "  <RectilinearGrid WholeExtent=\"0 " << nx << " 0 " << ny << " 0 " << nz << "\">\n";
@@ -108,7 +216,7 @@ struct Output {
       std::vector<double> x((size_t)c.ncells[a] + 1);
       double d = c.length[a] / (double)c.ncells[a];
       for (int i = 0; i <= c.ncells[a]; i++) x[i] = i * d;
-      write_array(o, "", x, 1);
+      write_array(o, "", x, 1, binary);
     }
     o << "      </Coordinates>\n      <CellData>\n";
     auto slice = [&](const std::vector<double>& v, int k) {
@@ -116,13 +224,13 @@ struct Output {
     };
     if (euler) {
       std::string e = strip_xml(ecg_input_eos_name(in, 0));
-      write_array(o, "F0_Density_" + e, f[0], 1);
-      write_array(o, "F0_Pressure_" + e, f[1], 1);
-      write_array(o, "F0_Temperature_" + e, slice(T, 0), 1);
+      write_array(o, "F0_Density_" + e, f[0], 1, binary);
+      write_array(o, "F0_Pressure_" + e, f[1], 1, binary);
+      write_array(o, "F0_Temperature_" + e, slice(T, 0), 1, binary);
       std::vector<double> u((size_t)3 * n);
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 + d][i];
-      write_array(o, "F0_Velocity_" + e, u, 3);
+      write_array(o, "F0_Velocity_" + e, u, 3, binary);
     } else {
       for (int k = 0; k < np; k++) {  // PhasePUEq scalars (src/Models/PUEq/PhasePUEq.cpp:60-110)
         std::string e = strip_xml(ecg_input_eos_name(in, k));
@@ -133,21 +241,21 @@ struct Output {
           if (t[i] < 1.e-20) t[i] = 1.e-20;
           if (y[i] < 1.e-20) y[i] = 0.;
         }
-        write_array(o, "F" + std::to_string(k) + "_Alpha_" + e, a, 1);
-        write_array(o, "F" + std::to_string(k) + "_Density_" + e, r, 1);
-        write_array(o, "F" + std::to_string(k) + "_Temperature_" + e, t, 1);
-        write_array(o, "F" + std::to_string(k) + "_Mass fraction_" + e, y, 1);
+        write_array(o, "F" + std::to_string(k) + "_Alpha_" + e, a, 1, binary);
+        write_array(o, "F" + std::to_string(k) + "_Density_" + e, r, 1, binary);
+        write_array(o, "F" + std::to_string(k) + "_Temperature_" + e, t, 1, binary);
+        write_array(o, "F" + std::to_string(k) + "_Mass fraction_" + e, y, 1, binary);
       }
       std::vector<double> rho((size_t)n, 0.);
       for (int k = 0; k < np; k++)
         for (int64_t i = 0; i < n; i++) rho[i] += f[k][i] * f[np + k][i];
-      write_array(o, "Density_Mixture", rho, 1);
-      write_array(o, "Pressure_Mixture", f[2 * np], 1);
-      write_array(o, "Total_energy_Mixture", f[2 * np + 4], 1);
+      write_array(o, "Density_Mixture", rho, 1, binary);
+      write_array(o, "Pressure_Mixture", f[2 * np], 1, binary);
+      write_array(o, "Total_energy_Mixture", f[2 * np + 4], 1, binary);
       std::vector<double> u((size_t)3 * n);
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 * np + 1 + d][i];
-      write_array(o, "Velocity_Mixture", u, 3);
+      write_array(o, "Velocity_Mixture", u, 3, binary);
     }
     o << "      </CellData>\n    </Piece>\n  </RectilinearGrid>\n</VTKFile>\n";
     return (bool)o;
@@ -175,28 +283,107 @@ int run_case(const std::string& work, const std::string& rel) {
     ecg_input_free(in);
     return 1;
   }
+  int32_t binary = 1, precision = 0, restart = 0;
+  ecg_input_output_control(in, &binary, &precision, &restart);
   const int nf = c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5;
   std::vector<std::vector<double>> f(nf, std::vector<double>((size_t)n));
   std::vector<double*> ptr;
   for (auto& v : f) ptr.push_back(v.data());
-  s = ecg_input_fill(in, ptr.data(), n);
-  if (s == ECG_OK) s = ecg_upload_prim(ctx, ptr.data(), n);
   std::string out = work + "results/" + ecg_input_run_name(in) + "/";
-  if (s != ECG_OK || !mkdirs(out + "datasets")) {
-    std::fprintf(stderr, "%s: cannot start: %s\n", rel.c_str(), ecg_last_error());
+  Output w{out, in, c, n, 0, binary != 0, precision};
+  double dt = 1.e-15, t = 0.;
+  int32_t it = 0;
+  std::string fail_msg;
+  // infoCalcul.out lines as Output::saveInfos writes them (src/InputOutput/Output.cpp:491-515): the CPU
+  // count, then "file iteration time nextDt computeSeconds amrSeconds commSeconds" per print
+  std::vector<std::string> info_lines;
+  if (restart > 0) {
+    // Output::readInfos :524: the line of file N gives iteration, time and the next dt (as printed)
+    std::ifstream fi(out + "infoCalcul.out");
+    std::string line;
+    bool found = false;
+    if (fi && std::getline(fi, line)) {
+      info_lines.push_back(line);
+      if (std::atoi(line.c_str()) != 1) fail_msg = "restart needs a single-CPU infoCalcul.out";
+      while (fail_msg.empty() && std::getline(fi, line)) {
+        info_lines.push_back(line);
+        std::istringstream ls(line);
+        int num = -1;
+        ls >> num;
+        if (num == restart) {
+          ls >> it >> t >> dt;
+          found = (bool)ls;
+          break;
+        }
+      }
+    }
+    if (fail_msg.empty() && !found) fail_msg = "restart not possible - check file 'infoCalcul.out'";
+    std::vector<std::vector<double>> arrays;
+    if (fail_msg.empty() && !read_cell_arrays(out + "datasets/" + result_name(binary != 0, restart), arrays, &fail_msg))
+      fail_msg = "restart: " + fail_msg;
+    if (fail_msg.empty()) {
+      // phase scalars then vectors, mixture scalars then vectors (OutputXML::ReadPhysicalDataXML :194)
+      const int np = c.nphases;
+      const bool euler = c.model == ECG_MODEL_EULER;
+      const size_t need = euler ? 4 : (size_t)4 * np + 4;
+      bool ok = arrays.size() >= need;
+      for (size_t a = 0; ok && a < need; a++) {
+        bool vec = euler ? a == 3 : a == need - 1;
+        ok = arrays[a].size() == (size_t)n * (vec ? 3 : 1);
+      }
+      if (!ok) {
+        fail_msg = "restart: result file does not hold this case's fields";
+      } else if (euler) {  // F0 density, pressure, temperature, velocity
+        f[0] = arrays[0];
+        f[1] = arrays[1];
+        for (int64_t i = 0; i < n; i++)
+          for (int d = 0; d < 3; d++) f[2 + d][i] = arrays[3][3 * i + d];
+      } else {  // F<k> alpha, density, temperature, mass fraction; mixture density, pressure, energy, velocity
+        for (int k = 0; k < np; k++) {
+          f[k] = arrays[4 * k];
+          f[np + k] = arrays[4 * k + 1];
+        }
+        f[2 * np] = arrays[4 * np + 1];
+        f[2 * np + 4] = arrays[4 * np + 2];
+        for (int64_t i = 0; i < n; i++)
+          for (int d = 0; d < 3; d++) f[2 * np + 1 + d][i] = arrays[4 * np + 3][3 * i + d];
+      }
+    }
+    if (fail_msg.empty()) {
+      s = ecg_restart_fill(&c, ptr.data(), n);
+      if (s == ECG_OK) s = ecg_upload_prim(ctx, ptr.data(), n);
+      if (s != ECG_OK) fail_msg = ecg_last_error();
+    }
+    w.file = restart + 1;
+  } else {
+    s = ecg_input_fill(in, ptr.data(), n);
+    if (s == ECG_OK) s = ecg_upload_prim(ctx, ptr.data(), n);
+    if (s != ECG_OK) fail_msg = ecg_last_error();
+  }
+  if (fail_msg.empty() && !mkdirs(out + "datasets")) fail_msg = "cannot create " + out + "datasets";
+  if (!fail_msg.empty()) {
+    std::fprintf(stderr, "%s: cannot start: %s\n", rel.c_str(), fail_msg.c_str());
     ecg_destroy(ctx);
     ecg_input_free(in);
     return 1;
   }
-  Output w{out, in, c, n, 0};
   std::ofstream info(out + "infoCalcul.out", std::ios::trunc);
-  info.precision(17);
-  double dt = 1.e-15, t = 0.;
-  int32_t it = 0;
-  w.write(ctx);
-  info << w.file - 1 << " " << it << " " << t << " " << dt << "\n";
-  std::printf("T | %s: %lld cells, %s\n", rel.c_str(), (long long)n, c.time_iterations ? "iterations" : "physical time");
-  double next_print = time_freq;
+  if (precision != 0) info.precision(precision);
+  const std::clock_t clock0 = std::clock();
+  auto save_info = [&](double next_dt) {
+    double secs = (double)(std::clock() - clock0) / CLOCKS_PER_SEC;
+    info << w.file - 1 << " " << it << " " << t << " " << next_dt << " " << secs << " " << 0. << " " << 0. << std::endl;
+  };
+  if (restart > 0) {
+    for (auto& l : info_lines) info << l << std::endl;
+  } else {
+    info << 1 << std::endl;
+    w.write(ctx);
+    save_info(0.);  // the next dt is not known before the first step (printed as 0)
+  }
+  std::printf("T | %s: %lld cells, %s%s\n", rel.c_str(), (long long)n, c.time_iterations ? "iterations" : "physical time",
+              restart > 0 ? ", restarted" : "");
+  double next_print = t + time_freq;
   int rc = 0;
   for (bool finished = false; !finished;) {
     int32_t chunk = 1;
@@ -229,7 +416,7 @@ int run_case(const std::string& work, const std::string& rel) {
     }
     if (print) {
       w.write(ctx);
-      info << w.file - 1 << " " << it << " " << t << " " << dt << "\n";
+      save_info(dt);
       std::printf("T | iteration %d, t = %.6e s, dt = %.6e s, file %d\n", it, t, dt, w.file - 1);
     }
   }

@@ -111,11 +111,21 @@ ecg_status ecg_input_case(const ecg_input* in, ecg_case* out);
 const char* ecg_input_run_name(const ecg_input* in);
 /* Print control of main.xml: iterFreq (iteration mode) or timeFreq (physical-time mode). */
 ecg_status ecg_input_print_control(const ecg_input* in, int32_t* iter_freq, double* time_freq);
+/* Output and restart control of main.xml: <outputMode binary precision> (precision 0 = the stream
+ * default of 6 significant digits) and <restartSimulation restartFileNumber> (0 = no restart). */
+ecg_status ecg_input_output_control(const ecg_input* in, int32_t* binary, int32_t* precision, int32_t* restart_file);
 /* EOS file name of phase k (model.xml <EOS name>), used for output field names. */
 const char* ecg_input_eos_name(const ecg_input* in, int32_t k);
 /* Fills the initial primitive fields on the host, domain by domain in document order
  * (GeometricalDomain::fillIn src/Geometries/GeometricalDomain.cpp:64).  Field layout as above. */
 ecg_status ecg_input_fill(const ecg_input* in, double* const* fields, int64_t ncells);
+
+/* Completes fields read from a result file the way a restart does (Run::restartSimulation src/Run.cpp:345):
+ * Kapila: every phase takes the mixture pressure and is corrected (ModPUEq::fulfillStateRestart
+ * src/Models/PUEq/ModPUEq.cpp:76, PhaseUEq::verifyAndCorrectPhase), then the total energy is rebuilt
+ * (Cell::completeFulfillState src/Order1/Cell.cpp:344); Euler: the total energy only.  alpha_k and rho_k
+ * are corrected in place and E is overwritten; p and u are kept.  Host-only, no GPU work. */
+ecg_status ecg_restart_fill(const ecg_case* c, double* const* fields, int64_t ncells);
 
 /* ------------------------------------------------------------------ one case on one GPU */
 /* Creates a context on the current CUDA device: device state, stream, dt accumulator.

@@ -33,8 +33,12 @@ def _decode(payload: str) -> np.ndarray:
     return np.frombuffer(data[:nbytes], dtype="<f8").copy()
 
 
+_ASCII_RE = re.compile(r'<DataArray type="Float64" Name="([^"]+)"(?: NumberOfComponents="(\d)")? format="ascii">'
+                       r'([^<]*)</DataArray>')
+
+
 def read_vtr(path: str) -> Dict[str, np.ndarray]:
-    """Read every named Float64 cell array of one reference ``.vtr`` result file."""
+    """Read every named Float64 cell array of one reference ``.vtr`` result file (base64 or ASCII)."""
     with open(path) as f:
         txt = f.read()
     out: Dict[str, np.ndarray] = {}
@@ -43,7 +47,32 @@ def read_vtr(path: str) -> Dict[str, np.ndarray]:
         if ncomp:
             arr = arr.reshape(-1, int(ncomp))
         out[name] = arr
+    for name, ncomp, payload in _ASCII_RE.findall(txt):
+        arr = np.array([float(x) for x in payload.split()], dtype=np.float64)
+        if ncomp:
+            arr = arr.reshape(-1, int(ncomp))
+        out[name] = arr
     return out
+
+
+def read_vtr_ordered(path: str):
+    """(name, array) of every cell array in document order (the order a restart reads them in)."""
+    with open(path) as f:
+        txt = f.read()
+    body = txt[txt.index("<CellData>"):]
+    items = []
+    for m in re.finditer(r'<DataArray type="Float64" Name="([^"]+)"(?: NumberOfComponents="(\d)")? '
+                         r'format="(ascii|binary)">([^<]*)</DataArray>', body):
+        name, ncomp, fmt, payload = m.groups()
+        arr = _decode(payload.strip()) if fmt == "binary" else np.array([float(x) for x in payload.split()])
+        items.append((name, arr.reshape(-1, int(ncomp)) if ncomp else arr))
+    return items
+
+
+def result_file(work: str, run_name: str, number: int, binary: bool = True) -> str:
+    """Path of result file ``number`` (OutputXML::createFilenameXML: result[B64]_CPU0_TIME<k>.vtr)."""
+    return os.path.join(work, "results", run_name, "datasets",
+                        f"result{'B64' if binary else ''}_CPU0_TIME{number}.vtr")
 
 
 def available() -> bool:
