@@ -105,7 +105,7 @@ def lib():
     L.ecg_stream.argtypes = [vp]
     L.ecg_set_newton_cap.argtypes = [vp, C.c_int32]
     L.ecg_set_seed_model.argtypes = [vp, P(Mlp)]
-    L.ecg_record_pairs.argtypes = [vp, C.c_int64]
+    L.ecg_record_pairs.argtypes = [vp, C.c_int64, C.c_int32]
     L.ecg_fetch_pairs.argtypes = [vp, fp, fp, P(C.c_int64)]
     for name in ("ecg_trainer_create", "ecg_trainer_destroy", "ecg_trainer_epoch", "ecg_trainer_grad",
                  "ecg_trainer_forward", "ecg_trainer_export", "ecg_trainer_import", "ecg_trainer_set_norm",
@@ -282,8 +282,8 @@ class Context:
     def set_seed_model(self, mlp: Optional["Mlp"]):
         check(lib().ecg_set_seed_model(self.h, C.byref(mlp) if mlp is not None else None), "ecg_set_seed_model")
 
-    def record_pairs(self, max_pairs: int):
-        check(lib().ecg_record_pairs(self.h, max_pairs), "ecg_record_pairs")
+    def record_pairs(self, max_pairs: int, min_evals: int = 1):
+        check(lib().ecg_record_pairs(self.h, max_pairs, min_evals), "ecg_record_pairs")
 
     def fetch_pairs(self):
         cnt = C.c_int64(0)

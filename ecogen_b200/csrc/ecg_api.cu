@@ -94,12 +94,12 @@ struct ecg_ctx {
   DevStats* stats = nullptr;
   int cur = 0;
   int newton_cap = 100;
-  float* mlp = nullptr;
-  int mlp_nin = 0;
+  MlpDev* mlp = nullptr;
   float* rec_x = nullptr;
   float* rec_y = nullptr;
   unsigned long long* rec_count = nullptr;
   unsigned long long rec_max = 0;
+  int rec_min_evals = 1;
   double pcrit = 0.;
   Geometry geo{};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step sequences starting from state[0] / state[1]
@@ -172,11 +172,11 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   for (int i = 0; i < 4; i++) P.lim[i] = x->c.limiter[i];
   P.newton_cap = x->newton_cap;
   P.mlp = x->mlp;
-  P.mlp_nin = x->mlp_nin;
   P.rec_x = x->rec_x;
   P.rec_y = x->rec_y;
   P.rec_count = x->rec_count;
   P.rec_max = x->rec_max;
+  P.rec_min_evals = x->rec_min_evals;
   P.ptmu = x->c.ptmu;
   P.ptmu_liq = x->c.ptmu_liquid;
   P.ptmu_vap = x->c.ptmu_vapor;
@@ -277,6 +277,90 @@ void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
 }
 
 }  // namespace
+
+namespace ecg {
+
+// B fragments of the seed model's two hidden layers (layout of MlpDev, ecg_mlp_device.cuh).
+__global__ void k_mlp_pack(const float* __restrict__ W, int nin, MlpDev* out) {
+  const int H = MLP_H;
+  const float* w1 = W;
+  const float* b1 = w1 + H * nin;
+  const float* w2 = b1 + H;
+  const float* b2 = w2 + H * H;
+  const float* w3 = b2 + H;
+  const float* b3 = w3 + H;
+  const float* ish = b3 + 1;
+  const float* isc = ish + nin;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int i = tid; i < 8 * 32; i += nth) {
+    const int nt = i / 32, lane = i % 32, g = lane >> 2, t = lane & 3, n = 8 * nt + g;
+    auto word = [&](int j) {
+      const float lo = (2 * j < nin) ? w1[n * nin + 2 * j] : 0.f, hi = (2 * j + 1 < nin) ? w1[n * nin + 2 * j + 1] : 0.f;
+      return pack_bf16(lo, hi);
+    };
+    out->w1[nt][lane] = make_uint2(word(t), word(t + 4));
+  }
+  for (int i = tid; i < 8 * 4 * 32; i += nth) {
+    const int nt = i / 128, kc = (i / 32) % 4, lane = i % 32, g = lane >> 2, t = lane & 3, n = 8 * nt + g;
+    const int j0 = kc * 8 + t, j1 = j0 + 4;
+    out->w2[nt][kc][lane] = make_uint2(pack_bf16(w2[n * H + 2 * j0], w2[n * H + 2 * j0 + 1]),
+                                       pack_bf16(w2[n * H + 2 * j1], w2[n * H + 2 * j1 + 1]));
+  }
+  for (int i = tid; i < H; i += nth) {
+    out->b1[i] = b1[i];
+    out->b2[i] = b2[i];
+    out->w3[i] = w3[i];
+  }
+  for (int i = tid; i < 16; i += nth) {
+    out->ish[i] = i < nin ? ish[i] : 0.f;
+    out->isc[i] = i < nin ? isc[i] : 0.f;
+  }
+  if (tid == 0) {
+    out->b3 = b3[0];
+    out->osh = isc[nin];
+    out->osc = isc[nin + 1];
+    out->pad = 0.f;
+  }
+}
+
+cudaError_t mlp_install(const float* d_params, int nin, MlpDev* d_out, cudaStream_t stream) {
+  k_mlp_pack<<<4, 256, 0, stream>>>(d_params, nin, d_out);
+  return cudaGetLastError();
+}
+
+ecg_status mlp_upload(const ecg_mlp* m, int np, MlpDev** dev, cudaStream_t stream) {
+  if (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * np) {
+    set_error("seed model shape must be 3*nphases -> 64 -> 64 -> 1");
+    return ECG_ERR_INVALID;
+  }
+  const int nin = m->n_in, H = ECG_MLP_HIDDEN;
+  std::vector<float> pk((size_t)mlp_packed_size(nin));
+  float* q = pk.data();
+  std::memcpy(q, m->w1, sizeof(float) * H * nin); q += H * nin;
+  std::memcpy(q, m->b1, sizeof(float) * H); q += H;
+  std::memcpy(q, m->w2, sizeof(float) * H * H); q += H * H;
+  std::memcpy(q, m->b2, sizeof(float) * H); q += H;
+  std::memcpy(q, m->w3, sizeof(float) * H); q += H;
+  *q++ = m->b3;
+  for (int i = 0; i < nin; i++) *q++ = m->in_shift[i];
+  for (int i = 0; i < nin; i++) *q++ = m->in_scale[i];
+  *q++ = m->out_shift;
+  *q++ = m->out_scale;
+  float* tmp = nullptr;
+  cudaError_t e = cudaMalloc(&tmp, sizeof(float) * pk.size());
+  if (e == cudaSuccess && !*dev) e = cudaMalloc(dev, sizeof(MlpDev));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = mlp_install(tmp, nin, *dev, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) {
+    set_error(std::string("seed model upload: ") + cudaGetErrorString(e));
+    return ECG_ERR_CUDA;
+  }
+  return ECG_OK;
+}
+
+}  // namespace ecg
 
 extern "C" const char* ecg_status_str(ecg_status s) {
   switch (s) {
@@ -629,30 +713,13 @@ extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
     return ECG_OK;
   }
   if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
-  if (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * x->np) { set_error("seed model shape must be 3*nphases -> 64 -> 64 -> 1"); return ECG_ERR_INVALID; }
-  const int nin = m->n_in, H = ECG_MLP_HIDDEN;
-  std::vector<float> pk((size_t)mlp_packed_size(nin));
-  float* q = pk.data();
-  std::memcpy(q, m->w1, sizeof(float) * H * nin); q += H * nin;
-  std::memcpy(q, m->b1, sizeof(float) * H); q += H;
-  std::memcpy(q, m->w2, sizeof(float) * H * H); q += H * H;
-  std::memcpy(q, m->b2, sizeof(float) * H); q += H;
-  std::memcpy(q, m->w3, sizeof(float) * H); q += H;
-  *q++ = m->b3;
-  for (int i = 0; i < nin; i++) *q++ = m->in_shift[i];
-  for (int i = 0; i < nin; i++) *q++ = m->in_scale[i];
-  *q++ = m->out_shift;
-  *q++ = m->out_scale;
-  if (!x->mlp) ECG_CUDA(cudaMalloc(&x->mlp, sizeof(float) * pk.size()));
-  ECG_CUDA(cudaMemcpyAsync(x->mlp, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice, x->stream));
-  ECG_CUDA(cudaStreamSynchronize(x->stream));
-  x->mlp_nin = nin;
-  return ECG_OK;
+  return mlp_upload(m, x->np, &x->mlp, x->stream);
 }
 
-extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs) {
-  if (!x || max_pairs < 0) { set_error("bad argument"); return ECG_ERR_INVALID; }
+extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs, int32_t min_evals) {
+  if (!x || max_pairs < 0 || min_evals < 1) { set_error("bad argument"); return ECG_ERR_INVALID; }
   x->graph_dirty = true;
+  x->rec_min_evals = min_evals;
   cudaFree(x->rec_x);
   cudaFree(x->rec_y);
   cudaFree(x->rec_count);

@@ -65,7 +65,6 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
   double* sa0 = sq + (size_t)FL::NQ * RS;
   double* ssl = sq + (size_t)K::NQ * RS;
   double* sfl = ssl + (O2 ? (size_t)FL::NSL * SS : 0);
-  MlpSmem* smlp = reinterpret_cast<MlpSmem*>(sfl + (size_t)FL::NFL * FS);  // present when a seed model is set
   __shared__ int s_item;
   __shared__ double red[32];
   const StepParams& P = B.P;
@@ -73,10 +72,6 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
   const int tid = threadIdx.x;
   CellCounters total;
   unsigned int max_iters = 0;
-  if (P.mlp != nullptr) {
-    mlp_load(smlp, P.mlp, P.mlp_nin);
-    __syncthreads();
-  }
 
   for (;;) {
     if (tid == 0) s_item = (int)atomicAdd(B.queue, 1u);
@@ -193,12 +188,16 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
         boundary_face<NP, 1>(M, P.q, nn, cell, 0, false, C.lcfl, C.coefA, dtmax, an, pn, aa, am, ae, amom, aE);
       kapila_rebuild<NP, 1, PASS>(P, M, nn, cell, B.scal[c].dt, an, rn, pn, aa, am, ae, amom, aE, cp);
     }
-    double seed = 0.;
-    if (P.mlp != nullptr) seed = mlp_seed_warp<NP>(smlp, g < n, cp.a, cp.r, cp.pk);
+    SeedGate<NP> sg;
+    const bool seeded = P.mlp != nullptr;  // uniform over the launch
+    if (seeded) seed_gate<NP, 1>(P, M, g < n, cp, sg);
     if (g < n) {
       const int64_t cell = C.off + g;
       CellCounters cc;
-      kapila_finish<NP, 1, PASS, false>(P, M, nn, cell, cp, seed, P.mlp != nullptr, cc);
+      if (seeded)
+        kapila_finish<NP, 1, PASS, false, true>(P, M, nn, cell, cp, sg, cc);
+      else
+        kapila_finish<NP, 1, PASS, false, false>(P, M, nn, cell, cp, sg, cc);
       total.relax += cc.relax;
       total.iters += cc.iters;
       total.fallback += cc.fallback;
@@ -244,11 +243,11 @@ static cudaError_t batch_one(const BatchParams& B, const ecg_eos* eos, double ep
                              bool prepare, int* max_blocks) {
   auto kern = k_batch<NP, TB, PASS>;
   const size_t base = BatchTile<NP, TB, PASS>::smem_bytes();
-  const size_t sm = base + (B.P.mlp != nullptr ? sizeof(MlpSmem) : 0);
+  const size_t sm = base;
   if (prepare) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(base + sizeof(MlpSmem)));
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)base);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks, kern, TB, base + sizeof(MlpSmem));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_blocks, kern, TB, base);
   }
   Model<NP> M;
   for (int k = 0; k < NP; k++) M.eos[k] = make_eos_params(eos[k]);
@@ -304,8 +303,7 @@ struct ecg_batch {
   int grid = 0;
   int cur = 0;
   int newton_cap = 100;
-  float* mlp = nullptr;
-  int mlp_nin = 0;
+  MlpDev* mlp = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 };
 
@@ -376,7 +374,6 @@ ecg_status launch_pass(ecg_batch* b, int pass, double* q, double* sn, double* ou
   for (int i = 0; i < 4; i++) B.P.lim[i] = b->c0.limiter[i];
   B.P.newton_cap = b->newton_cap;
   B.P.mlp = b->mlp;
-  B.P.mlp_nin = b->mlp_nin;
   B.cases = b->cases;
   B.scal = b->scal;
   B.items = b->items;
@@ -649,27 +646,7 @@ extern "C" ecg_status ecg_batch_set_seed_model(ecg_batch* b, const ecg_mlp* m) {
     b->mlp = nullptr;
     return ECG_OK;
   }
-  if (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * b->np) {
-    set_error("seed model shape must be 3*nphases -> 64 -> 64 -> 1");
-    return ECG_ERR_INVALID;
-  }
-  const int nin = m->n_in, H = ECG_MLP_HIDDEN;
-  std::vector<float> pk((size_t)mlp_packed_size(nin));
-  float* q = pk.data();
-  std::memcpy(q, m->w1, sizeof(float) * H * nin); q += H * nin;
-  std::memcpy(q, m->b1, sizeof(float) * H); q += H;
-  std::memcpy(q, m->w2, sizeof(float) * H * H); q += H * H;
-  std::memcpy(q, m->b2, sizeof(float) * H); q += H;
-  std::memcpy(q, m->w3, sizeof(float) * H); q += H;
-  *q++ = m->b3;
-  for (int i = 0; i < nin; i++) *q++ = m->in_shift[i];
-  for (int i = 0; i < nin; i++) *q++ = m->in_scale[i];
-  *q++ = m->out_shift;
-  *q++ = m->out_scale;
-  if (!b->mlp) BCUDA(cudaMalloc(&b->mlp, sizeof(float) * pk.size()));
-  BCUDA(cudaMemcpy(b->mlp, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice));
-  b->mlp_nin = nin;
-  return ECG_OK;
+  return mlp_upload(m, b->np, &b->mlp, b->stream);
 }
 
 extern "C" ecg_status ecg_batch_set_shape(ecg_batch* b, int32_t tile, int32_t threads) {

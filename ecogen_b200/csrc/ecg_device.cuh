@@ -468,6 +468,99 @@ static __device__ __noinline__ double cr_log(double x) {
 
 // ------------------------------------------------------------------ relaxation (p-T-mu, 2 phases)
 
+// Pieces of the same relaxation for the seeded kernels, which gate the learned seed on the first
+// evaluation: a Newton state after k evaluations, one evaluation at an iterate (verifyAndModifyPressure
+// of every phase, then f = sum_k alpha_k rho_k / rho_k*(p) - 1 and its derivative) and the
+// interface-pressure fallback (RelaxationP::NewtonRaphson src/Relaxations/RelaxationP.cpp:43-68,
+// RelaxationPInfinite.cpp:43-97).  The arithmetic is relax_pinf's, operation for operation.
+struct NewtonState {
+  double ps, f, df;
+  int it;
+};
+
+template <int NP>
+__device__ __forceinline__ bool pinf_applies(const Model<NP>& M, const double a[NP]) {
+  if (M.eps > 1.e-20) {
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+      if (a[k] > (1. - 1.e-5)) return false;
+  }
+  return true;
+}
+
+template <int NP>
+__device__ __forceinline__ void pinf_eval(const Model<NP>& M, const double a[NP], const double r[NP], NewtonState& s,
+                                          const double p[NP], double aS[NP], double rS[NP]) {
+  double drhodp = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) s.ps = eos_fix_p(M.eos[k], s.ps);
+  s.f = -1.;
+  s.df = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    rS[k] = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], s.ps, &drhodp);
+    aS[k] = a[k] * r[k] / rS[k];
+    double dalpha = a[k] * r[k] * drhodp / (rS[k] * rS[k]);
+    s.f += aS[k];
+    s.df -= dalpha;
+  }
+}
+
+// First evaluation at the plain start sum_k alpha_k p_k (relax_pinf's first iteration).
+template <int NP>
+__device__ __forceinline__ void pinf_first(const Model<NP>& M, const double a[NP], const double r[NP],
+                                           const double p[NP], NewtonState& s, double aS[NP], double rS[NP]) {
+  double ps = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) ps += a[k] * p[k];
+  s.ps = ps - 0. / 1.;
+  s.it = 1;
+  pinf_eval<NP>(M, a, r, s, p, aS, rS);
+}
+
+// Continues from state s to |f| <= 1e-10 or the cap; relaxes a, r like relax_pinf.
+template <int NP>
+__device__ __forceinline__ void pinf_finish(const Model<NP>& M, double a[NP], double r[NP], const double p[NP],
+                                            NewtonState s, double aS[NP], double rS[NP], double& pstar, RelaxStats& st,
+                                            int max_iter) {
+  while (fabs(s.f) > 1e-10 && s.it < max_iter) {
+    s.it++;
+    s.ps -= s.f / s.df;
+    pinf_eval<NP>(M, a, r, s, p, aS, rS);
+  }
+  st.iters = s.it;
+  if (s.it < max_iter) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) { a[k] = aS[k]; r[k] = rS[k]; }
+    pstar = s.ps;
+    return;
+  }
+  st.fallback = true;
+  double drhodp = 0.;
+  double zk[NP], pI = 0., sumZk = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) zk[k] = r[k] * eos_c(M.eos[k], M.eps, r[k], p[k]);
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    sumZk += zk[k];
+    double sumZj = 0.;
+#pragma unroll
+    for (int j = 0; j < NP; j++)
+      if (j != k) sumZj += zk[j];
+    pI += sumZj * (p[k] - 0.);
+  }
+  pI /= sumZk * (NP - 1);
+#pragma unroll
+  for (int k = 0; k < NP; k++) pI = eos_fix_p(M.eos[k], pI);
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double rr = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], pI, &drhodp);
+    a[k] = a[k] * r[k] / rr;
+    r[k] = rr;
+  }
+  pstar = pI;
+}
+
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
 __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
                                                bool& err) {

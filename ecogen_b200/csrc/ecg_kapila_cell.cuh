@@ -298,11 +298,38 @@ __device__ __forceinline__ void kapila_rebuild(const StepParams& P, const Model<
 }
 
 
-// Relaxations, energy correction, clamps and store of one rebuilt cell.  seed / use_seed: learned
-// initial guess of the pressure relaxation (see ecg_mlp_device.cuh).
-template <int NP, int DIM, int PASS, bool PTMU>
+// The learned seed of a seeded kernel, gated on the plain start: the first Newton evaluation at
+// sum_k alpha_k p_k is made for every cell (the plain iteration's first step); only cells it leaves
+// unconverged ("hard") take the network's seed, which the warp evaluates when any of its lanes needs it.
+template <int NP>
+struct SeedGate {
+  NewtonState ns;        // state after the first evaluation
+  double aS[NP], rS[NP];
+  double seed;
+  bool applies, hard;
+};
+
+// First evaluation and the warp-wide seed (all lanes of the warp call it; `active` marks a cell).
+template <int NP, int DIM>
+__device__ __forceinline__ void seed_gate(const StepParams& P, const Model<NP>& M, bool active,
+                                          const CellPrim<NP, DIM>& cp, SeedGate<NP>& g) {
+  g.applies = active && pinf_applies<NP>(M, cp.a);
+  g.hard = false;
+  if (g.applies) {
+    pinf_first<NP>(M, cp.a, cp.r, cp.pk, g.ns, g.aS, g.rS);
+    g.hard = fabs(g.ns.f) > 1e-10 && g.ns.it < P.newton_cap;
+  }
+  g.seed = 0.;
+  if (__any_sync(0xffffffffu, g.hard)) g.seed = mlp_seed_warp<NP>(P.mlp, g.hard, cp.a, cp.r, cp.pk);
+}
+
+// Relaxations, energy correction, clamps and store of one rebuilt cell.  SEED: the pressure
+// relaxation continues from the seed gate (see seed_gate); a hard cell restarts Newton from the
+// network's seed when it is finite and inside the bracket of the phase pressures, otherwise it
+// continues the plain iteration.  Newton still stops at |f| <= 1e-10 either way.
+template <int NP, int DIM, int PASS, bool PTMU, bool SEED = false>
 __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
-                                              CellPrim<NP, DIM>& cp, double seed, bool use_seed, CellCounters& cc) {
+                                              CellPrim<NP, DIM>& cp, const SeedGate<NP>& g, CellCounters& cc) {
   using FL = Fields<NP, DIM>;
   double* a = cp.a;
   double* r = cp.r;
@@ -316,11 +343,39 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
 #pragma unroll
   for (int k = 0; k < NP; k++) { a0[k] = a[k]; r0[k] = r[k]; p0[k] = pk[k]; }
   double pstar = 0.;
-  bool relaxed = relax_pinf<NP>(M, a, r, pk, pstar, rs, seed, use_seed, P.newton_cap);
+  bool relaxed;
+  if (SEED) {
+    rs.iters = 0;
+    rs.fallback = rs.seeded = rs.rejected = false;
+    relaxed = g.applies;
+    if (relaxed) {
+      NewtonState s = g.ns;
+      double aS[NP], rS[NP];
+#pragma unroll
+      for (int k = 0; k < NP; k++) { aS[k] = g.aS[k]; rS[k] = g.rS[k]; }
+      if (g.hard) {
+        double lo = pk[0], hi = pk[0];
+#pragma unroll
+        for (int k = 1; k < NP; k++) { lo = dmin(lo, pk[k]); hi = dmax(hi, pk[k]); }
+        if (isfinite(g.seed) && g.seed >= lo && g.seed <= hi) {
+          s.ps = g.seed - 0. / 1.;
+          s.it += 1;
+          pinf_eval<NP>(M, a, r, s, pk, aS, rS);
+          rs.seeded = true;
+        } else {
+          rs.rejected = true;
+        }
+      }
+      pinf_finish<NP>(M, a, r, pk, s, aS, rS, pstar, rs, P.newton_cap);
+    }
+  } else {
+    relaxed = relax_pinf<NP>(M, a, r, pk, pstar, rs, 0., false, P.newton_cap);
+  }
   if (relaxed) {
 #pragma unroll
     for (int k = 0; k < NP; k++) pk[k] = pstar;
-    if (P.rec_x != nullptr && !rs.fallback) record_pair<NP>(P.rec_x, P.rec_y, P.rec_count, P.rec_max, a0, r0, p0, pstar);
+    if (P.rec_x != nullptr && !rs.fallback && rs.iters >= P.rec_min_evals)
+      record_pair<NP>(P.rec_x, P.rec_y, P.rec_count, P.rec_max, a0, r0, p0, pstar);
   }
   if (PTMU) {
     // mixture internal energy of the rebuilt state (MixUEq::computeMixtureVariables :136), which

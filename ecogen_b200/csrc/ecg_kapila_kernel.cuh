@@ -54,7 +54,6 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
   double* sa0 = sq + (size_t)FL::NQ * RS;                  // [NA0][RS]
   double* ssl = sa0 + (size_t)K::NA0 * RS;                 // [NSL][SS]
   double* sfl = ssl + (K::O2 ? (size_t)FL::NSL * SS : 0);  // [NFL][FS]
-  MlpSmem* smlp = reinterpret_cast<MlpSmem*>(sfl + (size_t)FL::NFL * FS);  // present when a seed model is set
 
   if (*P.done) return;  // stop condition reached earlier in a captured step sequence
   const int tid = threadIdx.x;
@@ -88,7 +87,6 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
   double wallp[DIM];  // normal momentum flux of the cell's symmetry sides, per axis
 #pragma unroll
   for (int d = 0; d < DIM; d++) wallp[d] = 0.;
-  if (SEED) mlp_load(smlp, P.mlp, P.mlp_nin);  // visible after the first barrier below
 
 #pragma unroll
   for (int ax = 0; ax < DIM; ax++) {
@@ -259,10 +257,10 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
 
     kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
   }
-  // learned seed of the pressure relaxation: one warp-wide tensor-core evaluation (all lanes)
-  double seed = 0.;
-  if (SEED) seed = mlp_seed_warp<NP>(smlp, active, cp.a, cp.r, cp.pk);
-  if (active) kapila_finish<NP, DIM, PASS, PTMU>(P, M, nn, cell, cp, seed, SEED, cc);
+  // learned seed of the pressure relaxation, gated on the plain start (all lanes of the warp)
+  SeedGate<NP> sg;
+  if (SEED) seed_gate<NP, DIM>(P, M, active, cp, sg);
+  if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED>(P, M, nn, cell, cp, sg, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
 
   // ---- dtMax: block min, one atomic per block

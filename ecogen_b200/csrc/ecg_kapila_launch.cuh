@@ -11,7 +11,7 @@ cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eo
   using K = KapilaStep<NP, DIM, PASS>;
   using TS = TileShape<DIM>;
   auto kern = k_kapila_step<NP, DIM, PASS, PTMU, SEED>;
-  const size_t sm = K::smem_bytes() + (SEED ? sizeof(MlpSmem) : 0);
+  const size_t sm = K::smem_bytes();
   if (prepare) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;

@@ -54,55 +54,25 @@ __device__ __forceinline__ void record_pair(float* rx, float* ry, unsigned long 
 }
 
 // ----------------------------------------------------------------------------------------------
-// Warp-level evaluation with BF16 tensor-core MMA (mma.sync m16n8k16, FP32 accumulation) and the
-// weights held in shared memory as BF16.  The 32 lanes of a warp form a 32 x 16 feature matrix
-// (inputs padded to 16); layer 1 is 2 x 8 MMAs, layer 2 is 2 x 8 x 4 MMAs, the 64 -> 1 output is
-// a dot product over the accumulator fragments reduced across each lane quad.  The accumulator
-// fragment of an m16n8 tile is, register for register, the A fragment of the next layer's k16
-// slice, so layer outputs never leave registers.  Every lane of the warp must call it.
+// Warp-level evaluation with BF16 tensor-core MMA (mma.sync m16n8k16, FP32 accumulation).  The 32
+// lanes of a warp form a 32 x 16 feature matrix (inputs padded to 16), gathered into A fragments by
+// warp shuffles; layer 1 is 2 x 8 MMAs, layer 2 is 2 x 8 x 4 MMAs, the 64 -> 1 output is a dot
+// product over the accumulator fragments reduced across each lane quad.  The accumulator fragment
+// of an m16n8 tile is, register for register, the A fragment of the next layer's k16 slice, so
+// layer outputs never leave registers.  The weights are read as ready-made BF16 B fragments from
+// an installed model (MlpDev, about 11 KB, L1-resident), so the kernels keep no shared memory for
+// them.  Every lane of the warp must call mlp_seed_warp.
 
-constexpr int MLP_WARPS = 8;  // warps per block that may call mlp_seed_warp (blocks of <= 256 threads)
-
-struct MlpSmem {
-  __nv_bfloat16 w1[MLP_H][16];
-  __nv_bfloat16 w2[MLP_H][MLP_H];
+// Device form of an installed seed model, built once by mlp_install (ecg_api.cu) from the packed
+// FP32 parameters: w1[n-tile][lane] and w2[n-tile][k-chunk][lane] are the two 32-bit words of each
+// lane's B fragment (bf16 pairs of a weight row, rounded to nearest even).
+struct MlpDev {
+  uint2 w1[8][32];
+  uint2 w2[8][4][32];
   float b1[MLP_H], b2[MLP_H], w3[MLP_H];
-  float b3, osh, osc, pad;
   float ish[16], isc[16];
-  __nv_bfloat16 xs[MLP_WARPS][32][16];
-  float ys[MLP_WARPS][32];
+  float b3, osh, osc, pad;
 };
-
-// Cooperative load of the packed FP32 parameters into shared memory (all threads of the block).
-__device__ __forceinline__ void mlp_load(MlpSmem* S, const float* __restrict__ W, int nin) {
-  const float* w1 = W;
-  const float* b1 = w1 + MLP_H * nin;
-  const float* w2 = b1 + MLP_H;
-  const float* b2 = w2 + MLP_H * MLP_H;
-  const float* w3 = b2 + MLP_H;
-  const float* b3 = w3 + MLP_H;
-  const float* ish = b3 + 1;
-  const float* isc = ish + nin;
-  for (int i = threadIdx.x; i < MLP_H * 16; i += blockDim.x) {
-    int o = i / 16, k = i % 16;
-    S->w1[o][k] = __float2bfloat16_rn(k < nin ? w1[o * nin + k] : 0.f);
-  }
-  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) S->w2[i / MLP_H][i % MLP_H] = __float2bfloat16_rn(w2[i]);
-  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
-    S->b1[i] = b1[i];
-    S->b2[i] = b2[i];
-    S->w3[i] = w3[i];
-  }
-  for (int i = threadIdx.x; i < 16; i += blockDim.x) {
-    S->ish[i] = i < nin ? ish[i] : 0.f;
-    S->isc[i] = i < nin ? isc[i] : 0.f;
-  }
-  if (threadIdx.x == 0) {
-    S->b3 = b3[0];
-    S->osh = isc[nin];
-    S->osc = isc[nin + 1];
-  }
-}
 
 __device__ __forceinline__ unsigned int pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -117,38 +87,56 @@ __device__ __forceinline__ void mma_bf16(float d[4], const unsigned int a[4], un
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Returns the seed for this lane's cell (valid lanes), NaN for lanes without a cell.
+// Returns the seed for this lane's cell (lanes with `valid`), NaN for the other lanes.
 template <int NP>
-__device__ __forceinline__ double mlp_seed_warp(MlpSmem* S, bool valid, const double a[NP], const double r[NP],
-                                                const double p[NP]) {
+__device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bool valid, const double a[NP],
+                                                const double r[NP], const double p[NP]) {
   constexpr int NI = 3 * NP;
-  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5) % MLP_WARPS;
+  static_assert(NI <= 16, "inputs padded to one k16 slice");
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  float x[NI];
-  if (valid) mlp_features<NP>(a, r, p, x);
+  float xn[NI];
+  if (valid) {
+    float x[NI];
+    mlp_features<NP>(a, r, p, x);
 #pragma unroll
-  for (int i = 0; i < 16; i++) {
-    float v = (valid && i < NI) ? (x[i < NI ? i : 0] - S->ish[i]) * S->isc[i] : 0.f;
-    S->xs[warp][lane][i] = __float2bfloat16_rn(v);
+    for (int i = 0; i < NI; i++) xn[i] = (x[i] - __ldg(&W->ish[i])) * __ldg(&W->isc[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NI; i++) xn[i] = 0.f;
   }
-  __syncwarp();
-  const unsigned int* xw = reinterpret_cast<const unsigned int*>(&S->xs[warp][0][0]);  // 8 words per row
-  const unsigned int* w1w = reinterpret_cast<const unsigned int*>(&S->w1[0][0]);      // 8 words per row
-  const unsigned int* w2w = reinterpret_cast<const unsigned int*>(&S->w2[0][0]);      // 32 words per row
-  float out_lo[2], out_hi[2];
+  float out[4];  // row sums: tile 0 rows g, g+8; tile 1 rows g, g+8 (complete on lanes with t == 0)
 #pragma unroll
   for (int m = 0; m < 2; m++) {
-    const int r0 = 16 * m + g, r1 = r0 + 8;
-    unsigned int A1[4] = {xw[r0 * 8 + t], xw[r1 * 8 + t], xw[r0 * 8 + t + 4], xw[r1 * 8 + t + 4]};
+    // A fragment of rows (16m + g, 16m + g + 8), columns (2t, 2t+1) and (2t+8, 2t+9)
+    float v[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int src = 16 * m + g + 8 * h;
+#pragma unroll
+      for (int q = 0; q < 4; q++) v[h][q] = 0.f;
+#pragma unroll
+      for (int i = 0; i < NI; i++) {
+        const float xi = __shfl_sync(FULL, xn[i], src);
+        if (i == 2 * t) v[h][0] = xi;
+        if (i == 2 * t + 1) v[h][1] = xi;
+        if (i == 2 * t + 8) v[h][2] = xi;
+        if (i == 2 * t + 9) v[h][3] = xi;
+      }
+    }
+    unsigned int A1[4] = {pack_bf16(v[0][0], v[0][1]), pack_bf16(v[1][0], v[1][1]), pack_bf16(v[0][2], v[0][3]),
+                          pack_bf16(v[1][2], v[1][3])};
     unsigned int A2[4][4];
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
       float c[4] = {0.f, 0.f, 0.f, 0.f};
-      const int n = 8 * nt + g;
-      mma_bf16(c, A1, w1w[n * 8 + t], w1w[n * 8 + t + 4]);
+      const uint2 b = __ldg(&W->w1[nt][lane]);
+      mma_bf16(c, A1, b.x, b.y);
       const int col = 8 * nt + 2 * t;
-      unsigned int lo = pack_bf16(gelu_f(c[0] + S->b1[col]), gelu_f(c[1] + S->b1[col + 1]));
-      unsigned int hi = pack_bf16(gelu_f(c[2] + S->b1[col]), gelu_f(c[3] + S->b1[col + 1]));
+      const float2 bb = __ldg(reinterpret_cast<const float2*>(&W->b1[col]));
+      unsigned int lo = pack_bf16(gelu_f(c[0] + bb.x), gelu_f(c[1] + bb.y));
+      unsigned int hi = pack_bf16(gelu_f(c[2] + bb.x), gelu_f(c[3] + bb.y));
       const int kc = nt >> 1;
       if ((nt & 1) == 0) {
         A2[kc][0] = lo;
@@ -162,32 +150,36 @@ __device__ __forceinline__ double mlp_seed_warp(MlpSmem* S, bool valid, const do
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
       float c[4] = {0.f, 0.f, 0.f, 0.f};
-      const int n = 8 * nt + g;
 #pragma unroll
-      for (int kc = 0; kc < 4; kc++) mma_bf16(c, A2[kc], w2w[n * 32 + kc * 8 + t], w2w[n * 32 + kc * 8 + t + 4]);
+      for (int kc = 0; kc < 4; kc++) {
+        const uint2 b = __ldg(&W->w2[nt][kc][lane]);
+        mma_bf16(c, A2[kc], b.x, b.y);
+      }
       const int col = 8 * nt + 2 * t;
-      sum_lo += S->w3[col] * gelu_f(c[0] + S->b2[col]) + S->w3[col + 1] * gelu_f(c[1] + S->b2[col + 1]);
-      sum_hi += S->w3[col] * gelu_f(c[2] + S->b2[col]) + S->w3[col + 1] * gelu_f(c[3] + S->b2[col + 1]);
+      const float2 b2 = __ldg(reinterpret_cast<const float2*>(&W->b2[col]));
+      const float2 w3 = __ldg(reinterpret_cast<const float2*>(&W->w3[col]));
+      sum_lo += w3.x * gelu_f(c[0] + b2.x) + w3.y * gelu_f(c[1] + b2.y);
+      sum_hi += w3.x * gelu_f(c[2] + b2.x) + w3.y * gelu_f(c[3] + b2.y);
     }
 #pragma unroll
     for (int o = 1; o < 4; o <<= 1) {
-      sum_lo += __shfl_xor_sync(0xffffffffu, sum_lo, o);
-      sum_hi += __shfl_xor_sync(0xffffffffu, sum_hi, o);
+      sum_lo += __shfl_xor_sync(FULL, sum_lo, o);
+      sum_hi += __shfl_xor_sync(FULL, sum_hi, o);
     }
-    out_lo[m] = sum_lo;
-    out_hi[m] = sum_hi;
+    out[2 * m] = sum_lo;
+    out[2 * m + 1] = sum_hi;
   }
-  if (t == 0) {
-    S->ys[warp][g] = out_lo[0];
-    S->ys[warp][g + 8] = out_hi[0];
-    S->ys[warp][16 + g] = out_lo[1];
-    S->ys[warp][24 + g] = out_hi[1];
+  // row `lane` of the 32 x 1 output: tile lane / 16, row lane % 16 held by lane 4 * (lane % 8)
+  const int src = 4 * (lane & 7), sel = lane >> 3;
+  float y = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float v = __shfl_sync(FULL, out[q], src);
+    if (q == sel) y = v;
   }
-  __syncwarp();
-  float y = S->ys[warp][lane] + S->b3;
-  __syncwarp();
   if (!valid) return __longlong_as_double(0x7ff8000000000000LL);
-  double tt = (double)(y * S->osc + S->osh);
+  y += __ldg(&W->b3);
+  double tt = (double)(y * __ldg(&W->osc) + __ldg(&W->osh));
   double lo = p[0], hi = p[0];
 #pragma unroll
   for (int k = 1; k < NP; k++) {
@@ -197,5 +189,10 @@ __device__ __forceinline__ double mlp_seed_warp(MlpSmem* S, bool valid, const do
   tt = tt < 0. ? 0. : (tt > 1. ? 1. : tt);
   return lo + tt * (hi - lo);
 }
+
+// Builds the device form of a model from the packed FP32 parameters (see the top of this file).
+cudaError_t mlp_install(const float* d_params, int nin, MlpDev* d_out, cudaStream_t stream);
+// Checks, packs and installs an ABI model into *dev (allocated on first use); synchronous.
+ecg_status mlp_upload(const ecg_mlp* m, int np, MlpDev** dev, cudaStream_t stream);
 
 }  // namespace ecg

@@ -103,13 +103,14 @@ struct StepParams {
   int lim[4];
   int newton_cap;
   // learned seed (optional)
-  const float* mlp;     // packed weights (nullptr = plain start)
-  int mlp_nin;
-  // recording of (features, converged pressure) pairs
+  const struct MlpDev* mlp;  // installed model (nullptr = plain start)
+  // recording of (features, converged pressure) pairs of relaxations with at least rec_min_evals
+  // Newton evaluations
   float* rec_x;
   float* rec_y;
   unsigned long long* rec_count;
   unsigned long long rec_max;
+  int rec_min_evals;
   // p-T-mu relaxation
   int ptmu, ptmu_liq, ptmu_vap;
   double pcrit;

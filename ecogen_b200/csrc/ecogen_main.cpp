@@ -17,6 +17,7 @@
 #include <sys/stat.h>
 
 #include <cerrno>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -186,6 +187,56 @@ std::string result_name(bool binary, int file) {  // OutputXML::createFilenameXM
   return std::string("result") + (binary ? "B64" : "") + "_CPU0_TIME" + std::to_string(file) + ".vtr";
 }
 
+// |grad rho| of the mixture density by GradientFiniteDifference::computeGradients
+// (src/Gradients/GradientFiniteDifference.cpp:46-130, the default gradient method) as
+// Cell::getDensityGradient (src/Order1/Cell.cpp:627) evaluates it for the output: each internal face
+// of a cell adds n * (rho_R - rho_L) / |x_R - x_L| * |component distance| in the cell's face order
+// (x faces, y faces, z faces; minus side first), boundary faces only add twice their centre-to-face
+// distance to the normalising sums.
+std::vector<double> grad_rho(const ecg_case& c, const std::vector<double>& rho) {
+  const int nx = c.ncells[0], ny = c.ncells[1], nz = c.ncells[2];
+  const int64_t n = (int64_t)nx * ny * nz;
+  const int nn[3] = {nx, ny, nz};
+  double d[3], bm[3], bp[3];
+  for (int a = 0; a < 3; a++) {
+    d[a] = c.length[a] / (double)nn[a];
+    const double p0 = (0 + 0.5) * d[a], pl = (nn[a] - 1 + 0.5) * d[a];
+    bm[a] = std::fabs(p0 - 0.) * 2.;               // Xm face at 0
+    bp[a] = std::fabs(pl - (pl + 0.5 * d[a])) * 2.;  // Xp face at the last centre + d / 2
+  }
+  std::vector<double> g((size_t)n);
+  const int64_t stride[3] = {1, nx, (int64_t)nx * ny};
+  for (int64_t i = 0; i < n; i++) {
+    const int ijk[3] = {(int)(i % nx), (int)((i / nx) % ny), (int)(i / ((int64_t)nx * ny))};
+    double gr[3] = {0., 0., 0.}, sum[3] = {0., 0., 0.};
+    for (int a = 0; a < 3; a++) {
+      if (nn[a] == 1) continue;
+      for (int side = 0; side < 2; side++) {  // face with the previous cell, then with the next one
+        const int o = side ? ijk[a] + 1 : ijk[a] - 1;
+        if (o < 0 || o >= nn[a]) continue;
+        const int64_t L = side ? i : i - stride[a], R = side ? i + stride[a] : i;
+        const int iL = side ? ijk[a] : o, iR = side ? o : ijk[a];
+        const double xL = (iL + 0.5) * d[a], xR = (iR + 0.5) * d[a];
+        const double dist_a = std::fabs(xL - xR);
+        const double dist = std::sqrt((xL - xR) * (xL - xR) + 0. * 0. + 0. * 0.);
+        sum[a] += dist_a;
+        const double gf = (rho[R] - rho[L]) / dist;
+        for (int b = 0; b < 3; b++) gr[b] = gr[b] + (b == a ? 1. : 0.) * gf * (b == a ? dist_a : 0.);
+      }
+    }
+    for (int a = 0; a < 3; a++) {  // boundary faces: Xm, Xp, Ym, Yp, Zm, Zp
+      if (nn[a] == 1) continue;
+      if (ijk[a] == 0) sum[a] += bm[a];
+      if (ijk[a] == nn[a] - 1) sum[a] += bp[a];
+    }
+    for (int a = 0; a < 3; a++)
+      if (sum[a] <= 1.e-12) sum[a] = 1.;
+    const double x = gr[0] / sum[0], y = gr[1] / sum[1], z = gr[2] / sum[2];
+    g[i] = std::sqrt(x * x + y * y + z * z);
+  }
+  return g;
+}
+
 struct Output {
   std::string dir;
   const ecg_input* in;
@@ -231,6 +282,7 @@ struct Output {
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 + d][i];
       write_array(o, "F0_Velocity_" + e, u, 3, binary);
+      write_array(o, "gradRho", grad_rho(c, f[0]), 1, binary);
     } else {
       for (int k = 0; k < np; k++) {  // PhasePUEq scalars (src/Models/PUEq/PhasePUEq.cpp:60-110)
         std::string e = strip_xml(ecg_input_eos_name(in, k));
@@ -256,6 +308,7 @@ struct Output {
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 * np + 1 + d][i];
       write_array(o, "Velocity_Mixture", u, 3, binary);
+      write_array(o, "gradRho", grad_rho(c, rho), 1, binary);
     }
     o << "      </CellData>\n    </Piece>\n  </RectilinearGrid>\n</VTKFile>\n";
     return (bool)o;

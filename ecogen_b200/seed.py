@@ -5,9 +5,11 @@
    position of the relaxed pressure inside the bracket of the phase pressures.
 2. ``train``: fit the 3N -> 64 -> 64 -> 1 GELU MLP with the library's own CUDA training kernels
    (forward, backward and AdamW in ecg_mlp_train.cu).
-3. ``SeedModel.install(ctx)``: copy the weights into a context; the step kernels then evaluate the
-   network with BF16 tensor-core MMA inside the fused update and start Newton from its output.
-   Newton still iterates to |f| <= 1e-10, so the plain iteration stays the judge of convergence.
+3. ``SeedModel.install(ctx)``: copy the weights into a context; the step kernels then make the
+   plain first Newton evaluation for every cell and, in warps where it leaves a cell unconverged,
+   evaluate the network with BF16 tensor-core MMA inside the fused update and restart those cells
+   from its output.  Newton still iterates to |f| <= 1e-10, so the plain iteration stays the judge
+   of convergence.
 """
 from __future__ import annotations
 
@@ -63,12 +65,13 @@ def make_model(w1, b1, w2, b2, w3, b3, in_shift, in_scale, out_shift, out_scale)
     return SeedModel(m, arrays)
 
 
-def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000, warm: int = 0
+def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000, warm: int = 0, min_evals: int = 2
            ) -> Tuple[np.ndarray, np.ndarray]:
     """Run each case on the GPU and collect (features, target) pairs of its relaxations.
 
-    Each case first runs `warm` steps unrecorded, then records during `steps` steps; the pair
-    budget is shared evenly between the cases.
+    Each case first runs `warm` steps unrecorded, then records during `steps` steps the
+    relaxations that took at least `min_evals` Newton evaluations (the seeded kernels ask the
+    network only for those); the pair budget is shared evenly between the cases.
     """
     xs, ys = [], []
     per_case = max(1, max_pairs // max(1, len(case_specs)))
@@ -80,7 +83,7 @@ def record(case_specs: Sequence, steps: int, max_pairs: int = 2_000_000, warm: i
             ctx.upload(inp.fill())
             if warm:
                 ctx.step(warm)
-            ctx.record_pairs(per_case)
+            ctx.record_pairs(per_case, min_evals)
             ctx.step(steps)
             x, y = ctx.fetch_pairs()
             ctx.close()

@@ -202,11 +202,15 @@ typedef struct {
   float in_shift[ECG_MLP_MAX_IN], in_scale[ECG_MLP_MAX_IN]; /* feature normalisation */
   float out_shift, out_scale;   /* target de-normalisation */
 } ecg_mlp;
-/* Installs (copies) the weights; NULL restores the plain start sum_k alpha_k p_k. */
+/* Installs (copies) the weights; NULL restores the plain start sum_k alpha_k p_k.  With a model the
+ * step makes the plain iteration's first Newton evaluation for every cell and starts the cells it
+ * leaves unconverged again from the network's seed (kept only when finite and inside the bracket of
+ * the phase pressures); Newton still stops at |f| <= 1e-10. */
 ecg_status ecg_set_seed_model(ecg_ctx* ctx, const ecg_mlp* mlp);
 /* Records up to max_pairs (features, converged pressure) pairs from the relaxations of the next
- * ecg_step calls into an internal device buffer; ecg_fetch_pairs copies them out. */
-ecg_status ecg_record_pairs(ecg_ctx* ctx, int64_t max_pairs);
+ * ecg_step calls that took at least min_evals Newton evaluations (1 = all) into an internal device
+ * buffer; ecg_fetch_pairs copies them out. */
+ecg_status ecg_record_pairs(ecg_ctx* ctx, int64_t max_pairs, int32_t min_evals);
 ecg_status ecg_fetch_pairs(ecg_ctx* ctx, float* features, float* targets, int64_t* count);
 
 /* ------------------------------------------------------------------ MLP training on the GPU */

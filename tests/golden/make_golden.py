@@ -91,7 +91,9 @@ def main():
             raise SystemExit(f"{key}: reference failed\n{r.stdout[-3000:]}")
         files = refrun.result_files(w, c.name)
         f0 = refrun.reference_prim(refrun.read_vtr(files[0]), c.nphases)
-        f1 = refrun.reference_prim(refrun.read_vtr(files[-1]), c.nphases)
+        raw1 = refrun.read_vtr(files[-1])
+        f1 = refrun.reference_prim(raw1, c.nphases)
+        f1["gradRho"] = raw1.get("gradRho")
         it, t, dt = refrun.info(w, c.name)
         arrays = {}
         for tag, f in (("init", f0), ("final", f1)):

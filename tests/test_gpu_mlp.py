@@ -60,7 +60,8 @@ def test_seeded_relaxation_same_residual_fewer_iterations(tmp_path):
     test_case = cases.cavity_collapse_3d(n=24, iterations=6, seed=999, ninclusions=10, radius_cells=(2.0, 5.0))
     plain, st0 = _run(test_case, tmp_path / "plain")
     seeded, st1 = _run(test_case, tmp_path / "seeded", model)
-    assert st1.seeded + st1.seed_rejected == st1.relax_calls
+    # the network is asked only for cells the plain first evaluation leaves unconverged
+    assert 0 < st1.seeded + st1.seed_rejected < st1.relax_calls
     assert st1.newton_fallback == 0
     # same residual: Newton stops at |f| <= 1e-10 from either start, so fields agree to that level
     for name in ("alpha", "rho", "p", "E"):

@@ -118,9 +118,12 @@ def test_driver_writes_reference_results(key, golden_cases, tmp_path):
     assert r.returncode == 0, r.stderr
     files = refrun.result_files(str(tmp_path), case.name)
     assert len(files) >= 2
-    got = refrun.reference_prim(refrun.read_vtr(files[-1]), case.nphases)
+    raw = refrun.read_vtr(files[-1])
+    got = refrun.reference_prim(raw, case.nphases)
     for name in ("alpha", "rho", "p", "u", "E"):
         ref = g.get("final_" + name)
         if ref is None or got.get(name) is None:
             continue
         assert rel_l1(got[name], ref) <= TOL, name
+    # |grad rho| of the output (finite differences of the density: differences amplify the 1e-12)
+    assert rel_l1(raw["gradRho"], g["final_gradRho"]) <= 1e-9
