@@ -39,7 +39,7 @@ class Case(C.Structure):
                 ("limiter", C.c_int32 * 4), ("ncells", C.c_int32 * 3), ("length", C.c_double * 3),
                 ("cfl", C.c_double), ("time_iterations", C.c_int32), ("max_iterations", C.c_int32),
                 ("total_time", C.c_double), ("ptmu", C.c_int32), ("ptmu_liquid", C.c_int32),
-                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6)]
+                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6), ("ntransports", C.c_int32)]
 
 
 class StepStats(C.Structure):
@@ -152,7 +152,7 @@ def _field_ptrs(arrs: Sequence[np.ndarray]):
 
 
 def nfields(case: Case) -> int:
-    return 6 if case.model == MODEL_EULER else 2 * case.nphases + 5
+    return (6 if case.model == MODEL_EULER else 2 * case.nphases + 5) + case.ntransports
 
 
 def case_from_spec(spec) -> Case:
@@ -182,6 +182,7 @@ def case_from_spec(spec) -> Case:
         c.eos[k] = Eos(EOS_CODE[e.kind], e.gamma, e.pinf, e.b, e.cv, e.eref, e.sref)
     for i, b in enumerate(spec.boundary_types()):
         c.bc[i] = BC_CODE[b.upper()]
+    c.ntransports = len(spec.transports or [])
     return c
 
 
@@ -237,12 +238,13 @@ class Context:
 
     def download_dict(self) -> Dict[str, np.ndarray]:
         f = self.download()
+        nt = self.case.ntransports
         if self.case.model == MODEL_EULER:
             return {"alpha": np.ones((1, self.n)), "rho": f[0][None, :], "p": f[1], "u": np.stack(f[2:5]),
-                    "E": f[5]}
+                    "E": f[5], "tr": np.array(f[6:6 + nt]).reshape(nt, self.n)}
         k = self.case.nphases
         return {"alpha": np.stack(f[:k]), "rho": np.stack(f[k:2 * k]), "p": f[2 * k], "u": np.stack(f[2 * k + 1:2 * k + 4]),
-                "E": f[2 * k + 4]}
+                "E": f[2 * k + 4], "tr": np.array(f[2 * k + 5:2 * k + 5 + nt]).reshape(nt, self.n)}
 
     def derived(self):
         k = self.case.nphases

@@ -91,6 +91,7 @@ class State:
     phases: List[PhaseState]
     pressure: float
     velocity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    transports: Optional[Dict[str, float]] = None  # value of each passive transport in this state
 
 
 @dataclass
@@ -153,6 +154,7 @@ class Case:
     interface_vf_limiter: Optional[str] = None
     ptmu: Optional[Tuple[int, int]] = None  # (liquid phase, vapour phase)
     boundaries: Optional[List[str]] = None  # boundCond types Xm, Xp, Ym, Yp, Zm, Zp (default nonReflecting)
+    transports: Optional[List[str]] = None  # names of passive transports (model.xml <transport>)
     output_format: str = "XML"
     output_binary: bool = True
     output_precision: Optional[int] = None  # outputMode precision (ASCII values, infoCalcul.out)
@@ -218,13 +220,17 @@ class Case:
 
     def model_xml(self) -> str:
         s = '<?xml version = "1.0" encoding = "UTF-8" standalone = "yes"?>\n<model>\n'
+        nt = len(self.transports or [])
+        ntr = f' numberTransports="{nt}"' if nt else ""
         if self.model.upper() == "EULER":
-            s += '  <flowModel name="Euler"/>\n'
+            s += f'  <flowModel name="Euler"{ntr}/>\n'
         else:
             an = "true" if self.alpha_null else "false"
-            s += f'  <flowModel name="{self.model}" numberPhases="{self.nphases}" alphaNull="{an}"/>\n'
+            s += f'  <flowModel name="{self.model}" numberPhases="{self.nphases}"{ntr} alphaNull="{an}"/>\n'
         for e in self.eos:
             s += f'  <EOS name="{e.name}"/>\n'
+        for name in self.transports or []:
+            s += f'  <transport name="{name}"/>\n'
         if self.ptmu is not None:
             liq, vap = self.ptmu
             s += ('  <relaxation type="PTMu">\n'
@@ -263,6 +269,8 @@ class Case:
                 u = st.velocity
                 s += (f'    <mixture>\n      <dataMix pressure="{st.pressure!r}"/>\n'
                       f'      <velocity x="{u[0]!r}" y="{u[1]!r}" z="{u[2]!r}"/>\n    </mixture>\n')
+            for name, v in (st.transports or {}).items():
+                s += f'    <transport name="{name}" value="{v!r}"/>\n'
             s += "  </state>\n"
         return s + "</CI>\n"
 

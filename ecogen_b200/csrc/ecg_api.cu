@@ -130,12 +130,11 @@ ecg_status validate_case(const ecg_case* c) {
   if (c->ncells[2] > 1 && c->ncells[1] <= 1) { set_error("z cells without y cells"); return ECG_ERR_INVALID; }
   for (int i = 0; i < 4; i++)
     if (c->limiter[i] < 0 || c->limiter[i] > ECG_LIM_THINC) { set_error("bad limiter"); return ECG_ERR_INVALID; }
-  if (c->order == 2 && (c->limiter[2] == ECG_LIM_THINC || c->limiter[3] == ECG_LIM_THINC)) {
-    set_error("THINC volume-fraction reconstruction is not supported");
-    return ECG_ERR_UNSUPPORTED;
-  }
+  
   for (int i = 0; i < 6; i++)
     if (c->bc[i] != ECG_BC_NONREFLECTING && c->bc[i] != ECG_BC_SYMMETRY) { set_error("bad boundary condition"); return ECG_ERR_INVALID; }
+  if (c->ntransports < 0) { set_error("negative number of transports"); return ECG_ERR_INVALID; }
+  if (c->ntransports > 2) { set_error("more than two passive transports"); return ECG_ERR_UNSUPPORTED; }
   if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
   int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
   if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
@@ -177,6 +176,8 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.rec_count = x->rec_count;
   P.rec_max = x->rec_max;
   P.rec_min_evals = x->rec_min_evals;
+  P.ntr = x->c.ntransports;
+  set_thinc(P, x->c);
   P.ptmu = x->c.ptmu;
   P.ptmu_liq = x->c.ptmu_liquid;
   P.ptmu_vap = x->c.ptmu_vapor;
@@ -402,14 +403,15 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaGetDevice"));
   e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaStreamCreate"));
-  size_t sbytes = sizeof(double) * (size_t)x->nstate * (size_t)x->n;
+  // state: the 2N + 2 + d (Euler 3 + d) fields, then the passive transports
+  size_t sbytes = sizeof(double) * (size_t)(x->nstate + c->ntransports) * (size_t)x->n;
   for (int i = 0; i < 2; i++) {
     e = cudaMalloc(&x->state[i], sbytes);
     if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(state)"));
     cudaMemsetAsync(x->state[i], 0, sbytes, x->stream);
   }
   if (c->order == 2) {
-    e = cudaMalloc(&x->half, sizeof(double) * (size_t)x->nq * (size_t)x->n);
+    e = cudaMalloc(&x->half, sizeof(double) * (size_t)(x->nstate + c->ntransports) * (size_t)x->n);
     if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(half)"));
   }
   e = cudaMalloc(&x->tmp, sizeof(double) * (size_t)x->n);
@@ -464,6 +466,7 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   // kernel attributes (dynamic shared memory) for every pass of this case shape
   for (int pass = 0; pass < 3; pass++) {
     StepParams P{};
+    P.ntr = c->ntransports;
     cudaError_t pe = euler ? euler_launch(x->dim, pass, P, x->geo, c->eos, x->eps, x->stream, true)
                            : kapila_launch(x->np, x->dim, c->ptmu != 0, pass, P, x->geo, c->eos, x->eps, x->stream, true);
     if (pe == cudaErrorNotSupported) {
@@ -523,6 +526,9 @@ static ecg_status upload_impl(ecg_ctx* x, const double* const* f, int64_t ncells
   for (int i = 0; i < pre; i++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)i * n, f[i], fb, kind, x->stream));
   for (int d = 0; d < x->dim; d++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)(pre + d) * n, f[pre + d], fb, kind, x->stream));
   ECG_CUDA(cudaMemcpyAsync(S + (size_t)(pre + x->dim) * n, f[pre + 3], fb, kind, x->stream));
+  // passive transports follow E on both sides
+  for (int j = 0; j < x->c.ntransports; j++)
+    ECG_CUDA(cudaMemcpyAsync(S + (size_t)(x->nstate + j) * n, f[pre + 4 + j], fb, kind, x->stream));
   if (kind == cudaMemcpyHostToDevice) {
     // transverse velocity components of a lower-dimensional case must be zero (they are not stored)
     for (int d = x->dim; d < 3; d++)
@@ -574,6 +580,8 @@ static ecg_status download_impl(ecg_ctx* x, double* const* f, int64_t ncells, cu
     } else ECG_CUDA(cudaMemsetAsync(f[pre + d], 0, fb, x->stream));
   }
   ECG_CUDA(cudaMemcpyAsync(f[pre + 3], S + (size_t)(pre + x->dim) * n, fb, kind, x->stream));
+  for (int j = 0; j < x->c.ntransports; j++)
+    ECG_CUDA(cudaMemcpyAsync(f[pre + 4 + j], S + (size_t)(x->nstate + j) * n, fb, kind, x->stream));
   return ECG_OK;
 }
 
@@ -713,6 +721,7 @@ extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
     return ECG_OK;
   }
   if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
+  if (x->c.ntransports > 0) { set_error("the seeded kernels run without passive transports"); return ECG_ERR_UNSUPPORTED; }
   return mlp_upload(m, x->np, &x->mlp, x->stream);
 }
 

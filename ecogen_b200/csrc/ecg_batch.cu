@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
         double aLL = hasL ? a0[rl - 1] : 0., aRR = hasR ? a0[rr + 1] : 0.;
         double pl = (gl + 0.5) * C.dx, pf = pl + 0.5 * C.dx, pr = (gl + 1 + 0.5) * C.dx;
         double y = pf - pl, z = pf - pr;
-        reconstruct_side<NP, 1>(M, P.lim, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1., tl, ug);
-        reconstruct_side<NP, 1>(M, P.lim, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z), -1.,
+        reconstruct_side<NP, 1>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1., tl, ug);
+        reconstruct_side<NP, 1>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z), -1.,
                                 tr, vg);
       }
       double Fn[3];
@@ -373,6 +373,7 @@ ecg_status launch_pass(ecg_batch* b, int pass, double* q, double* sn, double* ou
   B.P.stats = b->stats;
   for (int i = 0; i < 4; i++) B.P.lim[i] = b->c0.limiter[i];
   B.P.newton_cap = b->newton_cap;
+  set_thinc(B.P, b->c0);
   B.P.mlp = b->mlp;
   B.cases = b->cases;
   B.scal = b->scal;
@@ -446,6 +447,10 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
       set_error("batched mode runs 1D cases");
       return ECG_ERR_UNSUPPORTED;
     }
+    if (x.ntransports != 0) {
+      set_error("batched mode runs without passive transports");
+      return ECG_ERR_UNSUPPORTED;
+    }
     if (x.bc[0] != ECG_BC_NONREFLECTING || x.bc[1] != ECG_BC_NONREFLECTING) {
       set_error("batched mode runs non-reflecting sides only");
       return ECG_ERR_UNSUPPORTED;
@@ -454,10 +459,6 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
         std::memcmp(x.limiter, c0.limiter, sizeof(x.limiter)) != 0 || std::memcmp(x.eos, c0.eos, sizeof(x.eos)) != 0) {
       set_error("all cases of a batch share model, phases, EOS, order, limiters and alphaNull");
       return ECG_ERR_INVALID;
-    }
-    if ((c0.limiter[2] == ECG_LIM_THINC || c0.limiter[3] == ECG_LIM_THINC) && c0.order == 2) {
-      set_error("THINC is not supported");
-      return ECG_ERR_UNSUPPORTED;
     }
   }
   auto b = new ecg_batch();

@@ -18,6 +18,16 @@
 
 #include "ecg_types.h"
 
+// Inlining of the two largest face routines (HLLC and the MUSCL side reconstruction).  Inlined, the
+// fused pass holds one copy per axis and side; as calls, one copy each (smaller instruction
+// footprint, call overhead).  Build-time choice, measured by the benchmark.
+#ifndef ECG_HLLC_INLINE
+#define ECG_HLLC_INLINE __forceinline__
+#endif
+#ifndef ECG_RECON_INLINE
+#define ECG_RECON_INLINE __forceinline__
+#endif
+
 namespace ecg {
 
 // std::max / std::min with libstdc++'s argument order (NaN behaviour included)
@@ -107,6 +117,25 @@ struct Model {
   EosParams eos[NP];
   double eps;  // epsilonAlphaNull: 1e-15 with alphaNull, else 0 (src/Eos/Eos.cpp:88-97)
 };
+
+// EOS types known at compile time: TYPES holds the type of phase k in bits 2k..2k+1
+// (ECG_EOS_IG 0, SG 1, NASG 2), or is EOS_DYNAMIC.  With known types every EOS branch folds away
+// (the arithmetic is unchanged), which shrinks the fused kernels' code; the generic kernels read
+// the types at run time.
+constexpr int EOS_DYNAMIC = -1;
+template <int NP>
+__host__ __device__ constexpr int eos_types_code(int t0, int t1, int t2 = 0) {
+  return NP == 2 ? (t0 | (t1 << 2)) : (t0 | (t1 << 2) | (t2 << 4));
+}
+template <int NP, int TYPES>
+__device__ __forceinline__ Model<NP> specialize_eos(const Model<NP>& M0) {
+  Model<NP> M = M0;
+  if (TYPES != EOS_DYNAMIC) {
+#pragma unroll
+    for (int k = 0; k < NP; k++) M.eos[k].type = (TYPES >> (2 * k)) & 3;
+  }
+  return M;
+}
 
 // PhaseUEq::verifyAndCorrectPhase src/Models/UEq/PhaseUEq.cpp:348 (alpha / density clamps)
 __device__ __forceinline__ void phase_fix_ar(double eps, double& a, double& r) {
@@ -205,7 +234,7 @@ struct Flux {
 // HLLC: ModUEq::solveRiemannIntern src/Models/UEq/ModUEq.cpp:113-267.  L and R carry local-frame
 // velocities ul/ur (normal first).  dtmax is min-updated with lCFL/|s|.
 template <int NP>
-__device__ __forceinline__ void hllc(const Model<NP>& M, const Thermo<NP>& L, const double ul[3],
+__device__ ECG_HLLC_INLINE void hllc(const Model<NP>& M, const Thermo<NP>& L, const double ul[3],
                                      const Thermo<NP>& R, const double ur[3], double dxL, double dxR,
                                      double& dtmax, double Fn[3], Flux<NP>& F) {
   double uL = ul[0], cL = L.cF, pL = L.pm, rhoL = L.rho;

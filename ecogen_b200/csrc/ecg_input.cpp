@@ -30,6 +30,7 @@ struct StateIC {
   double alpha[ECG_MAX_PHASES], rho[ECG_MAX_PHASES];
   double p = 0.;
   double u[3] = {0., 0., 0.};
+  double tr[2] = {0., 0.};  // passive transports (0 unless the state gives them)
 };
 
 struct ecg_input {
@@ -40,6 +41,7 @@ struct ecg_input {
   std::string run_name;
   std::string output_format;
   std::vector<std::string> eos_names;
+  std::vector<std::string> transport_names;
   std::vector<StateIC> states;
   std::vector<Domain> domains;
 };
@@ -177,8 +179,6 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
     int iv = il;
     if (const Node* n = so->child("interfaceVolumeFractionLimiter")) iv = limiter_code(n->text);
     if (gv < 0 || iv < 0) return bail(ECG_ERR_XML, "main.xml: bad volume-fraction limiter");
-    if (gv == ECG_LIM_THINC || iv == ECG_LIM_THINC)
-      return bail(ECG_ERR_UNSUPPORTED, "THINC volume-fraction reconstruction is not supported");
     c.limiter[0] = gl;
     c.limiter[1] = il;
     c.limiter[2] = gv;
@@ -222,7 +222,18 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   std::string model = upper(fm->attr("name"));
   int ntr = 0;
   fm->get_int("numberTransports", &ntr);
-  if (ntr > 0) return bail(ECG_ERR_UNSUPPORTED, "passive transports are not supported");
+  if (ntr < 0) return bail(ECG_ERR_XML, "model.xml: negative numberTransports");
+  if (ntr > 2) return bail(ECG_ERR_UNSUPPORTED, "more than two passive transports are not supported");
+  c.ntransports = ntr;
+  {  // Input::inputModel src/InputOutput/Input.cpp:707-719: names in order, at least numberTransports
+    std::vector<std::string> names;
+    for (const Node* t : modx->all("transport")) {
+      if (t->attr("name").empty()) return bail(ECG_ERR_XML, "model.xml: <transport name> missing");
+      names.push_back(t->attr("name"));
+    }
+    if ((int)names.size() < ntr) return bail(ECG_ERR_XML, "model.xml: fewer <transport> than numberTransports");
+    in->transport_names = names;
+  }
   bool alpha_null = false;
   if (model == "EULER") {
     c.model = ECG_MODEL_EULER;
@@ -256,7 +267,6 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   if (modx->child("additionalPhysic")) return bail(ECG_ERR_UNSUPPORTED, "additional physics are not supported");
   if (modx->child("symmetryTerm")) return bail(ECG_ERR_UNSUPPORTED, "symmetry terms are not supported");
   if (modx->child("sourceTerms")) return bail(ECG_ERR_UNSUPPORTED, "source terms are not supported");
-  if (modx->child("transport")) return bail(ECG_ERR_UNSUPPORTED, "passive transports are not supported");
   for (const Node* r : modx->all("relaxation")) {
     std::string t = upper(r->attr("type"));
     if (t == "PTMU") {
@@ -346,6 +356,18 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
         k++;
       }
       if (k != c.nphases) return bail(ECG_ERR_XML, "state " + st + ": one material per phase expected");
+      {  // state transports (Input.cpp:1034-1050): matched by name, others ignored; a missing "value"
+         // keeps the previous one read, as the reference's loop does
+        double v = 0.;
+        for (const Node* t : sn->all("transport")) {
+          t->get_double("value", &v);
+          for (int e = 0; e < c.ntransports; e++)
+            if (t->attr("name") == in->transport_names[e]) {
+              S.tr[e] = v;
+              break;
+            }
+        }
+      }
       in->states.push_back(S);
       si = (int)in->states.size() - 1;
     }
@@ -593,6 +615,7 @@ extern "C" ecg_status ecg_input_fill(const ecg_input* in, double* const* fields,
       fields[2 * np][i] = S->p;
       for (int dd = 0; dd < 3; dd++) fields[2 * np + 1 + dd][i] = S->u[dd];
       fields[2 * np + 4][i] = E;
+      for (int j = 0; j < c.ntransports; j++) fields[2 * np + 5 + j][i] = S->tr[j];
     } else {
       double e = ecg::host_eos_e(c.eos[0], eps, S->rho[0], S->p);
       E = e + 0.5 * (S->u[0] * S->u[0] + S->u[1] * S->u[1] + S->u[2] * S->u[2]);
@@ -600,6 +623,7 @@ extern "C" ecg_status ecg_input_fill(const ecg_input* in, double* const* fields,
       fields[1][i] = S->p;
       for (int dd = 0; dd < 3; dd++) fields[2 + dd][i] = S->u[dd];
       fields[5][i] = E;
+      for (int j = 0; j < c.ntransports; j++) fields[6 + j][i] = S->tr[j];
     }
   }
   return ECG_OK;

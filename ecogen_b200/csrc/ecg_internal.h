@@ -10,7 +10,9 @@ namespace ecg {
 void set_error(const std::string& msg);
 
 // Number of field pointers in the ABI layout of a case (see include/ecogen_b200.h).
-inline int abi_nfields(const ecg_case& c) { return c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5; }
+inline int abi_nfields(const ecg_case& c) {
+  return (c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5) + c.ntransports;
+}
 
 // EOS internal energy e(rho, p), same expression as the kernels and the reference EOS classes.
 inline double host_eos_e(const ecg_eos& q, double eps, double rho, double p) {

@@ -16,12 +16,16 @@ struct CellCounters {
 // src/Order2/CellO2Cartesian.cpp:23-171 on a Cartesian mesh): the limited slope combines the slope
 // of this face (s1) and of the face on the opposite side of the cell along the same axis (s2, zero
 // when that face is a boundary); the interface detector decides between the global and interface
-// limiters; the state is extrapolated by `sign * slope * dist` and clamped.
-template <int NP, int DIM>
-__device__ __forceinline__ void reconstruct_side(const Model<NP>& M, const int lim[4], const double* sq, int RS, int rc,
-                                                 const double* ssl, int SS, int f1, int f2, double alphaCell,
+// limiters; the state is extrapolated by `sign * slope * dist` and clamped.  With THINC
+// (CellInterfaceO2Cartesian.cpp:132-150 left side, :164-181 right side, whose final expressions
+// differ and are kept as they are) alpha_0 and alpha_1 = 1 - alpha_0 of an interface cell are then
+// replaced by the hyperbolic-tangent reconstruction.
+template <int NP, int DIM, bool THINC = true>
+__device__ ECG_RECON_INLINE void reconstruct_side(const Model<NP>& M, const StepParams& P, const double* sq, int RS,
+                                                 int rc, const double* ssl, int SS, int f1, int f2, double alphaCell,
                                                  double alphaOther, double alphaAfter, double dist, double sign,
                                                  Thermo<NP>& t, double u[3]) {
+  const int* lim = P.lim;
   using FL = Fields<NP, DIM>;
   const bool iface = (alphaCell >= 1.e-4) && (alphaCell <= 1. - 1.e-4) &&
                      ((alphaOther - alphaCell) * (alphaCell - alphaAfter) >= 1.e-8);
@@ -56,6 +60,24 @@ __device__ __forceinline__ void reconstruct_side(const Model<NP>& M, const int l
     double s2 = (f2 >= 0) ? ssl[(3 * NP + d) * SS + f2] : 0.;
     double l = limiter(lg, s1, s2);
     u[d] = sq[(FL::U + d) * RS + rc] + (sign * l) * dist;
+  }
+  if (THINC && NP >= 2 && P.thinc && iface) {
+    const double beta = 1.6, eps = 1.e-4;
+    const bool right = sign < 0.;
+    // neighbours: (right cell, left-left cell) for a left side, (right-right cell, left cell) for a right side
+    const double hi = right ? alphaAfter : alphaOther, lo = right ? alphaOther : alphaAfter;
+    const double sg = (hi - lo > 0.) ? 1. : -1.;
+    const double qmin = dmin(hi, lo);
+    const double qmax = dmax(hi, lo) - qmin;
+    const double C = (alphaCell - qmin + 1.e-20) / (qmax + 1.e-20);
+    const double B = exp(sg * beta * (2. * C - 1.));
+    const double A = (B / P.thinc_cosh - 1.) / P.thinc_tanh;
+    double na = right ? qmin + 0.5 * qmax * (1. + sg * A)
+                      : qmin + 0.5 * qmax * (1. + sg * (P.thinc_tanh + A) / (1. + A * P.thinc_tanh));
+    if (na < eps) na = eps;
+    if (na > 1. - eps) na = 1. - eps;
+    t.a[0] = na;
+    t.a[1] = 1. - na;
   }
   fulfill<NP>(M, t);
 }
@@ -123,7 +145,7 @@ template <int NP, int DIM>
 __device__ __forceinline__ void boundary_face(const Model<NP>& M, const double* q, int64_t nn, int64_t cell, int ax,
                                               bool neg, double lcfl, double coefA, double& dtmax, const double an[NP],
                                               const double pn[NP], double aa[NP], double am[NP], double ae[NP],
-                                              double amom[DIM], double& aE) {
+                                              double amom[DIM], double& aE, double* sM_out = nullptr) {
   using FL = Fields<NP, DIM>;
   Thermo<NP> t;
   double ug[3], ul[3], Fn[3];
@@ -142,6 +164,7 @@ __device__ __forceinline__ void boundary_face(const Model<NP>& M, const double* 
   hllc<NP>(M, t, ul, t, ul, lcfl, lcfl, dtmax, Fn, F);
   to_global(ax, neg, Fn, F.mom);
   acc_face<NP, DIM>(coefA, false, F, an, pn, aa, am, ae, amom, aE);
+  if (sM_out) *sM_out = F.sM;
 }
 
 // Buffer cell of a symmetry side in a MUSCL pass (BoundCondWallO2Cartesian::solveRiemann

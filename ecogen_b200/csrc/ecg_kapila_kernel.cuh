@@ -7,7 +7,7 @@
 
 namespace ecg {
 
-template <int NP, int DIM, int PASS>
+template <int NP, int DIM, int PASS, int NTM = 0>
 struct KapilaStep {
   using FL = Fields<NP, DIM>;
   using TS = TileShape<DIM>;
@@ -35,15 +35,23 @@ struct KapilaStep {
     return cmax(nface(0), cmax(DIM > 1 ? nface(1) : 0, DIM > 2 ? nface(2) : 0));
   }
   static constexpr int NA0 = (PASS == PASS_CORR) ? 1 : 0;  // separate time-n alpha_0 plane
+  // passive transports (up to NTM): staged planes, slopes and face fluxes after the others
   static constexpr size_t smem_bytes() {
-    return sizeof(double) * ((size_t)RMAX() * (FL::NQ + NA0) + (size_t)SMAX() * FL::NSL + (size_t)FMAX() * FL::NFL);
+    return sizeof(double) * ((size_t)RMAX() * (FL::NQ + NA0 + NTM) + (size_t)SMAX() * (FL::NSL + NTM) +
+                             (size_t)FMAX() * (FL::NFL + NTM));
   }
 };
 
-template <int NP, int DIM, int PASS, bool PTMU, bool SEED>
-__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>::MINB)
-    k_kapila_step(StepParams P, Geometry G, Model<NP> M) {
-  using K = KapilaStep<NP, DIM, PASS>;
+// Interface detector of CellO2Cartesian::computeLocalSlopes (src/Order2/CellO2Cartesian.cpp:150).
+__device__ __forceinline__ bool iface_detect(double aCell, double aOther, double aAfter) {
+  return (aCell >= 1.e-4) && (aCell <= 1. - 1.e-4) && ((aOther - aCell) * (aCell - aAfter) >= 1.e-8);
+}
+
+template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES, int NTM = 0>
+__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH, TileShape<DIM>::MINB)
+    k_kapila_step(StepParams P, Geometry G, Model<NP> M0) {
+  const Model<NP> M = specialize_eos<NP, TYPES>(M0);
+  using K = KapilaStep<NP, DIM, PASS, NTM>;
   using FL = Fields<NP, DIM>;
   using TS = TileShape<DIM>;
   extern __shared__ double smem[];
@@ -52,8 +60,10 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
   constexpr int FS = K::FMAX();
   double* sq = smem;                                       // [NQ][RS]
   double* sa0 = sq + (size_t)FL::NQ * RS;                  // [NA0][RS]
-  double* ssl = sa0 + (size_t)K::NA0 * RS;                 // [NSL][SS]
-  double* sfl = ssl + (K::O2 ? (size_t)FL::NSL * SS : 0);  // [NFL][FS]
+  double* str = sa0 + (size_t)K::NA0 * RS;                 // [NTM][RS] transports
+  double* ssl = str + (size_t)NTM * RS;                    // [NSL + NTM][SS]
+  double* sfl = ssl + (K::O2 ? (size_t)(FL::NSL + NTM) * SS : 0);  // [NFL + NTM][FS]
+  constexpr int NTA = NTM > 0 ? NTM : 1;
 
   if (*P.done) return;  // stop condition reached earlier in a captured step sequence
   const int tid = threadIdx.x;
@@ -83,6 +93,15 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
       pn[k] = eos_fix_p(M.eos[k], p0);
     }
   }
+  // passive transports of the own cell: time-n values and accumulated fluxes
+  double tn[NTA], at[NTA];
+#pragma unroll
+  for (int j = 0; j < NTA; j++) tn[j] = at[j] = 0.;
+  if (NTM > 0 && active) {
+#pragma unroll
+    for (int j = 0; j < NTM; j++)
+      if (j < P.ntr) tn[j] = P.sn[(int64_t)(FL::NS + j) * nn + cell];
+  }
   double dtmax = 1.e10;
   double wallp[DIM];  // normal momentum flux of the cell's symmetry sides, per axis
 #pragma unroll
@@ -108,6 +127,9 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
 #pragma unroll
         for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
         if (K::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
+#pragma unroll
+        for (int j = 0; j < NTM; j++)
+          if (j < P.ntr) str[j * RS + e] = P.q[(int64_t)(FL::NS + j) * nn + c];
       }
     }
     __syncthreads();
@@ -124,7 +146,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
           if (sd < 0 || G.bc[2 * ax + sd] != ECG_BC_SYMMETRY) continue;
           if (org[b1] + line % e1 >= G.n[b1] || org[b2] + line / e1 >= G.n[b2]) continue;
 #pragma unroll
-          for (int f = 0; f < FL::NSL; f++) ssl[f * SS + e] = 0.;
+          for (int f = 0; f < FL::NSL + NTM; f++) ssl[f * SS + e] = 0.;
           const double wd = G.wslope[2 * ax + sd];
           if (fabs(wd) > 1.e-8) ssl[(3 * NP + ax) * SS + e] = sq[(FL::U + ax) * RS + (sd ? rl : rr)] / wd;
           continue;
@@ -140,6 +162,9 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
 #pragma unroll
         for (int dd = 0; dd < DIM; dd++)
           ssl[(3 * NP + dd) * SS + e] = (sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl]) / d;
+#pragma unroll
+        for (int j = 0; j < NTM; j++)  // Transport::computeSlopeTransport
+          if (j < P.ntr) ssl[(FL::NSL + j) * SS + e] = (str[j * RS + rr] - str[j * RS + rl]) / d;
       }
       __syncthreads();
     }
@@ -152,9 +177,15 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
       int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
       Thermo<NP> tl, tr;
       double ug[3], vg[3];
+      double xl[NTA], xr[NTA];  // transports of the two sides
       if (!K::O2) {
         cell_thermo<NP, DIM>(M, sq, RS, rl, tl, ug);
         cell_thermo<NP, DIM>(M, sq, RS, rr, tr, vg);
+#pragma unroll
+        for (int t = 0; t < NTM; t++) {
+          xl[t] = str[t * RS + rl];
+          xr[t] = str[t * RS + rr];
+        }
       } else {
         const int fs = line * (T + 3);
         const int f1 = fs + j + 1;                         // this face
@@ -169,8 +200,22 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
         const double* a0 = K::NA0 ? sa0 : sq;              // time-n alpha_0 planes
         double aL = sq[FL::A * RS + rl], aR = sq[FL::A * RS + rr];
         double aLL = hasL ? a0[rl - 1] : (wL ? a0[rl] : 0.), aRR = hasR ? a0[rr + 1] : (wR ? a0[rr] : 0.);
-        reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl, ug);
-        reconstruct_side<NP, DIM>(M, P.lim, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr, vg);
+        // THINC is compiled into the generic kernels only (the EOS-specialised ones run without it)
+        constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
+        reconstruct_side<NP, DIM, kThinc>(M, P, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl, ug);
+        reconstruct_side<NP, DIM, kThinc>(M, P, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr, vg);
+        if (NTM > 0) {  // transports: volume-fraction limiter of each side, Transport::extrapolate
+          const int lvL = iface_detect(aL, aR, aLL) ? P.lim[3] : P.lim[2];
+          const int lvR = iface_detect(aR, aL, aRR) ? P.lim[3] : P.lim[2];
+#pragma unroll
+          for (int t = 0; t < NTM; t++) {
+            const double s1 = ssl[(FL::NSL + t) * SS + f1];
+            const double sl2 = f2l >= 0 ? ssl[(FL::NSL + t) * SS + f2l] : 0.;
+            const double sr2 = f2r >= 0 ? ssl[(FL::NSL + t) * SS + f2r] : 0.;
+            xl[t] = str[t * RS + rl] + (1. * limiter(lvL, s1, sl2)) * G.dfl[ax][gl];
+            xr[t] = str[t * RS + rr] + (-1. * limiter(lvR, s1, sr2)) * G.dfr[ax][gl];
+          }
+        }
       }
       double ul[3], ur[3], Fn[3];
       to_local(ax, false, ug, ul);
@@ -189,6 +234,9 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
       sfl[(3 * NP + DIM) * FS + e] = F.E;
       sfl[(3 * NP + DIM + 1) * FS + e] = F.sM;
       sfl[(3 * NP + DIM + 2) * FS + e] = F.uStar;
+#pragma unroll
+      for (int t = 0; t < NTM; t++)  // Transport::solveRiemann: upwind by sM
+        sfl[(FL::NFL + t) * FS + e] = (F.sM > 0.) ? xl[t] * F.sM : xr[t] * F.sM;
     }
     __syncthreads();
     // ---- accumulate the two faces of this axis into the own cell (left +, right -)
@@ -215,6 +263,18 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
         F.sM = sfl[(3 * NP + DIM + 1) * FS + e];
         F.uStar = sfl[(3 * NP + DIM + 2) * FS + e];
         acc_face<NP, DIM>(cA, side == 0, F, an, pn, aa, am, ae, amom, aE);
+#pragma unroll
+        for (int t = 0; t < NTM; t++) {  // Transport::addFlux / addNonCons (time-n value), or subtract
+          if (t >= P.ntr) continue;
+          const double ft = sfl[(FL::NFL + t) * FS + e];
+          if (side == 0) {
+            at[t] += cA * ft;
+            at[t] += -cA * tn[t] * F.sM;
+          } else {
+            at[t] -= cA * ft;
+            at[t] -= -cA * tn[t] * F.sM;
+          }
+        }
       }
       // a symmetry side of this cell along ax: its flux is computed now, while the slopes of this axis
       // are staged, and subtracted with the other boundary faces below (reference face order)
@@ -249,13 +309,28 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS>::NTH, TileShape<DIM>
       int ax = bf >> 1;
       bool neg = (bf & 1) == 0;
       if (neg ? (gc[ax] != 0) : (gc[ax] != G.n[ax] - 1)) continue;
+      double sMb = 0.;
       if (G.bc[bf] == ECG_BC_SYMMETRY)
         wall_acc<NP, DIM>(ax, neg, wallp[ax], G.coefA[ax], an, pn, aa, am, ae, amom, aE);
       else
-        boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE);
+        boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE,
+                               &sMb);
+#pragma unroll
+      for (int t = 0; t < NTM; t++) {  // transports: T sM on a non-reflecting side, nothing on a symmetry side
+        if (t >= P.ntr) continue;
+        const double ft = (G.bc[bf] == ECG_BC_SYMMETRY) ? 0. : P.q[(int64_t)(FL::NS + t) * nn + cell] * sMb;
+        at[t] -= G.coefA[ax] * ft;
+        at[t] -= -G.coefA[ax] * tn[t] * sMb;
+      }
     }
 
     kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
+    if (NTM > 0) {  // Cell::timeEvolution :294-298 / CellO2::predictionOrdre2 :121-125
+      const double scale = (PASS == PASS_PRED) ? 0.5 * *P.dt : *P.dt;
+#pragma unroll
+      for (int t = 0; t < NTM; t++)
+        if (t < P.ntr) P.out[(int64_t)(FL::NS + t) * nn + cell] = tn[t] + at[t] * scale;
+    }
   }
   // learned seed of the pressure relaxation, gated on the plain start (all lanes of the warp)
   SeedGate<NP> sg;

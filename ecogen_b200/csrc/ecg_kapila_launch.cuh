@@ -5,12 +5,12 @@
 
 namespace ecg {
 
-template <int NP, int DIM, int PASS, bool PTMU, bool SEED>
+template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES = EOS_DYNAMIC, int NTM = 0>
 cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps, cudaStream_t s,
                               bool prepare) {
-  using K = KapilaStep<NP, DIM, PASS>;
+  using K = KapilaStep<NP, DIM, PASS, NTM>;
   using TS = TileShape<DIM>;
-  auto kern = k_kapila_step<NP, DIM, PASS, PTMU, SEED>;
+  auto kern = k_kapila_step<NP, DIM, PASS, PTMU, SEED, TYPES, NTM>;
   const size_t sm = K::smem_bytes();
   if (prepare) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -25,14 +25,33 @@ cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eo
   return cudaGetLastError();
 }
 
-template <int NP, int DIM, bool PTMU, bool SEED>
+template <int NP, int DIM, bool PTMU, bool SEED, int TYPES = EOS_DYNAMIC, int NTM = 0>
 cudaError_t launch_pass_seed(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
                              cudaStream_t s, bool prepare) {
   switch (pass) {
-    case PASS_O1: return launch_one<NP, DIM, PASS_O1, PTMU, SEED && !PTMU>(P, G, eos, eps, s, prepare);
-    case PASS_PRED: return launch_one<NP, DIM, PASS_PRED, PTMU, SEED && !PTMU>(P, G, eos, eps, s, prepare);
-    default: return launch_one<NP, DIM, PASS_CORR, PTMU, SEED && !PTMU>(P, G, eos, eps, s, prepare);
+    case PASS_O1: return launch_one<NP, DIM, PASS_O1, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    case PASS_PRED: return launch_one<NP, DIM, PASS_PRED, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    default: return launch_one<NP, DIM, PASS_CORR, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
   }
+}
+
+// Kernels with passive transports (up to two, generic EOS, no seed) live in their own translation
+// units (ecg_kapila_tr_np2.cu, ecg_kapila_tr_np3.cu).
+cudaError_t kapila_launch_tr(int np, int dim, bool ptmu, int pass, const StepParams& P, const Geometry& G,
+                             const ecg_eos* eos, double eps, cudaStream_t s, bool prepare);
+constexpr int KAPILA_MAX_TRANSPORTS = 2;
+
+// The EOS combination of the shipped workloads (SG liquid first, ideal gases after) has kernels
+// (plain and seeded) with the types compiled in and no THINC code; every other case (other EOS,
+// THINC, passive transports, p-T-mu) runs the generic kernels.
+template <int NP>
+constexpr int eos_fast_types() {
+  return NP == 2 ? eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG) : eos_types_code<3>(ECG_EOS_SG, ECG_EOS_IG, ECG_EOS_IG);
+}
+template <int NP>
+inline bool eos_is_fast(const ecg_eos* eos) {
+  int t[3] = {eos[0].type, eos[1].type, NP > 2 ? eos[2].type : 0};
+  return eos_types_code<NP>(t[0], t[1], t[2]) == eos_fast_types<NP>();
 }
 
 template <int NP, int DIM, bool PTMU>
@@ -40,15 +59,35 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
                                cudaStream_t s, bool prepare) {
   // kernels with the learned seed are separate variants, so that the plain kernels carry none of
   // its registers; with prepare both are configured
+#ifndef ECG_NO_EOS_SPECIALIZATION
+  constexpr bool kFast = !PTMU;
+#else
+  constexpr bool kFast = false;
+#endif
+  if (P.ntr > 0) {
+    if (P.mlp != nullptr) return cudaErrorNotSupported;
+    return kapila_launch_tr(NP, DIM, PTMU, pass, P, G, eos, eps, s, prepare);
+  }
   if (prepare) {
     cudaError_t e = launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast)
+      e = launch_pass_seed<NP, DIM, PTMU, false, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s, true);
     if (e != cudaSuccess || PTMU) return e;
-    return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, true);
+    e = launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast)
+      e = launch_pass_seed<NP, DIM, PTMU, true, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s, true);
+    return e;
   }
   if (P.mlp != nullptr) {
     if (PTMU) return cudaErrorNotSupported;
+    if (kFast && !P.thinc && eos_is_fast<NP>(eos))
+      return launch_pass_seed<NP, DIM, PTMU, true, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
+                                                                                                 false);
     return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, false);
   }
+  if (kFast && !P.thinc && eos_is_fast<NP>(eos))
+    return launch_pass_seed<NP, DIM, PTMU, false, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
+                                                                                                false);
   return launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, false);
 }
 

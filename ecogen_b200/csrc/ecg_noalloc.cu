@@ -127,6 +127,10 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
     set_error("order must be 1 or 2");
     return ECG_ERR_INVALID;
   }
+  if (c->ntransports != 0) {
+    set_error("ecg_step_noalloc runs without passive transports");
+    return ECG_ERR_UNSUPPORTED;
+  }
   for (int a = 0; a < 3; a++)
     if (c->ncells[a] < 1 || !(c->length[a] > 0.)) {
       set_error("bad mesh");
@@ -176,6 +180,7 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
   P.stats = &S->stats;
   for (int i = 0; i < 4; i++) P.lim[i] = c->limiter[i];
   P.newton_cap = 100;
+  set_thinc(P, *c);
   P.ptmu = c->ptmu;
   P.ptmu_liq = c->ptmu_liquid;
   P.ptmu_vap = c->ptmu_vapor;

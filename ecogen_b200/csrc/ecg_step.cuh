@@ -114,7 +114,20 @@ struct StepParams {
   // p-T-mu relaxation
   int ptmu, ptmu_liq, ptmu_vap;
   double pcrit;
+  // THINC reconstruction of alpha (a volume-fraction limiter is THINC): cosh and tanh of the
+  // sharpness beta = 1.6, evaluated once on the host like the reference does
+  int thinc;
+  double thinc_cosh, thinc_tanh;
+  // passive transports: stored after the NS fields of a state (at NS + j), j < ntr
+  int ntr;
 };
+
+// Host side of the THINC parameters (CellInterfaceO2Cartesian::solveRiemann's beta = 1.6).
+inline void set_thinc(StepParams& P, const ecg_case& c) {
+  P.thinc = (c.order == 2 && (c.limiter[2] == ECG_LIM_THINC || c.limiter[3] == ECG_LIM_THINC)) ? 1 : 0;
+  P.thinc_cosh = std::cosh(1.6);
+  P.thinc_tanh = std::tanh(1.6);
+}
 
 __device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, double v) {
   // positive doubles order like their bit patterns

@@ -12,7 +12,7 @@
 
 namespace ecg {
 
-template <int DIM, int PASS>
+template <int DIM, int PASS, int NTM = 0>
 struct EulerStep {
   using TS = TileShape<DIM>;
   static constexpr int H = (PASS == PASS_O1) ? 1 : 2;
@@ -34,8 +34,10 @@ struct EulerStep {
   __host__ __device__ static constexpr int RMAX() { return cmax(region(0), cmax(DIM > 1 ? region(1) : 0, DIM > 2 ? region(2) : 0)); }
   __host__ __device__ static constexpr int SMAX() { return cmax(nslope(0), cmax(DIM > 1 ? nslope(1) : 0, DIM > 2 ? nslope(2) : 0)); }
   __host__ __device__ static constexpr int FMAX() { return cmax(nface(0), cmax(DIM > 1 ? nface(1) : 0, DIM > 2 ? nface(2) : 0)); }
+  // passive transports (up to NTM): staged planes, slopes, and per face sM plus the transport fluxes
+  static constexpr int NFT = NTM > 0 ? NTM + 1 : 0;
   static constexpr size_t smem_bytes() {
-    return sizeof(double) * ((size_t)RMAX() * NQ + (size_t)SMAX() * NSL + (size_t)FMAX() * NFL);
+    return sizeof(double) * ((size_t)RMAX() * (NQ + NTM) + (size_t)SMAX() * (NSL + NTM) + (size_t)FMAX() * (NFL + NFT));
   }
 };
 
@@ -54,7 +56,7 @@ __device__ __forceinline__ void euler_complete(const EosParams& q, double eps, E
 // ModEuler::solveRiemannIntern src/Models/Euler/ModEuler.cpp:105-225 (strict sL > 0 / sR < 0).
 __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3], const EulerSide& R,
                                            const double ur[3], double dxL, double dxR, double& dtmax, double& Fm,
-                                           double Fn[3], double& FE) {
+                                           double Fn[3], double& FE, double* sM_out = nullptr) {
   double uL = ul[0], vL = ul[1], wL = ul[2], pL = L.p, rhoL = L.rho, cL = L.c, EL = L.E;
   double uR = ur[0], vR = ur[1], wR = ur[2], pR = R.p, rhoR = R.rho, cR = R.c, ER = R.E;
   double sL = dmin(uL - cL, uR - cR);
@@ -64,6 +66,7 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
   double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
   double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
   if (fabs(sM) < 1.e-8) sM = 0.;
+  if (sM_out) *sM_out = sM;
   if (sL > 0.) {
     Fm = rhoL * uL;
     Fn[0] = rhoL * uL * uL + pL;
@@ -97,10 +100,10 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
   }
 }
 
-template <int DIM, int PASS>
-__global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
+template <int DIM, int PASS, int NTM = 0>
+__global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH)
     k_euler_step(StepParams P, Geometry G, EosParams q, double eps) {
-  using K = EulerStep<DIM, PASS>;
+  using K = EulerStep<DIM, PASS, NTM>;
   using TS = TileShape<DIM>;
   if (*P.done) return;
   extern __shared__ double smem[];
@@ -109,8 +112,11 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
   constexpr int FS = K::FMAX();
   constexpr int NQ = K::NQ;
   double* sq = smem;
-  double* ssl = sq + (size_t)NQ * RS;
-  double* sfl = ssl + (K::O2 ? (size_t)K::NSL * SS : 0);
+  double* str = sq + (size_t)NQ * RS;                           // [NTM][RS] transports
+  double* ssl = str + (size_t)NTM * RS;                         // [NSL + NTM][SS]
+  double* sfl = ssl + (K::O2 ? (size_t)(K::NSL + NTM) * SS : 0);  // [NFL + NFT][FS]
+  constexpr int NTA = NTM > 0 ? NTM : 1;
+  constexpr int NS = 3 + DIM;  // fields of the Euler state; transports at NS + j
   const int tid = threadIdx.x;
   const int org[3] = {(int)blockIdx.x * TS::X, (int)blockIdx.y * TS::Y, (int)blockIdx.z * TS::Z};
   const int lc[3] = {tid % TS::X, (tid / TS::X) % TS::Y, tid / (TS::X * TS::Y)};
@@ -121,6 +127,14 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
   double am = 0., amom[DIM], aE = 0.;
 #pragma unroll
   for (int d = 0; d < DIM; d++) amom[d] = 0.;
+  double tn[NTA], at[NTA];  // transports: time-n values, accumulated fluxes
+#pragma unroll
+  for (int t = 0; t < NTA; t++) tn[t] = at[t] = 0.;
+  if (NTM > 0 && active) {
+#pragma unroll
+    for (int t = 0; t < NTM; t++)
+      if (t < P.ntr) tn[t] = P.sn[(int64_t)(NS + t) * nn + cell];
+  }
   double dtmax = 1.e10;
   double wallp[DIM];  // normal momentum flux of the cell's symmetry sides, per axis
 #pragma unroll
@@ -142,6 +156,9 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
         int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
 #pragma unroll
         for (int f = 0; f < NQ; f++) sq[f * RS + e] = (f < NQ - 1 || !K::O2) ? P.q[(int64_t)f * nn + c] : 0.;
+#pragma unroll
+        for (int t = 0; t < NTM; t++)
+          if (t < P.ntr) str[t * RS + e] = P.q[(int64_t)(NS + t) * nn + c];
       }
     }
     __syncthreads();
@@ -157,7 +174,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
           if (sd < 0 || G.bc[2 * ax + sd] != ECG_BC_SYMMETRY) continue;
           if (org[b1] + line % e1 >= G.n[b1] || org[b2] + line / e1 >= G.n[b2]) continue;
 #pragma unroll
-          for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = 0.;
+          for (int f = 0; f < K::NSL + NTM; f++) ssl[f * SS + e] = 0.;
           const double wd = G.wslope[2 * ax + sd];
           if (fabs(wd) > 1.e-8) ssl[(2 + ax) * SS + e] = sq[(2 + ax) * RS + (sd ? rl : rr)] / wd;
           continue;
@@ -165,6 +182,9 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
         double d = G.dcc[ax][gl];
 #pragma unroll
         for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = (sq[f * RS + rr] - sq[f * RS + rl]) / d;
+#pragma unroll
+        for (int t = 0; t < NTM; t++)  // Transport::computeSlopeTransport
+          if (t < P.ntr) ssl[(K::NSL + t) * SS + e] = (str[t * RS + rr] - str[t * RS + rl]) / d;
       }
       __syncthreads();
     }
@@ -175,10 +195,13 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
       if (gl < 0 || gl + 1 >= nax || org[b1] + l1 >= G.n[b1] || org[b2] + l2 >= G.n[b2]) continue;
       int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
       EulerSide L, R;
+      double xs[2][NTA];  // transports of the two sides
 #pragma unroll
       for (int side = 0; side < 2; side++) {
         EulerSide& S = side ? R : L;
         int rc = side ? rr : rl;
+#pragma unroll
+        for (int t = 0; t < NTM; t++) xs[side][t] = str[t * RS + rc];
         S.rho = sq[0 * RS + rc];
         S.p = sq[1 * RS + rc];
         S.u[0] = S.u[1] = S.u[2] = 0.;
@@ -201,6 +224,11 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
           S.rho += (sign * lr) * dist;
           S.p += (sign * lp) * dist;
 #pragma unroll
+          for (int t = 0; t < NTM; t++) {  // global volume-fraction limiter (no interface detection for Euler)
+            double lt = limiter(P.lim[2], ssl[(K::NSL + t) * SS + f1], f2 >= 0 ? ssl[(K::NSL + t) * SS + f2] : 0.);
+            xs[side][t] += (sign * lt) * dist;
+          }
+#pragma unroll
           for (int d = 0; d < DIM; d++) {
             double l = limiter(P.lim[0], ssl[(2 + d) * SS + f1], f2 >= 0 ? ssl[(2 + d) * SS + f2] : 0.);
             S.u[d] = S.u[d] + (sign * l) * dist;
@@ -214,12 +242,19 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
       double ul[3], ur[3], Fn[3], Fm, FE, Fg[3];
       to_local(ax, false, L.u, ul);
       to_local(ax, false, R.u, ur);
-      hllc_euler(L, ul, R, ur, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE);
+      double sM = 0.;
+      hllc_euler(L, ul, R, ur, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE, &sM);
       to_global(ax, false, Fn, Fg);
       sfl[0 * FS + e] = Fm;
 #pragma unroll
       for (int d = 0; d < DIM; d++) sfl[(1 + d) * FS + e] = Fg[d];
       sfl[(1 + DIM) * FS + e] = FE;
+      if (NTM > 0) {
+        sfl[K::NFL * FS + e] = sM;
+#pragma unroll
+        for (int t = 0; t < NTM; t++)  // Transport::solveRiemann: upwind by sM
+          sfl[(K::NFL + 1 + t) * FS + e] = (sM > 0.) ? xs[0][t] * sM : xs[1][t] * sM;
+      }
     }
     __syncthreads();
     if (active) {
@@ -243,6 +278,21 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
 #pragma unroll
           for (int d = 0; d < DIM; d++) amom[d] -= cA * sfl[(1 + d) * FS + e];
           aE -= cA * FE;
+        }
+        if (NTM > 0) {  // Transport::addFlux / addNonCons (time-n value), or subtract
+          const double sM = sfl[K::NFL * FS + e];
+#pragma unroll
+          for (int t = 0; t < NTM; t++) {
+            if (t >= P.ntr) continue;
+            const double ft = sfl[(K::NFL + 1 + t) * FS + e];
+            if (side == 0) {
+              at[t] += cA * ft;
+              at[t] += -cA * tn[t] * sM;
+            } else {
+              at[t] -= cA * ft;
+              at[t] -= -cA * tn[t] * sM;
+            }
+          }
         }
       }
       // symmetry side along ax: flux now (slopes of this axis staged), subtracted below in face order
@@ -294,6 +344,12 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
 #pragma unroll
         for (int d = 0; d < DIM; d++) amom[d] -= cA * Fg[d];
         aE -= cA * 0.;
+#pragma unroll
+        for (int t = 0; t < NTM; t++) {  // no transport flux through a symmetry side, sM = 0
+          if (t >= P.ntr) continue;
+          at[t] -= cA * 0.;
+          at[t] -= -cA * tn[t] * 0.;
+        }
         continue;
       }
       EulerSide S;
@@ -305,13 +361,21 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
       euler_complete(q, eps, S);  // BoundCond::solveRiemann calls fulfillState on its buffer
       double ul[3], Fn[3], Fm, FE, Fg[3];
       to_local(ax, neg, S.u, ul);
-      hllc_euler(S, ul, S, ul, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE);
+      double sMb = 0.;
+      hllc_euler(S, ul, S, ul, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE, &sMb);
       to_global(ax, neg, Fn, Fg);
       const double cA = G.coefA[ax];
       am -= cA * Fm;
 #pragma unroll
       for (int d = 0; d < DIM; d++) amom[d] -= cA * Fg[d];
       aE -= cA * FE;
+#pragma unroll
+      for (int t = 0; t < NTM; t++) {  // non-reflecting side: T sM of the cell
+        if (t >= P.ntr) continue;
+        const double ft = P.q[(int64_t)(NS + t) * nn + cell] * sMb;
+        at[t] -= cA * ft;
+        at[t] -= -cA * tn[t] * sMb;
+      }
     }
     // FluxEuler::buildCons, Cell::timeEvolution, FluxEuler::buildPrim
     const double dt = *P.dt;
@@ -337,6 +401,9 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
 #pragma unroll
     for (int d = 0; d < DIM; d++) P.out[(int64_t)(2 + d) * nn + cell] = u[d];
     if (PASS != PASS_PRED) P.out[(int64_t)(2 + DIM) * nn + cell] = E;
+#pragma unroll
+    for (int t = 0; t < NTM; t++)  // Cell::timeEvolution / CellO2::predictionOrdre2
+      if (t < P.ntr) P.out[(int64_t)(NS + t) * nn + cell] = tn[t] + at[t] * scale;
   }
   __shared__ double red[32];
   double v = dtmax;
@@ -352,12 +419,12 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS>::NTH)
   }
 }
 
-template <int DIM, int PASS>
+template <int DIM, int PASS, int NTM>
 static cudaError_t euler_one(const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps, cudaStream_t s,
                              bool prepare) {
-  using K = EulerStep<DIM, PASS>;
+  using K = EulerStep<DIM, PASS, NTM>;
   using TS = TileShape<DIM>;
-  auto kern = k_euler_step<DIM, PASS>;
+  auto kern = k_euler_step<DIM, PASS, NTM>;
   const size_t sm = K::smem_bytes();
   if (prepare) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   EosParams q{eos[0].type, eos[0].gamma, eos[0].pinf, eos[0].b, eos[0].cv, eos[0].eref, eos[0].sref};
@@ -366,12 +433,20 @@ static cudaError_t euler_one(const StepParams& P, const Geometry& G, const ecg_e
   return cudaGetLastError();
 }
 
+template <int DIM, int NTM>
+static cudaError_t euler_dim_tr(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
+                                cudaStream_t s, bool prepare) {
+  if (pass == PASS_O1) return euler_one<DIM, PASS_O1, NTM>(P, G, eos, eps, s, prepare);
+  if (pass == PASS_PRED) return euler_one<DIM, PASS_PRED, NTM>(P, G, eos, eps, s, prepare);
+  return euler_one<DIM, PASS_CORR, NTM>(P, G, eos, eps, s, prepare);
+}
+
 template <int DIM>
 static cudaError_t euler_dim(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
                              cudaStream_t s, bool prepare) {
-  if (pass == PASS_O1) return euler_one<DIM, PASS_O1>(P, G, eos, eps, s, prepare);
-  if (pass == PASS_PRED) return euler_one<DIM, PASS_PRED>(P, G, eos, eps, s, prepare);
-  return euler_one<DIM, PASS_CORR>(P, G, eos, eps, s, prepare);
+  if (P.ntr > 2) return cudaErrorNotSupported;
+  if (P.ntr > 0) return euler_dim_tr<DIM, 2>(pass, P, G, eos, eps, s, prepare);  // up to two passive transports
+  return euler_dim_tr<DIM, 0>(pass, P, G, eos, eps, s, prepare);
 }
 
 cudaError_t euler_launch(int dim, int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,

@@ -246,10 +246,21 @@ struct Output {
   bool binary = true;
   int precision = 0;
 
+  // Passive transports T1, T2, ..., values below 1e-20 written as 0 (MeshCartesian::getData
+  // src/Meshes/MeshCartesian.cpp:1832-1836).
+  void write_transports(std::ostream& o, const std::vector<std::vector<double>>& f, int first) {
+    for (int j = 0; j < c.ntransports; j++) {
+      std::vector<double> v = f[first + j];
+      for (double& x : v)
+        if (x < 1.e-20) x = 0.;
+      write_array(o, "T" + std::to_string(j + 1), v, 1, binary);
+    }
+  }
+
   bool write(ecg_ctx* ctx) {
     const int np = c.nphases;
     const bool euler = c.model == ECG_MODEL_EULER;
-    const int nf = euler ? 6 : 2 * np + 5;
+    const int nf = (euler ? 6 : 2 * np + 5) + c.ntransports;
     std::vector<std::vector<double>> f(nf, std::vector<double>((size_t)n));
     std::vector<double*> ptr;
     for (auto& v : f) ptr.push_back(v.data());
@@ -282,6 +293,7 @@ struct Output {
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 + d][i];
       write_array(o, "F0_Velocity_" + e, u, 3, binary);
+      write_transports(o, f, 6);
       write_array(o, "gradRho", grad_rho(c, f[0]), 1, binary);
     } else {
       for (int k = 0; k < np; k++) {  // PhasePUEq scalars (src/Models/PUEq/PhasePUEq.cpp:60-110)
@@ -308,6 +320,7 @@ struct Output {
       for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 * np + 1 + d][i];
       write_array(o, "Velocity_Mixture", u, 3, binary);
+      write_transports(o, f, 2 * np + 5);
       write_array(o, "gradRho", grad_rho(c, rho), 1, binary);
     }
     o << "      </CellData>\n    </Piece>\n  </RectilinearGrid>\n</VTKFile>\n";
@@ -338,7 +351,7 @@ int run_case(const std::string& work, const std::string& rel) {
   }
   int32_t binary = 1, precision = 0, restart = 0;
   ecg_input_output_control(in, &binary, &precision, &restart);
-  const int nf = c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5;
+  const int nf = (c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5) + c.ntransports;
   std::vector<std::vector<double>> f(nf, std::vector<double>((size_t)n));
   std::vector<double*> ptr;
   for (auto& v : f) ptr.push_back(v.data());
@@ -378,10 +391,11 @@ int run_case(const std::string& work, const std::string& rel) {
       // phase scalars then vectors, mixture scalars then vectors (OutputXML::ReadPhysicalDataXML :194)
       const int np = c.nphases;
       const bool euler = c.model == ECG_MODEL_EULER;
-      const size_t need = euler ? 4 : (size_t)4 * np + 4;
+      const size_t base = euler ? 4 : (size_t)4 * np + 4;
+      const size_t need = base + c.ntransports;  // then the transports T1, T2, ...
       bool ok = arrays.size() >= need;
       for (size_t a = 0; ok && a < need; a++) {
-        bool vec = euler ? a == 3 : a == need - 1;
+        bool vec = euler ? a == 3 : a == base - 1;
         ok = arrays[a].size() == (size_t)n * (vec ? 3 : 1);
       }
       if (!ok) {
@@ -400,6 +414,10 @@ int run_case(const std::string& work, const std::string& rel) {
         f[2 * np + 4] = arrays[4 * np + 2];
         for (int64_t i = 0; i < n; i++)
           for (int d = 0; d < 3; d++) f[2 * np + 1 + d][i] = arrays[4 * np + 3][3 * i + d];
+      }
+      if (ok) {
+        const int first = euler ? 6 : 2 * np + 5;
+        for (int j = 0; j < c.ntransports; j++) f[first + j] = arrays[base + j];
       }
     }
     if (fail_msg.empty()) {

@@ -12,11 +12,11 @@
  * Field layout used by upload/download (n = number of cells, cell index i + j*nx + k*nx*ny as
  * src/Meshes/MeshCartesian.cpp:141 orders cells): a caller passes an array of pointers, one per
  * field, in the order
- *   alpha_0 .. alpha_{N-1}, rho_0 .. rho_{N-1}, p, u_x, u_y, u_z, E            (Kapila, N phases)
- *   rho, p, u_x, u_y, u_z, E                                                   (Euler)
- * each pointing at n doubles.  For Kapila, p is the mixture pressure sum_k alpha_k p_k as the
- * reference writes it ("Pressure_Mixture", src/Models/UEq/MixUEq.cpp:201); E is the specific
- * total energy ("Total_energy_Mixture").
+ *   alpha_0 .. alpha_{N-1}, rho_0 .. rho_{N-1}, p, u_x, u_y, u_z, E, T_0 .. T_{M-1}  (Kapila, N phases)
+ *   rho, p, u_x, u_y, u_z, E, T_0 .. T_{M-1}                                       (Euler)
+ * each pointing at n doubles, M = ecg_case.ntransports.  For Kapila, p is the mixture pressure
+ * sum_k alpha_k p_k as the reference writes it ("Pressure_Mixture", src/Models/UEq/MixUEq.cpp:201);
+ * E is the specific total energy ("Total_energy_Mixture"); T_j are the passive transports.
  */
 #ifndef ECOGEN_B200_H
 #define ECOGEN_B200_H
@@ -75,6 +75,7 @@ typedef struct {
   int32_t ptmu_liquid, ptmu_vapor;
   ecg_eos eos[ECG_MAX_PHASES];
   int32_t bc[6];                /* ECG_BC_* of the sides Xm, Xp, Ym, Yp, Zm, Zp (MeshCartesian::assignLimits) */
+  int32_t ntransports;          /* passive transports (model.xml numberTransports, src/Transport), 0..2 */
 } ecg_case;
 
 /* Counters of one ecg_step call (replace the reference's errors / warnings vectors). */

@@ -16,6 +16,7 @@
 #include <string.h>
 
 #define NP_MAX 3
+#define NT_MAX 4   /* passive transports (model.xml numberTransports) */
 
 /* std::max / std::min exactly as libstdc++ defines them (NaN handling included) */
 static inline double omax(double a, double b) { return (a < b) ? b : a; }
@@ -35,16 +36,19 @@ typedef struct {
 typedef struct {
   OPh ph[NP_MAX];
   OMix m;
+  double tr[NT_MAX];  /* Transport values (src/Transport/Transport.h) */
 } OSt;
 
 typedef struct {
   double alpha[NP_MAX], mass[NP_MAX], energ[NP_MAX], mom[3], energMix; /* FluxUEq / FluxEuler */
+  double tr[NT_MAX];  /* transport fluxes / accumulated m_consTransports */
   double sM, uStar;
 } OFlux;
 
 typedef struct {
   double alpha[NP_MAX], rho[NP_MAX], p[NP_MAX];
   double u[3];
+  double tr[NT_MAX];
 } OSlope; /* PhaseUEq/PhaseEuler slopes + MixUEq velocity slopes */
 
 typedef struct {
@@ -72,6 +76,7 @@ struct ecgo_sim {
   int* cellface;      /* per cell, per axis, [minus, plus] face index (-1 none) : 6 ints */
   OSlope* slopes;     /* per face */
   double pcrit;
+  int thinc;          /* a volume-fraction limiter is THINC */
   ecgo_stats st;
 };
 
@@ -436,6 +441,10 @@ static void hllc_euler(const ecgo_sim* S, const OSt* Ls, const OSt* Rs, double d
  * FluxPUEq::addNonCons/subtractNonCons src/Models/PUEq/FluxPUEq.cpp:44,56 ;
  * FluxEuler add/subtract (no non-conservative terms). */
 static void acc_add(const ecgo_sim* S, OFlux* acc, const OFlux* F, double cA, const OSt* cellN) {
+  for (int k = 0; k < S->c.ntr; k++) { /* Transport::addFlux, addNonCons (time-n value) */
+    acc->tr[k] += cA * F->tr[k];
+    acc->tr[k] += -cA * cellN->tr[k] * F->sM;
+  }
   if (S->c.model == ECGO_MODEL_EULER) {
     acc->mass[0] += cA * F->mass[0];
     for (int d = 0; d < 3; d++) acc->mom[d] += cA * F->mom[d];
@@ -457,6 +466,10 @@ static void acc_add(const ecgo_sim* S, OFlux* acc, const OFlux* F, double cA, co
 }
 
 static void acc_sub(const ecgo_sim* S, OFlux* acc, const OFlux* F, double cA, const OSt* cellN) {
+  for (int k = 0; k < S->c.ntr; k++) { /* Transport::subtractFlux, subtractNonCons */
+    acc->tr[k] -= cA * F->tr[k];
+    acc->tr[k] -= -cA * cellN->tr[k] * F->sM;
+  }
   if (S->c.model == ECGO_MODEL_EULER) {
     acc->mass[0] -= cA * F->mass[0];
     for (int d = 0; d < 3; d++) acc->mom[d] -= cA * F->mom[d];
@@ -929,6 +942,8 @@ static void riemann(ecgo_sim* S, OSt* L, OSt* R, const OFace* F, double dxL, dou
   proj_local(vel_of(S, &r), F->n, F->t, F->b);
   if (S->c.model == ECGO_MODEL_EULER) hllc_euler(S, &l, &r, dxL, dxR, dtMax, out);
   else hllc_ueq(S, &l, &r, dxL, dxR, dtMax, out);
+  for (int k = 0; k < S->c.ntr; k++) /* Transport::solveRiemann src/Transport/Transport.cpp: upwind by sM */
+    out->tr[k] = (out->sM > 0.) ? l.tr[k] * out->sM : r.tr[k] * out->sM;
   proj_reverse(out->mom, F->n, F->t, F->b);
 }
 
@@ -940,6 +955,7 @@ static void compute_slopes(ecgo_sim* S, OSt* st) {
     double dist = vnorm_diff(&S->pos[3 * F->L], &S->pos[3 * F->R]);
     OSt* L = &st[F->L];
     OSt* R = &st[F->R];
+    for (int k = 0; k < S->c.ntr; k++) sl->tr[k] = (R->tr[k] - L->tr[k]) / dist; /* computeSlopeTransport */
     if (S->c.model == ECGO_MODEL_EULER) {
       sl->rho[0] = (R->ph[0].rho - L->ph[0].rho) / dist;
       sl->p[0] = (R->ph[0].p - L->ph[0].p) / dist;
@@ -973,7 +989,8 @@ static void compute_slopes(ecgo_sim* S, OSt* st) {
  * AMR: slope 1 is the reference face's slope, slope 2 the slope of the face on the opposite side along the
  * same axis (zero if that side is a boundary); the neighbour across that face gives alphaCellAfterOppositeSide
  * (time-n volume fraction of phase 0). */
-static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, double alphaOther, OSlope* out) {
+static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, double alphaOther, OSlope* out,
+                         double* alphaAfterOut) {
   const OFace* F = &S->faces[face];
   int side_plus = (F->L == cell);  /* reference face is on the + side of the cell */
   int opp = S->cellface[6 * cell + 2 * F->axis + (side_plus ? 0 : 1)];
@@ -990,10 +1007,12 @@ static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, doub
   }
   int np = S->np;
   double eps = 1.e-4;
+  *alphaAfterOut = alphaAfter;
   int interface = (alphaCell >= eps) && (alphaCell <= 1. - eps) &&
                   ((alphaOther - alphaCell) * (alphaCell - alphaAfter) >= 1.e-8);
   int lim = interface ? S->c.lim[1] : S->c.lim[0];
   int limv = interface ? S->c.lim[3] : S->c.lim[2];
+  for (int k = 0; k < S->c.ntr; k++) out->tr[k] = ecgo_limiter(limv, s1.tr[k], s2.tr[k]);
   if (S->c.model == ECGO_MODEL_EULER) {
     out->rho[0] = ecgo_limiter(lim, s1.rho[0], s2.rho[0]);
     out->p[0] = ecgo_limiter(lim, s1.p[0], s2.p[0]);
@@ -1077,7 +1096,9 @@ static void extrapolate_side(ecgo_sim* S, OSt* b, const OSlope* sl, double dist)
 }
 
 static void extrapolate(ecgo_sim* S, OSt* b, const OSlope* sl, double dist, double sign) {
-  /* Phase::extrapolate + verifyAndCorrectPhase + verifyAndCorrectDensityMax, MixUEq::extrapolate */
+  /* Phase::extrapolate + verifyAndCorrectPhase + verifyAndCorrectDensityMax, MixUEq::extrapolate,
+   * Transport::extrapolate */
+  for (int k = 0; k < S->c.ntr; k++) b->tr[k] += (sign * sl->tr[k]) * dist;
   if (S->c.model == ECGO_MODEL_EULER) {
     OPh* ph = &b->ph[0];
     ph->rho += (sign * sl->rho[0]) * dist;
@@ -1097,6 +1118,29 @@ static void extrapolate(ecgo_sim* S, OSt* b, const OSlope* sl, double dist, doub
     eos_rho_max(&S->c.eos[k], &ph->rho);
   }
   for (int d = 0; d < 3; d++) b->m.u[d] = b->m.u[d] + (sign * sl->u[d]) * dist;
+}
+
+/* THINC reconstruction of alpha_0 (and alpha_1 = 1 - alpha_0) at an interface cell, after the MUSCL
+ * extrapolation of that side (CellInterfaceO2Cartesian::solveRiemann
+ * src/Order2/CellInterfaceO2Cartesian.cpp:132-150 for the left side, :164-181 for the right side;
+ * the two sides use different final expressions there, kept as they are). */
+static void thinc(OSt* b, double aCell, double aOther, double aAfter, int right) {
+  const double beta = 1.6, eps = 1.e-4;
+  if (!((aCell >= eps) && (aCell <= 1. - eps) && ((aOther - aCell) * (aCell - aAfter) >= 1.e-8))) return;
+  /* left side: neighbours (right cell, left-left cell); right side: (right-right cell, left cell) */
+  double hi = right ? aAfter : aOther, lo = right ? aOther : aAfter;
+  double sign = (hi - lo > 0.) ? 1. : -1.;
+  double qmin = omin(hi, lo);
+  double qmax = omax(hi, lo) - qmin;
+  double C = (aCell - qmin + 1.e-20) / (qmax + 1.e-20);
+  double B = exp(sign * beta * (2. * C - 1.));
+  double A = (B / cosh(beta) - 1.) / tanh(beta);
+  double na = right ? qmin + 0.5 * qmax * (1. + sign * A)
+                    : qmin + 0.5 * qmax * (1. + sign * (tanh(beta) + A) / (1. + A * tanh(beta)));
+  if (na < eps) na = eps;
+  if (na > 1. - eps) na = 1. - eps;
+  b->ph[0].alpha = na;
+  b->ph[1].alpha = 1. - na;
 }
 
 static void flux_pass(ecgo_sim* S, OSt* prim, int o2, double* dtMax) {
@@ -1140,12 +1184,15 @@ static void flux_pass(ecgo_sim* S, OSt* prim, int o2, double* dtMax) {
       double aL = (S->c.model == ECGO_MODEL_EULER) ? 0. : bl.ph[0].alpha;
       double aR = (S->c.model == ECGO_MODEL_EULER) ? 0. : br.ph[0].alpha;
       OSlope sl;
+      double aLL = 0., aRR = 0.;
       memset(&sl, 0, sizeof(sl));
-      local_slopes(S, F->L, f, aL, aR, &sl);
+      local_slopes(S, F->L, f, aL, aR, &sl, &aLL);
       extrapolate(S, &bl, &sl, dG, 1.);
+      if (S->thinc) thinc(&bl, aL, aR, aLL, 0);
       memset(&sl, 0, sizeof(sl));
-      local_slopes(S, F->R, f, aR, aL, &sl);
+      local_slopes(S, F->R, f, aR, aL, &sl, &aRR);
       extrapolate(S, &br, &sl, dD, -1.);
+      if (S->thinc) thinc(&br, aR, aL, aRR, 1);
       fulfill(S, &bl);
       fulfill(S, &br);
       riemann(S, &bl, &br, F, S->lcfl[F->L], S->lcfl[F->R], dtMax, &fl);
@@ -1175,6 +1222,7 @@ static void step_o1(ecgo_sim* S, double dt, double* dtMax) {
     build_cons(S, &S->s[i], &Un);
     time_evolve(S, &S->cons[i], &Un, dt);
     build_prim(S, &S->cons[i], &S->s[i]);
+    for (int k = 0; k < S->c.ntr; k++) S->s[i].tr[k] += S->cons[i].tr[k] * dt; /* Cell::timeEvolution :294-298 */
   }
   solve_relaxations(S);
 }
@@ -1191,6 +1239,8 @@ static void step_o2(ecgo_sim* S, double dt, double* dtMax) {
     time_evolve(S, &S->cons[i], &Un, 0.5 * dt);
     S->s2[i] = S->s[i];
     build_prim(S, &S->cons[i], &S->s2[i]);
+    for (int k = 0; k < S->c.ntr; k++) /* CellO2::predictionOrdre2 :121-125 */
+      S->s2[i].tr[k] = S->s[i].tr[k] + S->cons[i].tr[k] * (0.5 * dt);
     relaxations(S, &S->s2[i]);
     if (S->c.model != ECGO_MODEL_EULER) correction_energy(S, &S->s2[i]);
     fulfill(S, &S->s2[i]);
@@ -1204,13 +1254,16 @@ static void step_o2(ecgo_sim* S, double dt, double* dtMax) {
     build_cons(S, &S->s[i], &Un);
     time_evolve(S, &S->cons[i], &Un, dt);
     build_prim(S, &S->cons[i], &S->s[i]);
+    for (int k = 0; k < S->c.ntr; k++) S->s[i].tr[k] += S->cons[i].tr[k] * dt;
   }
   solve_relaxations(S);
 }
 
 /* -------------------------------------------------------------------------------------------- API */
 
-ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u) {
+ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u,
+                      const double* tr) {
+  if (c->ntr < 0 || c->ntr > NT_MAX || (c->ntr > 0 && !tr)) return NULL;
   ecgo_sim* S = (ecgo_sim*)calloc(1, sizeof(ecgo_sim));
   S->c = *c;
   S->np = (c->model == ECGO_MODEL_EULER) ? 1 : c->nphases;
@@ -1225,6 +1278,7 @@ ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho
   S->slopes = (OSlope*)calloc((size_t)(S->nfaces > 0 ? S->nfaces : 1), sizeof(OSlope));
   for (int i = 0; i < n; i++) {
     OSt* st = &S->s[i];
+    for (int k = 0; k < c->ntr; k++) st->tr[k] = tr[(size_t)k * n + i];
     if (c->model == ECGO_MODEL_EULER) {
       st->ph[0].rho = rho[i];
       st->ph[0].p = p[i];
@@ -1243,6 +1297,7 @@ ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho
       st->m.E = st->m.e + 0.5 * sqnorm(st->m.u); /* MixUEq::computeTotalEnergy :166 */
     }
   }
+  S->thinc = (c->order == 2) && (c->lim[2] == ECGO_LIM_THINC || c->lim[3] == ECGO_LIM_THINC);
   if (c->ptmu) { /* Mixture::computeCriticalPressure src/Models/Mixture.cpp:146 */
     const ecgo_eos* L = &c->eos[c->ptmu_liq];
     const ecgo_eos* V = &c->eos[c->ptmu_vap];
@@ -1271,6 +1326,11 @@ int ecgo_step(ecgo_sim* S, int nsteps, double* dt, double* t, ecgo_stats* st) {
   }
   if (st) *st = S->st;
   return 0;
+}
+
+void ecgo_get_transports(const ecgo_sim* S, double* tr) {
+  for (int k = 0; k < S->c.ntr; k++)
+    for (int i = 0; i < S->n; i++) tr[(size_t)k * S->n + i] = S->s[i].tr[k];
 }
 
 void ecgo_get(const ecgo_sim* S, double* alpha, double* rho, double* T, double* Y, double* rho_mix, double* p,

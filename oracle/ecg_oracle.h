@@ -10,7 +10,7 @@
  *
  * Layout of state arrays passed across this interface (n = number of cells,
  * cell index i + j*nx + k*nx*ny, reference src/Meshes/MeshCartesian.cpp:141):
- *   alpha[k*n + c], rho[k*n + c] for k < nphases, p[c], u[d*n + c] (d < 3), E[c]
+ *   alpha[k*n + c], rho[k*n + c] for k < nphases, p[c], u[d*n + c] (d < 3), E[c], tr[k*n + c] (k < ntr)
  */
 #ifndef ECG_ORACLE_H
 #define ECG_ORACLE_H
@@ -44,6 +44,7 @@ typedef struct {
   int ptmu, ptmu_liq, ptmu_vap;
   ecgo_eos eos[3];
   int bc[6];       /* ECGO_BC_* per side */
+  int ntr;         /* passive transports (0..4) */
 } ecgo_case;
 
 typedef struct {
@@ -59,7 +60,8 @@ typedef struct ecgo_sim ecgo_sim;
 /* Build a simulation from the initial primitive state (per-phase alpha, rho,
  * mixture pressure given to every phase, mixture velocity); total energy is
  * completed as in Cell::completeFulfillState (src/Order1/Cell.cpp:344). */
-ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u);
+ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u,
+                      const double* tr);
 void ecgo_destroy(ecgo_sim* s);
 /* Advance nsteps time steps.  *dt is the step to take first (1e-15 at start,
  * src/Run.cpp:38); on return it holds the next step cfl*dtMax (src/Run.cpp:439). */
@@ -68,6 +70,8 @@ int ecgo_step(ecgo_sim* s, int nsteps, double* dt, double* t, ecgo_stats* st);
  * mixture density, mixture pressure (sum alpha_k p_k), total energy, velocity. */
 void ecgo_get(const ecgo_sim* s, double* alpha, double* rho, double* T, double* Y, double* rho_mix, double* p,
               double* E, double* u);
+/* Passive transport values tr[k*n + c]. */
+void ecgo_get_transports(const ecgo_sim* s, double* tr);
 /* Per-phase pressures and the mixture internal energy (diagnostics). */
 void ecgo_get_phase_pressure(const ecgo_sim* s, double* pk);
 

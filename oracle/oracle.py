@@ -34,7 +34,7 @@ class Case(C.Structure):
                 ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("cfl", C.c_double),
                 ("lim", C.c_int * 4), ("ptmu", C.c_int), ("ptmu_liq", C.c_int), ("ptmu_vap", C.c_int),
-                ("eos", Eos * 3), ("bc", C.c_int * 6)]
+                ("eos", Eos * 3), ("bc", C.c_int * 6), ("ntr", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -60,7 +60,8 @@ def lib():
         L = C.CDLL(LIB_PATH)
         dp = C.POINTER(C.c_double)
         L.ecgo_create.restype = C.c_void_p
-        L.ecgo_create.argtypes = [C.POINTER(Case), dp, dp, dp, dp]
+        L.ecgo_create.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
+        L.ecgo_get_transports.argtypes = [C.c_void_p, dp]
         L.ecgo_destroy.argtypes = [C.c_void_p]
         L.ecgo_step.argtypes = [C.c_void_p, C.c_int, dp, dp, C.POINTER(Stats)]
         L.ecgo_get.argtypes = [C.c_void_p] + [dp] * 8
@@ -103,6 +104,7 @@ def make_case(case) -> Case:
         c.eos[k] = Eos(EOS_CODE[e.kind], e.gamma, e.pinf, e.b, e.cv, e.eref, e.sref)
     for i, b in enumerate(case.boundary_types()):
         c.bc[i] = BC_CODE[b.upper()]
+    c.ntr = len(case.transports or [])
     return c
 
 
@@ -161,6 +163,8 @@ def initial_fields(case) -> Dict[str, np.ndarray]:
     rho = np.zeros((npf, n))
     p = np.zeros(n)
     u = np.zeros((3, n))
+    names = list(case.transports or [])
+    tr = np.zeros((len(names), n))
     states = {s.name: s for s in case.states}
     for d in case.domains:
         m = _belongs(d, X, Y, Z)
@@ -176,7 +180,9 @@ def initial_fields(case) -> Dict[str, np.ndarray]:
         p[m] = st.pressure
         for dd in range(3):
             u[dd, m] = st.velocity[dd]
-    return {"alpha": alpha, "rho": rho, "p": p, "u": u}
+        for j, name in enumerate(names):  # a state without the transport leaves 0 (Input.cpp:1034-1050)
+            tr[j, m] = (st.transports or {}).get(name, 0.0)
+    return {"alpha": alpha, "rho": rho, "p": p, "u": u, "tr": tr}
 
 
 class Sim:
@@ -192,7 +198,12 @@ class Sim:
         r = np.ascontiguousarray(f["rho"], dtype=np.float64)
         p = np.ascontiguousarray(f["p"], dtype=np.float64)
         u = np.ascontiguousarray(f["u"], dtype=np.float64)
-        self.h = lib().ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u))
+        self.ntr = self.c.ntr
+        tr = np.ascontiguousarray(f.get("tr", np.zeros((self.ntr, self.n))), dtype=np.float64)
+        self._tr = tr
+        self.h = lib().ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u), _p(tr) if self.ntr else None)
+        if not self.h:
+            raise ValueError("ecgo_create refused the case")
         self.dt = C.c_double(1e-15)
         self.t = C.c_double(0.0)
         self.iteration = 0
@@ -213,6 +224,9 @@ class Sim:
                "rho_mix": np.zeros(n), "p": np.zeros(n), "E": np.zeros(n), "u": np.zeros((3, n))}
         lib().ecgo_get(self.h, _p(out["alpha"]), _p(out["rho"]), _p(out["T"]), _p(out["Y"]), _p(out["rho_mix"]),
                        _p(out["p"]), _p(out["E"]), _p(out["u"]))
+        out["tr"] = np.zeros((self.ntr, n))
+        if self.ntr:
+            lib().ecgo_get_transports(self.h, _p(out["tr"]))
         return out
 
     def phase_pressures(self) -> np.ndarray:

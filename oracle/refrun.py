@@ -106,13 +106,23 @@ def info(work: str, run_name: str):
     return int(last[1]), float(last[2]), float(last[3])
 
 
+def _transports(fields: Dict[str, np.ndarray]):
+    """Passive transports, written as T1, T2, ... (OutputXML::writePhysicalDataXML)."""
+    out, k = [], 1
+    while f"T{k}" in fields:
+        out.append(fields[f"T{k}"])
+        k += 1
+    return np.stack(out) if out else None
+
+
 def reference_prim(fields: Dict[str, np.ndarray], nphases: int):
-    """Map reference output names to (alpha[k], rho[k], p, u[3], E) arrays (PUEq or Euler output)."""
+    """Map reference output names to (alpha[k], rho[k], p, u[3], E, tr) arrays (PUEq or Euler output)."""
     if "Pressure_Mixture" not in fields:  # Euler: PhaseEuler scalars + velocity (no total energy written)
         get = lambda pre: [v for n, v in fields.items() if n.startswith(pre)][0]
         rho = get("F0_Density")
         return {"alpha": np.ones((1, rho.size)), "rho": rho[None, :], "p": get("F0_Pressure"),
-                "u": get("F0_Velocity").T.copy(), "E": None, "rho_mix": rho, "T": get("F0_Temperature")[None, :]}
+                "u": get("F0_Velocity").T.copy(), "E": None, "rho_mix": rho, "T": get("F0_Temperature")[None, :],
+                "tr": _transports(fields)}
     alpha, rho = [], []
     for k in range(nphases):
         a = [v for n, v in fields.items() if n.startswith(f"F{k}_Alpha")]
@@ -127,4 +137,5 @@ def reference_prim(fields: Dict[str, np.ndarray], nphases: int):
         "E": fields["Total_energy_Mixture"],
         "rho_mix": fields["Density_Mixture"],
         "T": np.stack([[v for n, v in fields.items() if n.startswith(f"F{k}_Temperature")][0] for k in range(nphases)]),
+        "tr": _transports(fields),
     }

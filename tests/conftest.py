@@ -28,6 +28,8 @@ def display(field, name):
         return np.where(field < 1e-20, 0.0, field)
     if name == "rho":
         return np.where(field < 1e-20, 1e-20, field)
+    if name == "tr":  # MeshCartesian::getData src/Meshes/MeshCartesian.cpp:1832-1836
+        return np.where(field < 1e-20, 0.0, field)
     return field
 
 

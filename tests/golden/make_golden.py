@@ -64,6 +64,36 @@ def golden_cases():
     c = cases.euler_shock_tube(ncells=100, iterations=80, order="vanleer", name="eulerWall")
     c.boundaries = ["wall", "symmetry"]
     g["euler1d_wall_o2"] = c
+    # THINC volume-fraction reconstruction (everywhere, and at interfaces only)
+    c = cases.shock_tube_1d(ncells=200, iterations=60, order="vanleer", name="tubeTHINC")
+    c.vf_limiter, c.interface_vf_limiter = "THINC", "THINC"
+    g["tube1d_thinc_o2"] = c
+    c = cases.shock_bubble_2d(n=24, iterations=10, limiter="minmod", name="bubbleTHINC")
+    c.interface_vf_limiter = "THINC"
+    c.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry"]
+    g["bubble2d_thinc"] = c
+    # passive transports (a colour function of the bubble and a second marker)
+    c = cases.shock_tube_1d(ncells=150, iterations=50, order="vanleer", name="tubeTransport")
+    c.transports = ["color", "marker"]
+    c.states[0].transports = {"color": 1.0, "marker": 0.25}
+    c.states[1].transports = {"color": 0.0}
+    c.boundaries = ["nonReflecting", "wall"]
+    g["tube1d_transport_o2"] = c
+    c = cases.shock_bubble_2d(n=24, iterations=10, limiter="vanleer", name="bubbleTransport")
+    c.transports = ["color"]
+    for st in c.states:
+        st.transports = {"color": 1.0 if st.phases[0].alpha < 0.5 else 0.0}
+    c.interface_vf_limiter = "THINC"
+    c.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry"]
+    g["bubble2d_transport"] = c
+    c = cases.shock_tube_1d(ncells=120, iterations=40, name="tubeTransportO1")
+    c.transports = ["color"]
+    c.states[0].transports = {"color": 1.0}
+    g["tube1d_transport_o1"] = c
+    c = cases.euler_shock_tube(ncells=100, iterations=40, order="minmod", name="eulerTransport")
+    c.transports = ["color"]
+    c.states[1].transports = {"color": 1.0}
+    g["euler1d_transport_o2"] = c
     g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
     return g
 

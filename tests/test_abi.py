@@ -114,3 +114,19 @@ def test_create_rejects_bad_cases_without_gpu_work():
     assert st == 2 and not h.value
     c.nphases, c.ncells[0] = 2, 1
     assert api.lib().ecg_create(api.C.byref(c), api.C.byref(h)) == 1
+
+
+def test_transports_read_and_filled(tmp_path):
+    """numberTransports, <transport name> of model.xml and the per-state values (0 when absent)."""
+    case = cases.shock_tube_1d(ncells=20, iterations=2)
+    case.transports = ["color", "marker"]
+    case.states[0].transports = {"color": 1.0, "marker": 0.25}
+    case.states[1].transports = {"marker": 2.0, "unknown": 7.0}
+    d = case.write(str(tmp_path))
+    inp = api.Input(d, os.path.join(str(tmp_path), "libEOS"))
+    assert inp.case.ntransports == 2
+    f = inp.fill()
+    assert len(f) == 2 * 2 + 5 + 2
+    ref = oracle.initial_fields(case)["tr"]
+    assert np.array_equal(np.stack(f[-2:]), ref)
+    assert set(np.unique(f[-2])) <= {0.0, 1.0} and set(np.unique(f[-1])) <= {0.25, 2.0}

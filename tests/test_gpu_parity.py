@@ -15,12 +15,13 @@ TOL = 1e-12
 KAPILA_KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_o2", "bubble2d_o2",
                "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
                "expansion2d_ptmu", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2", "bubble2d_sym_o1",
-               "cavity3d_wall_o2"]
-EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2"]
+               "cavity3d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc", "tube1d_transport_o2", "bubble2d_transport",
+               "tube1d_transport_o1"]
+EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2", "euler1d_transport_o2"]
 
 
 def _compare(key, got, g):
-    for name in ("alpha", "rho", "p", "u", "E"):
+    for name in ("alpha", "rho", "p", "u", "E", "tr"):
         ref = g.get("final_" + name)
         if ref is None:
             continue
@@ -86,6 +87,47 @@ def test_gpu_symmetry_sides_match_oracle_2d(order, tmp_path):
     for name in ("alpha", "rho", "p", "u", "E"):
         assert rel_l1(out[name], o[name]) <= TOL, name
     assert out["dt"] == pytest.approx(sim.dt.value, rel=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("vf", [("THINC", "THINC"), (None, "THINC")])
+def test_gpu_thinc_matches_oracle_2d(vf, tmp_path):
+    """THINC volume-fraction reconstruction on a mesh of several tiles per axis."""
+    from ecogen_b200 import cases
+    case = cases.shock_bubble_2d(n=64, iterations=25, limiter="vanleer", name="bubbleTHINC64")
+    case.vf_limiter, case.interface_vf_limiter = vf
+    case.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry"]
+    out = gpu_run(case, tmp_path)
+    sim = oracle.Sim(case)
+    sim.step(25)
+    o = sim.fields()
+    for name in ("alpha", "rho", "p", "u", "E"):
+        assert rel_l1(out[name], o[name]) <= TOL, name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_gpu_transports_match_oracle(dim, tmp_path):
+    """Two passive transports on meshes of several tiles per axis, with symmetry and open sides."""
+    from ecogen_b200 import cases
+    if dim == 2:
+        case = cases.shock_bubble_2d(n=60, iterations=20, limiter="vanleer", name="bubbleTransport60")
+        case.boundaries = ["wall", "nonReflecting", "symmetry", "nonReflecting"]
+        steps = 20
+    else:
+        case = cases.cavity_collapse_3d(n=14, iterations=4, ninclusions=5, radius_cells=(2.0, 4.0), name="cavityTr")
+        case.cells = (14, 9, 7)
+        case.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry", "nonReflecting", "wall"]
+        steps = 4
+    case.transports = ["color", "marker"]
+    for i, st in enumerate(case.states):
+        st.transports = {"color": float(i % 2), "marker": 0.5 * i}
+    out = gpu_run(case, tmp_path)
+    sim = oracle.Sim(case)
+    sim.step(steps)
+    o = sim.fields()
+    for name in ("alpha", "rho", "p", "u", "E", "tr"):
+        assert rel_l1(out[name], o[name]) <= TOL, name
 
 
 @pytest.mark.gpu

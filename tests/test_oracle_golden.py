@@ -12,7 +12,8 @@ from oracle import oracle
 KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_o2", "bubble2d_o2",
         "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
         "expansion2d_ptmu", "euler1d_o1", "euler1d_o2", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2",
-        "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2"]
+        "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc",
+        "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2"]
 
 
 @pytest.mark.parametrize("key", KEYS)
@@ -26,7 +27,7 @@ def test_oracle_matches_reference(key, golden_cases):
         sim.run_to_time(case.total_time)
     assert sim.iteration == meta["iterations_done"]
     o = sim.fields()
-    for name in ("alpha", "rho", "p", "u", "E"):
+    for name in ("alpha", "rho", "p", "u", "E", "tr"):
         ref = g.get("final_" + name)
         if ref is None:
             continue
