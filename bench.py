@@ -79,7 +79,7 @@ def pass_bytes_per_cell(case) -> dict:
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / cells, 2D two-phase MUSCL at 1536^2; profiles/k_kapila_step_shock_bubble_1536.md);
 # the kernels stream the state once, so traffic scales with the cell count.
-NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 192.52, ("kapila", 2, 2, True, "pass1"): 127.09}
+NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 195.72, ("kapila", 2, 2, True, "pass1"): 124.96}
 
 
 class ClockSampler:

@@ -39,7 +39,8 @@ class Case(C.Structure):
                 ("limiter", C.c_int32 * 4), ("ncells", C.c_int32 * 3), ("length", C.c_double * 3),
                 ("cfl", C.c_double), ("time_iterations", C.c_int32), ("max_iterations", C.c_int32),
                 ("total_time", C.c_double), ("ptmu", C.c_int32), ("ptmu_liquid", C.c_int32),
-                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6), ("ntransports", C.c_int32)]
+                ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6), ("ntransports", C.c_int32),
+                ("pt_relaxation", C.c_int32)]
 
 
 class StepStats(C.Structure):
@@ -183,6 +184,7 @@ def case_from_spec(spec) -> Case:
     for i, b in enumerate(spec.boundary_types()):
         c.bc[i] = BC_CODE[b.upper()]
     c.ntransports = len(spec.transports or [])
+    c.pt_relaxation = 1 if getattr(spec, "pt_relaxation", False) else 0
     return c
 
 

@@ -155,6 +155,7 @@ class Case:
     ptmu: Optional[Tuple[int, int]] = None  # (liquid phase, vapour phase)
     boundaries: Optional[List[str]] = None  # boundCond types Xm, Xp, Ym, Yp, Zm, Zp (default nonReflecting)
     transports: Optional[List[str]] = None  # names of passive transports (model.xml <transport>)
+    pt_relaxation: bool = False             # model.xml <relaxation type="PT"> (analytic p-T relaxation)
     output_format: str = "XML"
     output_binary: bool = True
     output_precision: Optional[int] = None  # outputMode precision (ASCII values, infoCalcul.out)
@@ -236,6 +237,8 @@ class Case:
             s += ('  <relaxation type="PTMu">\n'
                   f'    <dataPTMu liquid="{self.eos[liq].name}" vapor="{self.eos[vap].name}"/>\n'
                   '  </relaxation>\n')
+        if self.pt_relaxation:
+            s += '  <relaxation type="PT"/>\n'
         return s + "</model>\n"
 
     def ic_xml(self) -> str:

@@ -135,6 +135,11 @@ ecg_status validate_case(const ecg_case* c) {
     if (c->bc[i] != ECG_BC_NONREFLECTING && c->bc[i] != ECG_BC_SYMMETRY) { set_error("bad boundary condition"); return ECG_ERR_INVALID; }
   if (c->ntransports < 0) { set_error("negative number of transports"); return ECG_ERR_INVALID; }
   if (c->ntransports > 2) { set_error("more than two passive transports"); return ECG_ERR_UNSUPPORTED; }
+  if (c->pt_relaxation) {
+    if (c->model != ECG_MODEL_KAPILA || c->nphases != 2 || c->ptmu) { set_error("PT relaxation: two Kapila phases, without PTMu"); return ECG_ERR_UNSUPPORTED; }
+    for (int k = 0; k < 2; k++)
+      if (c->eos[k].type == ECG_EOS_NASG) { set_error("PT relaxation needs IG or SG phases"); return ECG_ERR_UNSUPPORTED; }
+  }
   if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
   int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
   if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
@@ -177,6 +182,7 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.rec_max = x->rec_max;
   P.rec_min_evals = x->rec_min_evals;
   P.ntr = x->c.ntransports;
+  P.pt = x->c.pt_relaxation;
   set_thinc(P, x->c);
   P.ptmu = x->c.ptmu;
   P.ptmu_liq = x->c.ptmu_liquid;

@@ -52,8 +52,9 @@ struct BatchTile {
   }
 };
 
-template <int NP, int TB, int PASS>
-__global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
+template <int NP, int TB, int PASS, int TYPES>
+__global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M0) {
+  const Model<NP> M = specialize_eos<NP, TYPES>(M0);  // EOS types compiled in for the shipped workload
   using FL = Fields<NP, 1>;
   using K = BatchTile<NP, TB, PASS>;
   constexpr bool O2 = (PASS != PASS_O1);
@@ -132,8 +133,10 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
         double aLL = hasL ? a0[rl - 1] : 0., aRR = hasR ? a0[rr + 1] : 0.;
         double pl = (gl + 0.5) * C.dx, pf = pl + 0.5 * C.dx, pr = (gl + 1 + 0.5) * C.dx;
         double y = pf - pl, z = pf - pr;
-        reconstruct_side<NP, 1>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1., tl, ug);
-        reconstruct_side<NP, 1>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z), -1.,
+        constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
+        reconstruct_side<NP, 1, kThinc>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1., tl,
+                                        ug);
+        reconstruct_side<NP, 1, kThinc>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z), -1.,
                                 tr, vg);
       }
       double Fn[3];
@@ -195,9 +198,9 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M) {
       const int64_t cell = C.off + g;
       CellCounters cc;
       if (seeded)
-        kapila_finish<NP, 1, PASS, false, true>(P, M, nn, cell, cp, sg, cc);
+        kapila_finish<NP, 1, PASS, false, true, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
       else
-        kapila_finish<NP, 1, PASS, false, false>(P, M, nn, cell, cp, sg, cc);
+        kapila_finish<NP, 1, PASS, false, false, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
       total.relax += cc.relax;
       total.iters += cc.iters;
       total.fallback += cc.fallback;
@@ -238,10 +241,10 @@ __global__ void k_batch_finalize(BatchScalars* s, const BatchCase* cases, int nc
   s[c].dtmax_bits = (unsigned long long)__double_as_longlong(1.e10);
 }
 
-template <int NP, int TB, int PASS>
+template <int NP, int TB, int PASS, int TYPES>
 static cudaError_t batch_one(const BatchParams& B, const ecg_eos* eos, double eps, int grid, cudaStream_t s,
                              bool prepare, int* max_blocks) {
-  auto kern = k_batch<NP, TB, PASS>;
+  auto kern = k_batch<NP, TB, PASS, TYPES>;
   const size_t base = BatchTile<NP, TB, PASS>::smem_bytes();
   const size_t sm = base;
   if (prepare) {
@@ -256,16 +259,23 @@ static cudaError_t batch_one(const BatchParams& B, const ecg_eos* eos, double ep
   return cudaGetLastError();
 }
 
-template <int NP, int TB>
+template <int NP, int TB, int TYPES = EOS_DYNAMIC>
 static cudaError_t batch_tb(int pass, const BatchParams& B, const ecg_eos* eos, double eps, int grid, cudaStream_t s,
                             bool prepare, int* mb) {
-  if (pass == PASS_O1) return batch_one<NP, TB, PASS_O1>(B, eos, eps, grid, s, prepare, mb);
-  if (pass == PASS_PRED) return batch_one<NP, TB, PASS_PRED>(B, eos, eps, grid, s, prepare, mb);
-  return batch_one<NP, TB, PASS_CORR>(B, eos, eps, grid, s, prepare, mb);
+  if (pass == PASS_O1) return batch_one<NP, TB, PASS_O1, TYPES>(B, eos, eps, grid, s, prepare, mb);
+  if (pass == PASS_PRED) return batch_one<NP, TB, PASS_PRED, TYPES>(B, eos, eps, grid, s, prepare, mb);
+  return batch_one<NP, TB, PASS_CORR, TYPES>(B, eos, eps, grid, s, prepare, mb);
 }
 
+// fast: two phases, SG liquid then ideal gas, no THINC -- the kernels with the EOS types compiled in
 static cudaError_t batch_launch(int np, int tb, int pass, const BatchParams& B, const ecg_eos* eos, double eps,
-                                int grid, cudaStream_t s, bool prepare, int* mb) {
+                                int grid, cudaStream_t s, bool prepare, int* mb, bool fast) {
+  constexpr int kSgIg = eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG);
+  if (np == 2 && fast) {
+    if (tb == 64) return batch_tb<2, 64, kSgIg>(pass, B, eos, eps, grid, s, prepare, mb);
+    if (tb == 128) return batch_tb<2, 128, kSgIg>(pass, B, eos, eps, grid, s, prepare, mb);
+    return batch_tb<2, 256, kSgIg>(pass, B, eos, eps, grid, s, prepare, mb);
+  }
   if (np == 2) {
     if (tb == 64) return batch_tb<2, 64>(pass, B, eos, eps, grid, s, prepare, mb);
     if (tb == 128) return batch_tb<2, 128>(pass, B, eos, eps, grid, s, prepare, mb);
@@ -282,6 +292,7 @@ using namespace ecg;
 
 struct ecg_batch {
   ecg_case c0;
+  bool fast = false;  // kernels with the EOS types compiled in apply
   int ncases = 0, np = 2, order = 1, nstate = 0, nq = 0;
   int64_t total = 0;
   double eps = 0.;
@@ -351,7 +362,7 @@ ecg_status set_shape(ecg_batch* b, int tile) {
   BatchParams B{};
   for (int pass = 0; pass < 3; pass++) {
     int mb = 0;
-    BCUDA(batch_launch(b->np, tile, pass, B, b->c0.eos, b->eps, 0, b->stream, true, &mb));
+    BCUDA(batch_launch(b->np, tile, pass, B, b->c0.eos, b->eps, 0, b->stream, true, &mb, b->fast));
     if ((b->order == 1 && pass == PASS_O1) || (b->order == 2 && pass != PASS_O1)) occ = std::min(occ, std::max(mb, 1));
   }
   b->tile = tile;
@@ -374,13 +385,14 @@ ecg_status launch_pass(ecg_batch* b, int pass, double* q, double* sn, double* ou
   for (int i = 0; i < 4; i++) B.P.lim[i] = b->c0.limiter[i];
   B.P.newton_cap = b->newton_cap;
   set_thinc(B.P, b->c0);
+  B.P.pt = b->c0.pt_relaxation;
   B.P.mlp = b->mlp;
   B.cases = b->cases;
   B.scal = b->scal;
   B.items = b->items;
   B.nitems = b->nitems;
   B.queue = queue;
-  BCUDA(batch_launch(b->np, b->tile, pass, B, b->c0.eos, b->eps, b->grid, b->stream, false, nullptr));
+  BCUDA(batch_launch(b->np, b->tile, pass, B, b->c0.eos, b->eps, b->grid, b->stream, false, nullptr, b->fast));
   return ECG_OK;
 }
 
@@ -456,13 +468,16 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
       return ECG_ERR_UNSUPPORTED;
     }
     if (x.model != c0.model || x.nphases != c0.nphases || x.order != c0.order || x.alpha_null != c0.alpha_null ||
-        std::memcmp(x.limiter, c0.limiter, sizeof(x.limiter)) != 0 || std::memcmp(x.eos, c0.eos, sizeof(x.eos)) != 0) {
+        std::memcmp(x.limiter, c0.limiter, sizeof(x.limiter)) != 0 || std::memcmp(x.eos, c0.eos, sizeof(x.eos)) != 0 ||
+        x.pt_relaxation != c0.pt_relaxation) {
       set_error("all cases of a batch share model, phases, EOS, order, limiters and alphaNull");
       return ECG_ERR_INVALID;
     }
   }
   auto b = new ecg_batch();
   b->c0 = c0;
+  b->fast = c0.nphases == 2 && c0.eos[0].type == ECG_EOS_SG && c0.eos[1].type == ECG_EOS_IG && !c0.pt_relaxation &&
+            !(c0.order == 2 && (c0.limiter[2] == ECG_LIM_THINC || c0.limiter[3] == ECG_LIM_THINC));
   b->ncases = ncases;
   b->np = c0.nphases;
   b->order = c0.order;

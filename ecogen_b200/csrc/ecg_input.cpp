@@ -285,6 +285,13 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
       if (c.ptmu_liquid < 0 || c.ptmu_vapor < 0) return bail(ECG_ERR_XML, "model.xml: dataPTMu names no model EOS");
       for (int k = 0; k < 2; k++)
         if (c.eos[k].type == ECG_EOS_NASG) return bail(ECG_ERR_UNSUPPORTED, "PTMu saturation needs IG or SG phases");
+    } else if (t == "PT") {  // RelaxationPT (Input.cpp:834-840), appended after the pressure relaxation
+      if (c.pt_relaxation) return bail(ECG_ERR_XML, "model.xml: PT relaxation given twice");
+      if (c.model != ECG_MODEL_KAPILA || c.nphases != 2)
+        return bail(ECG_ERR_UNSUPPORTED, "PT relaxation is built for two phases");
+      for (int k = 0; k < 2; k++)
+        if (c.eos[k].type == ECG_EOS_NASG) return bail(ECG_ERR_UNSUPPORTED, "PT relaxation needs IG or SG phases");
+      c.pt_relaxation = 1;
     } else if (t == "P") {
       std::string sp = upper(r->attr("speed"));
       if (sp == "FINITE") return bail(ECG_ERR_UNSUPPORTED, "finite-rate pressure relaxation is not supported");
@@ -292,6 +299,7 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
       return bail(ECG_ERR_UNSUPPORTED, "relaxation " + t + " is not supported");
     }
   }
+  if (c.ptmu && c.pt_relaxation) return bail(ECG_ERR_UNSUPPORTED, "PTMu and PT relaxations together are not built");
 
   // ---------------------------------------------------------------- initialConditions.xml (:917)
   auto icx = ecg::xml::parse_file(dir + "initialConditions.xml", &err);

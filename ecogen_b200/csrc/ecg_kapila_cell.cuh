@@ -350,7 +350,47 @@ __device__ __forceinline__ void seed_gate(const StepParams& P, const Model<NP>& 
 // relaxation continues from the seed gate (see seed_gate); a hard cell restarts Newton from the
 // network's seed when it is finite and inside the bracket of the phase pressures, otherwise it
 // continues the plain iteration.  Newton still stops at |f| <= 1e-10 either way.
-template <int NP, int DIM, int PASS, bool PTMU, bool SEED = false>
+// RelaxationPT::relaxation src/Relaxations/RelaxationPT.cpp:43-140: analytic pressure-temperature
+// equilibrium of two IG/SG phases (Le Martelot 2013) from the mixture energy and density of the rebuilt
+// state (emix, rho0) and its mass fractions, then rho_k = computeDensity(p*, T*).
+template <int NP>
+__device__ __forceinline__ void relax_pt(const Model<NP>& M, double a[NP], double r[NP], double pk[NP],
+                                         const double Y[NP], double emix, double rho0) {
+  if (M.eps > 1.e-20) {
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+      if (a[k] > (1. - 1.e-5)) return;
+  }
+  const EosParams& E1 = M.eos[0];
+  const EosParams& E2 = M.eos[1];
+  const double pInf1 = (E1.type == ECG_EOS_IG) ? 0. : E1.pinf, pInf2 = (E2.type == ECG_EOS_IG) ? 0. : E2.pinf;
+  const double q = Y[0] * E1.eref + Y[1] * E2.eref;
+  const double cvMel = Y[0] * E1.cv + Y[1] * E2.cv;
+  const double A1 = Y[0] * (E1.gamma - 1.) * E1.cv / cvMel * (rho0 * (emix - q) - pInf1);
+  const double A2 = Y[1] * (E2.gamma - 1.) * E2.cv / cvMel * (rho0 * (emix - q) - pInf2);
+  const double pressure = 0.5 * (A1 + A2 - (pInf1 + pInf2)) +
+                          sqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
+  double temperature = 0.;
+  temperature += Y[0] * (E1.gamma - 1.) * E1.cv / (pressure + pInf1);
+  temperature += Y[1] * (E2.gamma - 1.) * E2.cv / (pressure + pInf2);
+  temperature = 1. / (temperature * rho0);
+  double rS[2], aS[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const EosParams& E = M.eos[k];
+    const double den = dmax((E.gamma - 1.) * E.cv * temperature, M.eps);
+    rS[k] = (E.type == ECG_EOS_IG) ? pressure / den : (pressure + E.pinf) / den;
+    aS[k] = a[k] * r[k] / rS[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    a[k] = aS[k];
+    r[k] = rS[k];
+    pk[k] = pressure;
+  }
+}
+
+template <int NP, int DIM, int PASS, bool PTMU, bool SEED = false, bool XPT = true>
 __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
                                               CellPrim<NP, DIM>& cp, const SeedGate<NP>& g, CellCounters& cc) {
   using FL = Fields<NP, DIM>;
@@ -416,6 +456,16 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
       for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
     }
     if (err) cc.ptmu = 1;
+  }
+  if (XPT && !PTMU && NP == 2 && P.pt) {
+    // RelaxationPT reads the mass fractions and mixture energy of the rebuilt state
+    double Y[NP], emix = 0.;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      Y[k] = a0[k] * r0[k] / dmax(rhomix, M.eps);
+      emix += Y[k] * eos_e(M.eos[k], M.eps, r0[k], p0[k]);
+    }
+    relax_pt<NP>(M, a, r, pk, Y, emix, rhomix);
   }
 
   // ---- energy correction (FluxPUEq::correctionEnergy) and clamps

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH, TileShape
   // learned seed of the pressure relaxation, gated on the plain start (all lanes of the warp)
   SeedGate<NP> sg;
   if (SEED) seed_gate<NP, DIM>(P, M, active, cp, sg);
-  if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED>(P, M, nn, cell, cp, sg, cc);
+  if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
 
   // ---- dtMax: block min, one atomic per block

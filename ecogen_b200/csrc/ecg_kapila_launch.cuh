@@ -42,8 +42,8 @@ cudaError_t kapila_launch_tr(int np, int dim, bool ptmu, int pass, const StepPar
 constexpr int KAPILA_MAX_TRANSPORTS = 2;
 
 // The EOS combination of the shipped workloads (SG liquid first, ideal gases after) has kernels
-// (plain and seeded) with the types compiled in and no THINC code; every other case (other EOS,
-// THINC, passive transports, p-T-mu) runs the generic kernels.
+// (plain and seeded) with the types compiled in and no THINC or PT-relaxation code; every other
+// case (other EOS, THINC, PT relaxation, passive transports, p-T-mu) runs the generic kernels.
 template <int NP>
 constexpr int eos_fast_types() {
   return NP == 2 ? eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG) : eos_types_code<3>(ECG_EOS_SG, ECG_EOS_IG, ECG_EOS_IG);
@@ -80,12 +80,12 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
   }
   if (P.mlp != nullptr) {
     if (PTMU) return cudaErrorNotSupported;
-    if (kFast && !P.thinc && eos_is_fast<NP>(eos))
+    if (kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos))
       return launch_pass_seed<NP, DIM, PTMU, true, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
                                                                                                  false);
     return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, false);
   }
-  if (kFast && !P.thinc && eos_is_fast<NP>(eos))
+  if (kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos))
     return launch_pass_seed<NP, DIM, PTMU, false, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
                                                                                                 false);
   return launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, false);

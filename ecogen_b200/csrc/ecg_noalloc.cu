@@ -181,6 +181,7 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
   for (int i = 0; i < 4; i++) P.lim[i] = c->limiter[i];
   P.newton_cap = 100;
   set_thinc(P, *c);
+  P.pt = c->pt_relaxation;
   P.ptmu = c->ptmu;
   P.ptmu_liq = c->ptmu_liquid;
   P.ptmu_vap = c->ptmu_vapor;

@@ -120,6 +120,8 @@ struct StepParams {
   double thinc_cosh, thinc_tanh;
   // passive transports: stored after the NS fields of a state (at NS + j), j < ntr
   int ntr;
+  // analytic pressure-temperature relaxation after the pressure one (two phases)
+  int pt;
 };
 
 // Host side of the THINC parameters (CellInterfaceO2Cartesian::solveRiemann's beta = 1.6).

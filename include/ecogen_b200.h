@@ -76,6 +76,7 @@ typedef struct {
   ecg_eos eos[ECG_MAX_PHASES];
   int32_t bc[6];                /* ECG_BC_* of the sides Xm, Xp, Ym, Yp, Zm, Zp (MeshCartesian::assignLimits) */
   int32_t ntransports;          /* passive transports (model.xml numberTransports, src/Transport), 0..2 */
+  int32_t pt_relaxation;        /* model.xml <relaxation type="PT">: analytic p-T relaxation (RelaxationPT) */
 } ecg_case;
 
 /* Counters of one ecg_step call (replace the reference's errors / warnings vectors). */

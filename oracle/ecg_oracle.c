@@ -769,10 +769,52 @@ static void relax_ptmu(ecgo_sim* S, OSt* st) {
   fulfill(S, st);
 }
 
+/* RelaxationPT::relaxation src/Relaxations/RelaxationPT.cpp:43-140: analytic pressure-temperature
+ * equilibrium of two IG/SG phases (Le Martelot 2013) from the mixture energy and density and the
+ * mass fractions of the rebuilt state, then rho_k = computeDensity(p*, T*). */
+static void relax_pt(ecgo_sim* S, OSt* st) {
+  if (S->eps > 1.e-20)
+    for (int k = 0; k < S->np; k++)
+      if (st->ph[k].alpha > (1. - 1.e-5)) return;
+  const ecgo_eos* E1 = &S->c.eos[0];
+  const ecgo_eos* E2 = &S->c.eos[1];
+  double e0 = st->m.e, rho0 = st->m.rho;
+  double gamma1 = E1->gamma, pInf1 = (E1->type == ECGO_EOS_IG) ? 0. : E1->pinf, cv1 = E1->cv, e01 = E1->eref;
+  double gamma2 = E2->gamma, pInf2 = (E2->type == ECGO_EOS_IG) ? 0. : E2->pinf, cv2 = E2->cv, e02 = E2->eref;
+  double Y1 = st->ph[0].Y, Y2 = st->ph[1].Y;
+  double q = Y1 * e01 + Y2 * e02;
+  double cvMel = Y1 * cv1 + Y2 * cv2;
+  double A1 = Y1 * (gamma1 - 1.) * cv1 / cvMel * (rho0 * (e0 - q) - pInf1);
+  double A2 = Y2 * (gamma2 - 1.) * cv2 / cvMel * (rho0 * (e0 - q) - pInf2);
+  double pressure = 0.5 * (A1 + A2 - (pInf1 + pInf2)) +
+                    sqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
+  double temperature = 0.;
+  for (int k = 0; k < 2; k++) {
+    const ecgo_eos* E = &S->c.eos[k];
+    double pInfk = (E->type == ECGO_EOS_IG) ? 0. : E->pinf;
+    temperature += st->ph[k].Y * (E->gamma - 1.) * E->cv / (pressure + pInfk);
+  }
+  temperature = 1. / (temperature * rho0);
+  double rhoS[2], aS[2];
+  for (int k = 0; k < 2; k++) {
+    const ecgo_eos* E = &S->c.eos[k];
+    double den = omax(((E->gamma - 1.) * E->cv * temperature), S->eps);
+    rhoS[k] = (E->type == ECGO_EOS_IG) ? pressure / den : (pressure + E->pinf) / den;
+    aS[k] = st->ph[k].alpha * st->ph[k].rho / rhoS[k];
+  }
+  for (int k = 0; k < 2; k++) {
+    st->ph[k].alpha = aS[k];
+    st->ph[k].rho = rhoS[k];
+    st->ph[k].p = pressure;
+  }
+  st->m.p = pressure;
+}
+
 static void relaxations(ecgo_sim* S, OSt* st) { /* Model::relaxations src/Models/Model.cpp:74 */
   if (S->c.model == ECGO_MODEL_EULER) return;
   relax_pinf(S, st);
   if (S->c.ptmu) relax_ptmu(S, st);
+  if (S->c.pt) relax_pt(S, st);
 }
 
 static void correction_energy(ecgo_sim* S, OSt* st) {

@@ -45,6 +45,7 @@ typedef struct {
   ecgo_eos eos[3];
   int bc[6];       /* ECGO_BC_* per side */
   int ntr;         /* passive transports (0..4) */
+  int pt;          /* model.xml <relaxation type="PT">: analytic p-T relaxation after the pressure one */
 } ecgo_case;
 
 typedef struct {

@@ -34,7 +34,7 @@ class Case(C.Structure):
                 ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("cfl", C.c_double),
                 ("lim", C.c_int * 4), ("ptmu", C.c_int), ("ptmu_liq", C.c_int), ("ptmu_vap", C.c_int),
-                ("eos", Eos * 3), ("bc", C.c_int * 6), ("ntr", C.c_int)]
+                ("eos", Eos * 3), ("bc", C.c_int * 6), ("ntr", C.c_int), ("pt", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -105,6 +105,7 @@ def make_case(case) -> Case:
     for i, b in enumerate(case.boundary_types()):
         c.bc[i] = BC_CODE[b.upper()]
     c.ntr = len(case.transports or [])
+    c.pt = 1 if getattr(case, "pt_relaxation", False) else 0
     return c
 
 

@@ -94,6 +94,13 @@ def golden_cases():
     c.transports = ["color"]
     c.states[1].transports = {"color": 1.0}
     g["euler1d_transport_o2"] = c
+    # analytic pressure-temperature relaxation after the pressure relaxation (RelaxationPT)
+    c = cases.shock_tube_1d(ncells=100, iterations=40, name="tubePT")
+    c.pt_relaxation = True
+    g["tube1d_pt_o1"] = c
+    c = cases.shock_bubble_2d(n=20, iterations=8, limiter="vanleer", name="bubblePT")
+    c.pt_relaxation = True
+    g["bubble2d_pt"] = c
     g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
     return g
 

@@ -16,7 +16,7 @@ KAPILA_KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1
                "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
                "expansion2d_ptmu", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2", "bubble2d_sym_o1",
                "cavity3d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc", "tube1d_transport_o2", "bubble2d_transport",
-               "tube1d_transport_o1"]
+               "tube1d_transport_o1", "tube1d_pt_o1", "bubble2d_pt"]
 EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2", "euler1d_transport_o2"]
 
 
@@ -127,6 +127,21 @@ def test_gpu_transports_match_oracle(dim, tmp_path):
     sim.step(steps)
     o = sim.fields()
     for name in ("alpha", "rho", "p", "u", "E", "tr"):
+        assert rel_l1(out[name], o[name]) <= TOL, name
+
+
+@pytest.mark.gpu
+def test_gpu_pt_relaxation_matches_oracle_2d(tmp_path):
+    """Analytic p-T relaxation after the pressure one, on a mesh of several tiles per axis."""
+    from ecogen_b200 import cases
+    case = cases.shock_bubble_2d(n=64, iterations=20, limiter="vanleer", name="bubblePT64")
+    case.pt_relaxation = True
+    case.boundaries = ["wall", "nonReflecting", "symmetry", "symmetry"]
+    out = gpu_run(case, tmp_path)
+    sim = oracle.Sim(case)
+    sim.step(20)
+    o = sim.fields()
+    for name in ("alpha", "rho", "p", "u", "E"):
         assert rel_l1(out[name], o[name]) <= TOL, name
 
 

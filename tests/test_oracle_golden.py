@@ -13,7 +13,8 @@ KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_
         "bubble2d_limiters", "bubble2d_vanalbada", "bubble2d_o1", "cavity3d_o2", "cavity3d_o1",
         "expansion2d_ptmu", "euler1d_o1", "euler1d_o2", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2",
         "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc",
-        "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2"]
+        "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2", "tube1d_pt_o1",
+        "bubble2d_pt"]
 
 
 @pytest.mark.parametrize("key", KEYS)
