@@ -247,6 +247,34 @@ def bench_batch(args, rank, world, local):
     dt_s = max_over_ranks(e0.elapsed_time(e1), "cuda") * 1e-3
     value = total * args.steps / dt_s
     api.lib().ecg_batch_destroy(h)
+
+    # the same batch with the learned seed installed (fresh copy of the initial state)
+    seeded = None
+    model_path = os.path.join(ROOT, "ecogen_b200", "models", f"seed_np{recs[0].nphases}.npz")
+    if not args.no_seeded and os.path.exists(model_path):
+        from ecogen_b200 import seed as seedmod
+        model = seedmod.SeedModel.load(model_path)
+        h2 = C.c_void_p()
+        api.check(api.lib().ecg_batch_create(arr, len(recs), C.byref(h2)), "ecg_batch_create")
+        api.check(api.lib().ecg_batch_upload_prim(h2, api._field_ptrs(cat), total), "upload")
+        api.check(api.lib().ecg_batch_set_shape(h2, tile, th), "set_shape")
+        model.install_batch(h2)
+        st2 = api.StepStats()
+        api.check(api.lib().ecg_batch_step(h2, args.warmup, None, None, C.byref(st2)), "warmup")
+        stream2 = torch.cuda.ExternalStream(api.lib().ecg_batch_stream(h2))
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream2)
+        api.check(api.lib().ecg_batch_step(h2, args.steps, None, None, C.byref(st2)), "step")
+        s1.record(stream2)
+        s1.synchronize()
+        ms2 = s0.elapsed_time(s1)
+        api.lib().ecg_batch_destroy(h2)
+        seeded = {"value": total * args.steps / (ms2 * 1e-3), "unit": "cell-updates/s",
+                  "speedup_vs_plain": dt_s * 1e3 / ms2,
+                  "newton_evals_per_relaxation": st2.newton_evals / max(1, st2.relax_calls),
+                  "plain_newton_evals_per_relaxation": st.newton_evals / max(1, st.relax_calls),
+                  "seeded": st2.seeded, "seed_rejected": st2.seed_rejected, "model": os.path.relpath(model_path, ROOT)}
     if rank == 0:
         peak, kind = measured_peak()
         B = 16 * (2 * 2 + 2 + 1)
@@ -260,6 +288,8 @@ def bench_batch(args, rank, world, local):
                              "frac": B * value / 1e9 / peak, "traffic": None, "peak_kind": kind},
                 "gpu_launches": args.steps * 3, "clocks": clk.summary(),
                 "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max}}
+        if seeded is not None:
+            line["mlp_seeded"] = seeded
         print(json.dumps(line))
 
 

@@ -134,9 +134,11 @@ __global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M0) {
         double pl = (gl + 0.5) * C.dx, pf = pl + 0.5 * C.dx, pr = (gl + 1 + 0.5) * C.dx;
         double y = pf - pl, z = pf - pr;
         constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
-        reconstruct_side<NP, 1, kThinc>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1., tl,
-                                        ug);
-        reconstruct_side<NP, 1, kThinc>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z), -1.,
+        constexpr int kLim = code_limiter(TYPES);
+        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1.,
+                                              tl, ug);
+        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z),
+                                              -1.,
                                 tr, vg);
       }
       double Fn[3];
@@ -270,7 +272,8 @@ static cudaError_t batch_tb(int pass, const BatchParams& B, const ecg_eos* eos, 
 // fast: two phases, SG liquid then ideal gas, no THINC -- the kernels with the EOS types compiled in
 static cudaError_t batch_launch(int np, int tb, int pass, const BatchParams& B, const ecg_eos* eos, double eps,
                                 int grid, cudaStream_t s, bool prepare, int* mb, bool fast) {
-  constexpr int kSgIg = eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG);
+  // the batched workload's configuration: SG liquid, IG gas, van Leer everywhere
+  constexpr int kSgIg = fast_code(eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG), ECG_LIM_VANLEER);
   if (np == 2 && fast) {
     if (tb == 64) return batch_tb<2, 64, kSgIg>(pass, B, eos, eps, grid, s, prepare, mb);
     if (tb == 128) return batch_tb<2, 128, kSgIg>(pass, B, eos, eps, grid, s, prepare, mb);
@@ -477,7 +480,8 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
   auto b = new ecg_batch();
   b->c0 = c0;
   b->fast = c0.nphases == 2 && c0.eos[0].type == ECG_EOS_SG && c0.eos[1].type == ECG_EOS_IG && !c0.pt_relaxation &&
-            !(c0.order == 2 && (c0.limiter[2] == ECG_LIM_THINC || c0.limiter[3] == ECG_LIM_THINC));
+            c0.order == 2 && c0.limiter[0] == ECG_LIM_VANLEER && c0.limiter[1] == ECG_LIM_VANLEER &&
+            c0.limiter[2] == ECG_LIM_VANLEER && c0.limiter[3] == ECG_LIM_VANLEER;
   b->ncases = ncases;
   b->np = c0.nphases;
   b->order = c0.order;

@@ -118,15 +118,18 @@ struct Model {
   double eps;  // epsilonAlphaNull: 1e-15 with alphaNull, else 0 (src/Eos/Eos.cpp:88-97)
 };
 
-// EOS types known at compile time: TYPES holds the type of phase k in bits 2k..2k+1
-// (ECG_EOS_IG 0, SG 1, NASG 2), or is EOS_DYNAMIC.  With known types every EOS branch folds away
-// (the arithmetic is unchanged), which shrinks the fused kernels' code; the generic kernels read
-// the types at run time.
+// Kernel configuration known at compile time ("fast" kernels): the type of phase k in bits
+// 2k..2k+1 (ECG_EOS_IG 0, SG 1, NASG 2) and, in bits 8 and up, one more than a limiter used for all
+// four limiter slots (0: limiters read at run time).  EOS_DYNAMIC marks the generic kernels.  With
+// known types and limiter every EOS and limiter branch folds away (the arithmetic is unchanged),
+// which shrinks the fused kernels' code.
 constexpr int EOS_DYNAMIC = -1;
 template <int NP>
 __host__ __device__ constexpr int eos_types_code(int t0, int t1, int t2 = 0) {
   return NP == 2 ? (t0 | (t1 << 2)) : (t0 | (t1 << 2) | (t2 << 4));
 }
+__host__ __device__ constexpr int fast_code(int types, int limiter) { return types | ((limiter + 1) << 8); }
+__host__ __device__ constexpr int code_limiter(int code) { return code == EOS_DYNAMIC ? -1 : (code >> 8) - 1; }
 template <int NP, int TYPES>
 __device__ __forceinline__ Model<NP> specialize_eos(const Model<NP>& M0) {
   Model<NP> M = M0;

@@ -20,7 +20,7 @@ struct CellCounters {
 // (CellInterfaceO2Cartesian.cpp:132-150 left side, :164-181 right side, whose final expressions
 // differ and are kept as they are) alpha_0 and alpha_1 = 1 - alpha_0 of an interface cell are then
 // replaced by the hyperbolic-tangent reconstruction.
-template <int NP, int DIM, bool THINC = true>
+template <int NP, int DIM, bool THINC = true, int LIMC = -1>
 __device__ ECG_RECON_INLINE void reconstruct_side(const Model<NP>& M, const StepParams& P, const double* sq, int RS,
                                                  int rc, const double* ssl, int SS, int f1, int f2, double alphaCell,
                                                  double alphaOther, double alphaAfter, double dist, double sign,
@@ -29,8 +29,9 @@ __device__ ECG_RECON_INLINE void reconstruct_side(const Model<NP>& M, const Step
   using FL = Fields<NP, DIM>;
   const bool iface = (alphaCell >= 1.e-4) && (alphaCell <= 1. - 1.e-4) &&
                      ((alphaOther - alphaCell) * (alphaCell - alphaAfter) >= 1.e-8);
-  const int lg = iface ? lim[1] : lim[0];
-  const int lv = iface ? lim[3] : lim[2];
+  // LIMC >= 0: one limiter compiled in for all four slots
+  const int lg = LIMC >= 0 ? LIMC : (iface ? lim[1] : lim[0]);
+  const int lv = LIMC >= 0 ? LIMC : (iface ? lim[3] : lim[2]);
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     double s1a = ssl[(k)*SS + f1], s1r = ssl[(NP + k) * SS + f1], s1p = ssl[(2 * NP + k) * SS + f1];

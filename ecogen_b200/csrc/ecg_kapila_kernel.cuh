@@ -202,8 +202,11 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH, TileShape
         double aLL = hasL ? a0[rl - 1] : (wL ? a0[rl] : 0.), aRR = hasR ? a0[rr + 1] : (wR ? a0[rr] : 0.);
         // THINC is compiled into the generic kernels only (the EOS-specialised ones run without it)
         constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
-        reconstruct_side<NP, DIM, kThinc>(M, P, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl, ug);
-        reconstruct_side<NP, DIM, kThinc>(M, P, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr, vg);
+        constexpr int kLim = code_limiter(TYPES);
+        reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[ax][gl], 1., tl,
+                                                ug);
+        reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[ax][gl], -1., tr,
+                                                vg);
         if (NTM > 0) {  // transports: volume-fraction limiter of each side, Transport::extrapolate
           const int lvL = iface_detect(aL, aR, aLL) ? P.lim[3] : P.lim[2];
           const int lvR = iface_detect(aR, aL, aRR) ? P.lim[3] : P.lim[2];

@@ -48,6 +48,12 @@ template <int NP>
 constexpr int eos_fast_types() {
   return NP == 2 ? eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG) : eos_types_code<3>(ECG_EOS_SG, ECG_EOS_IG, ECG_EOS_IG);
 }
+// ... and the limiter of the shipped workloads (van Leer in the two-phase cases, minmod in the
+// three-phase one), compiled into a further variant when all four limiter slots use it
+template <int NP>
+constexpr int eos_fast_limiter() {
+  return NP == 2 ? ECG_LIM_VANLEER : ECG_LIM_MINMOD;
+}
 template <int NP>
 inline bool eos_is_fast(const ecg_eos* eos) {
   int t[3] = {eos[0].type, eos[1].type, NP > 2 ? eos[2].type : 0};
@@ -68,26 +74,30 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
     if (P.mlp != nullptr) return cudaErrorNotSupported;
     return kapila_launch_tr(NP, DIM, PTMU, pass, P, G, eos, eps, s, prepare);
   }
+  // EOS types compiled in (limiters at run time), and EOS types plus the workload's limiter
+  constexpr int kEos = kFast ? fast_code(eos_fast_types<NP>(), -1) : EOS_DYNAMIC;
+  constexpr int kEosLim = kFast ? fast_code(eos_fast_types<NP>(), eos_fast_limiter<NP>()) : EOS_DYNAMIC;
   if (prepare) {
     cudaError_t e = launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, true);
-    if (e == cudaSuccess && kFast)
-      e = launch_pass_seed<NP, DIM, PTMU, false, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, false, kEos>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, false, kEosLim>(pass, P, G, eos, eps, s, true);
     if (e != cudaSuccess || PTMU) return e;
     e = launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, true);
-    if (e == cudaSuccess && kFast)
-      e = launch_pass_seed<NP, DIM, PTMU, true, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, true);
     return e;
   }
+  const bool fast_eos = kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos);
   if (P.mlp != nullptr) {
     if (PTMU) return cudaErrorNotSupported;
-    if (kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos))
-      return launch_pass_seed<NP, DIM, PTMU, true, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
-                                                                                                 false);
+    if (fast_eos) return launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, false);
     return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, false);
   }
-  if (kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos))
-    return launch_pass_seed<NP, DIM, PTMU, false, kFast ? eos_fast_types<NP>() : EOS_DYNAMIC>(pass, P, G, eos, eps, s,
-                                                                                                false);
+  if (fast_eos) {
+    const int L = eos_fast_limiter<NP>();
+    if (P.lim[0] == L && P.lim[1] == L && P.lim[2] == L && P.lim[3] == L)
+      return launch_pass_seed<NP, DIM, PTMU, false, kEosLim>(pass, P, G, eos, eps, s, false);
+    return launch_pass_seed<NP, DIM, PTMU, false, kEos>(pass, P, G, eos, eps, s, false);
+  }
   return launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, false);
 }
 
