@@ -52,6 +52,16 @@ def make_case(config: str, size: int | None):
     return cases.shock_bubble_2d(n=size or 2048, iterations=10 ** 6)
 
 
+def seed_model_path(config: str, nphases: int) -> str:
+    """The shipped seed model of a workload family (1D tubes have their own)."""
+    models = os.path.join(ROOT, "ecogen_b200", "models")
+    if config in ("c1", "c4"):
+        p = os.path.join(models, "seed_np2_tube1d.npz")
+        if os.path.exists(p):
+            return p
+    return os.path.join(models, f"seed_np{nphases}.npz")
+
+
 def state_fields(case) -> int:
     """Doubles per cell of the stored state: (alpha_k, rho_k)_k, p, u (d components), E."""
     per_phase = 1 if case.model.upper() == "EULER" else 2
@@ -250,7 +260,7 @@ def bench_batch(args, rank, world, local):
 
     # the same batch with the learned seed installed (fresh copy of the initial state)
     seeded = None
-    model_path = os.path.join(ROOT, "ecogen_b200", "models", f"seed_np{recs[0].nphases}.npz")
+    model_path = seed_model_path("c4", recs[0].nphases)
     if not args.no_seeded and os.path.exists(model_path):
         from ecogen_b200 import seed as seedmod
         model = seedmod.SeedModel.load(model_path)
@@ -376,7 +386,7 @@ def main():
 
     # ---- learned seed: same workload, relaxation Newton started from the installed MLP
     seeded = None
-    model_path = os.path.join(ROOT, "ecogen_b200", "models", f"seed_np{case.nphases}.npz")
+    model_path = seed_model_path(args.config, case.nphases)
     if not args.no_seeded and os.path.exists(model_path):
         from ecogen_b200 import seed as seedmod
         model = seedmod.SeedModel.load(model_path)

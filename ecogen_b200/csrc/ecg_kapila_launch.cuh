@@ -84,18 +84,20 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
     if (e != cudaSuccess || PTMU) return e;
     e = launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, true);
+    if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEosLim>(pass, P, G, eos, eps, s, true);
     return e;
   }
   const bool fast_eos = kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos);
-  if (P.mlp != nullptr) {
+  const int L = eos_fast_limiter<NP>();
+  const bool fast_lim = P.lim[0] == L && P.lim[1] == L && P.lim[2] == L && P.lim[3] == L;
+  if (P.mlp != nullptr) {  // the seeded kernels get the same compile-time configurations as the plain ones
     if (PTMU) return cudaErrorNotSupported;
+    if (fast_eos && fast_lim) return launch_pass_seed<NP, DIM, PTMU, true, kEosLim>(pass, P, G, eos, eps, s, false);
     if (fast_eos) return launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, false);
     return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, false);
   }
   if (fast_eos) {
-    const int L = eos_fast_limiter<NP>();
-    if (P.lim[0] == L && P.lim[1] == L && P.lim[2] == L && P.lim[3] == L)
-      return launch_pass_seed<NP, DIM, PTMU, false, kEosLim>(pass, P, G, eos, eps, s, false);
+    if (fast_lim) return launch_pass_seed<NP, DIM, PTMU, false, kEosLim>(pass, P, G, eos, eps, s, false);
     return launch_pass_seed<NP, DIM, PTMU, false, kEos>(pass, P, G, eos, eps, s, false);
   }
   return launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, false);

@@ -1,11 +1,14 @@
 """Trains the relaxation-seed MLPs shipped in ecogen_b200/models/ (on the GPU, with the library's kernels).
 
-    python -m ecogen_b200.train_seed [--phases 2|3] [--pairs 2000000] [--epochs 20]
+    python -m ecogen_b200.train_seed [--family cavity3d|bubble2d|tube1d] [--pairs 2000000] [--epochs 20]
 
-Three phases: pairs recorded by the plain solver on 3D cavity-collapse cases whose inclusion seeds
-(1000..) are disjoint from the benchmark case's seed (12345).  Two phases: pairs recorded on 2D
-shock-bubble cases with other shock positions and bubble radii than the benchmark case.  Writes
-models/seed_np<N>.npz and prints the training loss per epoch and the recording statistics.
+cavity3d (three phases, models/seed_np3.npz): pairs recorded by the plain solver on 3D
+cavity-collapse cases whose inclusion seeds (1000..) are disjoint from the benchmark case's seed
+(12345).  bubble2d (two phases, models/seed_np2.npz): 2D shock-bubble cases with other shock
+positions and bubble radii than the benchmark case.  tube1d (two phases,
+models/seed_np2_tube1d.npz): first-order 1D water/air shock tubes with other left pressures and
+interface positions than the benchmark tube (1e9 Pa at 0.7).  Prints the training loss per epoch
+and the recording statistics.
 """
 from __future__ import annotations
 
@@ -22,8 +25,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = os.path.join(HERE, "models")
 
 
-def training_cases(nphases: int, n: int):
-    if nphases == 3:
+FAMILIES = {"cavity3d": (3, "seed_np3.npz", 64), "bubble2d": (2, "seed_np2.npz", 512),
+            "tube1d": (2, "seed_np2_tube1d.npz", 1000)}
+
+
+def training_cases(family: str, n: int):
+    if family == "tube1d":
+        specs = [(3e8, 0.6), (6e8, 0.75), (2e9, 0.65), (1e8, 0.5), (8e8, 0.8), (5e9, 0.7)]
+        return [cases.shock_tube_1d(ncells=n, iterations=10 ** 6, p_left=pl, x_interface=xi, name=f"tube{s}")
+                for s, (pl, xi) in enumerate(specs)]
+    if family == "cavity3d":
         return [cases.cavity_collapse_3d(n=n, iterations=10 ** 6, seed=1000 + s, ninclusions=max(8, (n // 16) ** 3),
                                          radius_cells=(3.0, 10.0)) for s in range(6)]
     out = []
@@ -34,24 +45,29 @@ def training_cases(nphases: int, n: int):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--phases", type=int, default=3)
+    ap.add_argument("--family", default="cavity3d", choices=sorted(FAMILIES))
     ap.add_argument("--pairs", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warm", type=int, default=20)
     args = ap.parse_args()
-    n = args.size or (64 if args.phases == 3 else 512)
+    nphases, fname, default_n = FAMILIES[args.family]
+    n = args.size or default_n
     t0 = time.time()
-    x, y = seed.record(training_cases(args.phases, n), steps=args.steps, max_pairs=args.pairs, warm=args.warm)
+    steps, warm = args.steps, args.warm
+    if args.family == "tube1d":  # small cases: record along the whole run
+        steps, warm = max(steps, 400), 0
+    x, y = seed.record(training_cases(args.family, n), steps=steps, max_pairs=args.pairs, warm=warm)
     t1 = time.time()
     model, losses = seed.train(x, y, epochs=args.epochs, batch=8192, lr=2e-3, log=print)
     t2 = time.time()
     os.makedirs(MODELS, exist_ok=True)
-    path = os.path.join(MODELS, f"seed_np{args.phases}.npz")
+    path = os.path.join(MODELS, fname)
     model.save(path)
     info = {"pairs": int(len(y)), "record_s": t1 - t0, "train_s": t2 - t1, "loss_first": losses[0],
-            "loss_last": losses[-1], "epochs": args.epochs, "mesh": n, "steps_per_case": args.steps}
+            "loss_last": losses[-1], "epochs": args.epochs, "mesh": n, "steps_per_case": steps,
+            "family": args.family}
     with open(path.replace(".npz", ".json"), "w") as f:
         json.dump(info, f, indent=1)
     print(json.dumps(info))
