@@ -72,6 +72,8 @@ AIR_IG = Eos("IG_air.xml", "IG", gamma=1.4, cv=800.0)
 GAS_B_IG = Eos("IG_gasB.xml", "IG", gamma=1.67, cv=3116.0)
 LIQ_PC = Eos("SG_liquidPC.xml", "SG", gamma=2.35, pinf=1.0e9, cv=1816.0, eref=-1167.0e3, sref=0.0)
 VAP_PC = Eos("SG_vapourPC.xml", "SG", gamma=1.43, pinf=0.0, cv=1040.0, eref=2030.0e3, sref=-23.0e3)
+PTUEQ = "TemperaturePressureVelocityEq"
+WATER_SG300 = Eos("SG_water300K.xml", "SG", gamma=2.955, pinf=7.22e8, cv=1231.2)
 WATER_NASG = Eos("NASG_water.xml", "NASG", gamma=1.19, pinf=7.028e8, b=6.61e-4, cv=3610.0, eref=-1177788.0)
 
 
@@ -92,6 +94,7 @@ class State:
     pressure: float
     velocity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
     transports: Optional[Dict[str, float]] = None  # value of each passive transport in this state
+    temperature: Optional[float] = None  # mixture temperature (temperature-pressure equilibrium model)
 
 
 @dataclass
@@ -169,6 +172,11 @@ class Case:
         return b + ["nonReflecting"] * (6 - len(b))
 
     @property
+    def ptueq(self) -> bool:
+        """Temperature-pressure-velocity equilibrium model (ModPTUEq, src/Models/PTUEq)."""
+        return self.model.upper() == PTUEQ.upper()
+
+    @property
     def ncells(self) -> int:
         return int(self.cells[0]) * int(self.cells[1]) * int(self.cells[2])
 
@@ -225,6 +233,8 @@ class Case:
         ntr = f' numberTransports="{nt}"' if nt else ""
         if self.model.upper() == "EULER":
             s += f'  <flowModel name="Euler"{ntr}/>\n'
+        elif self.ptueq:  # Input::inputModel src/InputOutput/Input.cpp:642 (no alphaNull attribute)
+            s += f'  <flowModel name="{self.model}" numberPhases="{self.nphases}"{ntr}/>\n'
         else:
             an = "true" if self.alpha_null else "false"
             s += f'  <flowModel name="{self.model}" numberPhases="{self.nphases}"{ntr} alphaNull="{an}"/>\n'
@@ -260,6 +270,8 @@ class Case:
                     s += f'      <dataFluid density="{ph.density!r}" pressure="{st.pressure!r}">\n'
                     u = st.velocity
                     s += f'        <velocity x="{u[0]!r}" y="{u[1]!r}" z="{u[2]!r}"/>\n      </dataFluid>\n'
+                elif self.ptueq:  # PhasePTUEq::PhasePTUEq: alpha only
+                    s += f'      <dataFluid alpha="{ph.alpha!r}"/>\n'
                 else:
                     attr = f'alpha="{ph.alpha!r}"'
                     if ph.temperature is not None:
@@ -268,7 +280,11 @@ class Case:
                         attr += f' density="{ph.density!r}"'
                     s += f"      <dataFluid {attr}/>\n"
                 s += "    </material>\n"
-            if not euler:
+            if self.ptueq:  # MixPTUEq::MixPTUEq src/Models/PTUEq/MixPTUEq.cpp:44: pressure and temperature
+                u = st.velocity
+                s += (f'    <mixture>\n      <dataMix pressure="{st.pressure!r}" temperature="{st.temperature!r}"/>\n'
+                      f'      <velocity x="{u[0]!r}" y="{u[1]!r}" z="{u[2]!r}"/>\n    </mixture>\n')
+            elif not euler:
                 u = st.velocity
                 s += (f'    <mixture>\n      <dataMix pressure="{st.pressure!r}"/>\n'
                       f'      <velocity x="{u[0]!r}" y="{u[1]!r}" z="{u[2]!r}"/>\n    </mixture>\n')
@@ -450,3 +466,52 @@ def euler_shock_tube(ncells: int = 400, iterations: int = 50, order: Optional[st
                Domain("HP", "high", "halfSpace", {"axis": "x", "origin": 0.5, "direction": "negative"})]
     return Case(name, [AIR_IG], (1.0, 0.1, 0.1), (ncells, 1, 1), states, domains, model="Euler",
                 cfl=0.8, iterations=iterations, second_order=order)
+
+
+def ptueq_shock_tube_1d(ncells: int = 400, iterations: Optional[int] = 50, total_time: Optional[float] = None,
+                        order: Optional[str] = "vanleer", p_left: float = 1.0e8, x_interface: float = 0.7,
+                        alpha_floor: float = 1e-6, name: str = "ptueqShockTube1D",
+                        boundaries: Optional[List[str]] = None, transports: Optional[List[str]] = None) -> Case:
+    """1D water/air shock tube in temperature-pressure-velocity equilibrium (PTUEq model).
+
+    Air (IG) and water (SG) phases; left of ``x_interface`` water-rich at ``p_left`` and 341.5 K,
+    right of it air-rich at 1e5 Pa and 300 K, at rest (the layout of the reference's PTUEq
+    water/air shock tube, without its AMR).  With ``transports`` each side carries 0 / 1.
+    """
+    a = alpha_floor
+    tr_w = {t: 1.0 for t in transports or []}
+    tr_a = {t: 0.0 for t in transports or []}
+    states = [
+        State("water", [PhaseState(a), PhaseState(1.0 - a)], p_left, temperature=341.5, transports=tr_w or None),
+        State("air", [PhaseState(1.0 - a), PhaseState(a)], 1.0e5, temperature=300.0, transports=tr_a or None),
+    ]
+    domains = [Domain("left", "water", "entireDomain"),
+               Domain("right", "air", "halfSpace", {"axis": "x", "origin": x_interface, "direction": "positive"})]
+    return Case(name, [AIR_IG, WATER_SG300], (1.0, 0.1, 0.1), (ncells, 1, 1), states, domains, model=PTUEQ,
+                cfl=0.8, iterations=iterations, total_time=total_time if iterations is None else None,
+                second_order=order, boundaries=boundaries, transports=transports)
+
+
+def ptueq_bubble_2d(n: int = 64, iterations: int = 20, limiter: Optional[str] = "vanleer", alpha_floor: float = 1e-6,
+                    name: str = "ptueqBubble2D", ny: Optional[int] = None, nz: int = 1,
+                    boundaries: Optional[List[str]] = None) -> Case:
+    """2D air bubble in water hit by a planar pressure wave, PTUEq model, on a 1 cm square
+    (with ``nz`` > 1, a 1 cm cube crossed by an air cylinder along z).
+
+    Water at 1e5 Pa / 300 K with an air disc (radius 2 mm) at the centre; the water left of
+    x = 2 mm is at 1e8 Pa / 320 K and moves at +50 m/s.
+    """
+    a = alpha_floor
+    states = [
+        State("water", [PhaseState(a), PhaseState(1.0 - a)], 1.0e5, temperature=300.0),
+        State("hp", [PhaseState(a), PhaseState(1.0 - a)], 1.0e8, (50.0, 0.0, 0.0), temperature=320.0),
+        State("air", [PhaseState(1.0 - a), PhaseState(a)], 1.0e5, temperature=300.0),
+    ]
+    L = 0.01
+    domains = [Domain("base", "water", "entireDomain"),
+               Domain("bubble", "air", "disc", {"axis1": "x", "axis2": "y", "radius": 0.002,
+                                                "center": (0.5 * L, 0.5 * L, 0.0)}),
+               Domain("HP", "hp", "halfSpace", {"axis": "x", "origin": 0.002, "direction": "negative"})]
+    return Case(name, [AIR_IG, WATER_SG300], (L, L, L if nz > 1 else 1.0), (n, ny or n, nz), states, domains,
+                model=PTUEQ,
+                cfl=0.6, iterations=iterations, second_order=limiter, boundaries=boundaries)

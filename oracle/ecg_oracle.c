@@ -31,6 +31,7 @@ typedef struct {
 
 typedef struct {
   double rho, p, u[3], e, E, cF, cW; /* MixUEq (src/Models/UEq/MixUEq.h) */
+  double T;                          /* MixPTUEq temperature (src/Models/PTUEq/MixPTUEq.h) */
 } OMix;
 
 typedef struct {
@@ -48,8 +49,9 @@ typedef struct {
 typedef struct {
   double alpha[NP_MAX], rho[NP_MAX], p[NP_MAX];
   double u[3];
+  double pm, Tm;      /* MixPTUEq pressure and temperature slopes */
   double tr[NT_MAX];
-} OSlope; /* PhaseUEq/PhaseEuler slopes + MixUEq velocity slopes */
+} OSlope; /* PhaseUEq/PhaseEuler/PhasePTUEq slopes + MixUEq/MixPTUEq slopes */
 
 typedef struct {
   int L, R;           /* R < 0 for a boundary face */
@@ -261,9 +263,55 @@ static void euler_extended(const ecgo_sim* S, OPh* ph) { /* PhaseEuler::extended
   ph->T = eos_T(q, S->eps, ph->rho, ph->p);
 }
 
+/* ---- temperature-pressure-velocity equilibrium model (PTUEq, src/Models/PTUEq) ---- */
+
+static double eos_pinf(const ecgo_eos* q) { /* Eos::getPInf: 0 for IG (Errors::defaultDouble) */
+  return (q->type == ECGO_EOS_IG) ? 0. : q->pinf;
+}
+
+static double eos_rho_pT(const ecgo_eos* q, double eps, double p, double T) {
+  /* computeDensity(p, T): EosIG.cpp:85, EosSG.cpp:87 */
+  if (q->type == ECGO_EOS_IG) return p / omax(((q->gamma - 1.) * q->cv * T), eps);
+  return (p + q->pinf) / omax(((q->gamma - 1.) * q->cv * T), eps);
+}
+
+static void ptueq_mixture_vars(const ecgo_sim* S, OSt* st) {
+  /* MixPTUEq::computeMixtureVariables src/Models/PTUEq/MixPTUEq.cpp:293-313 (mass fractions without a floor) */
+  st->m.rho = 0.;
+  for (int k = 0; k < S->np; k++) st->m.rho += st->ph[k].alpha * st->ph[k].rho;
+  for (int k = 0; k < S->np; k++) st->ph[k].Y = st->ph[k].alpha * st->ph[k].rho / st->m.rho;
+  st->m.e = 0.;
+  st->m.cF = 0.;
+  for (int k = 0; k < S->np; k++) {
+    st->m.e += st->ph[k].Y * st->ph[k].e;
+    st->m.cF += st->ph[k].Y * st->ph[k].c * st->ph[k].c;
+  }
+  st->m.cF = sqrt(st->m.cF);
+}
+
+static void ptueq_phase(const ecgo_sim* S, int k, OPh* ph, double p, double T) {
+  /* ModPTUEq::fulfillState src/Models/PTUEq/ModPTUEq.cpp:99-108 for one phase:
+   * p_k = p, rho_k = computeDensity(p, T), then PhasePTUEq::extendedCalculusPhase (e_k, c_k) */
+  const ecgo_eos* q = &S->c.eos[k];
+  ph->p = p;
+  ph->rho = eos_rho_pT(q, S->eps, p, T);
+  ph->T = T;
+  ph->e = eos_e(q, S->eps, ph->rho, ph->p);
+  ph->c = eos_c(q, S->eps, ph->rho, ph->p);
+}
+
+static void ptueq_fulfill(const ecgo_sim* S, OSt* st) {
+  for (int k = 0; k < S->np; k++) ptueq_phase(S, k, &st->ph[k], st->m.p, st->m.T);
+  ptueq_mixture_vars(S, st);
+}
+
 static void fulfill(const ecgo_sim* S, OSt* st) { /* ModUEq::fulfillState :99 ; ModEuler::fulfillState :95 */
   if (S->c.model == ECGO_MODEL_EULER) {
     euler_extended(S, &st->ph[0]);
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) {
+    ptueq_fulfill(S, st);
     return;
   }
   for (int k = 0; k < S->np; k++) phase_extended(S, k, &st->ph[k]);
@@ -436,6 +484,69 @@ static void hllc_euler(const ecgo_sim* S, const OSt* Ls, const OSt* Rs, double d
   F->uStar = 0.;
 }
 
+static void hllc_ptueq(const ecgo_sim* S, const OSt* L, const OSt* R, double dxL, double dxR, double* dtMax,
+                       OFlux* F) {
+  /* ModPTUEq::solveRiemannIntern src/Models/PTUEq/ModPTUEq.cpp:113-227: mixture HLLC, phase masses
+   * carried by the mass fractions of the upwind side */
+  int np = S->np;
+  double uL = L->m.u[0], cL = L->m.cF, pL = L->m.p, rhoL = L->m.rho;
+  double uR = R->m.u[0], cR = R->m.cF, pR = R->m.p, rhoR = R->m.rho;
+  double sL = omin(uL - cL, uR - cR);
+  double sR = omax(uR + cR, uL + cL);
+  if (fabs(sL) > 1.e-3) *dtMax = omin(*dtMax, dxL / fabs(sL));
+  if (fabs(sR) > 1.e-3) *dtMax = omin(*dtMax, dxR / fabs(sR));
+  double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
+  double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+  if (fabs(sM) < 1.e-8) sM = 0.;
+  if (sL >= 0.) {
+    for (int k = 0; k < np; k++) F->mass[k] = L->ph[k].alpha * L->ph[k].rho * uL;
+    double vY = L->m.u[1], vZ = L->m.u[2];
+    double Et = L->m.e + 0.5 * sqnorm(L->m.u);
+    F->mom[0] = rhoL * uL * uL + pL;
+    F->mom[1] = rhoL * vY * uL;
+    F->mom[2] = rhoL * vZ * uL;
+    F->energMix = (rhoL * Et + pL) * uL;
+  } else if (sR <= 0.) {
+    for (int k = 0; k < np; k++) F->mass[k] = R->ph[k].alpha * R->ph[k].rho * uR;
+    double vY = R->m.u[1], vZ = R->m.u[2];
+    double Et = R->m.e + 0.5 * sqnorm(R->m.u);
+    F->mom[0] = rhoR * uR * uR + pR;
+    F->mom[1] = rhoR * vY * uR;
+    F->mom[2] = rhoR * vZ * uR;
+    F->energMix = (rhoR * Et + pR) * uR;
+  } else if (sM >= 0.) {
+    double vY = L->m.u[1], vZ = L->m.u[2];
+    double Et = L->m.e + 0.5 * sqnorm(L->m.u);
+    double rhoStar = mL / (sL - sM);
+    double EStar = Et + (sM - uL) * (sM + pL / mL);
+    double pStar = mL * (sM - uL) + pL;
+    for (int k = 0; k < np; k++) {
+      double mkL = L->ph[k].alpha * L->ph[k].rho * (sL - uL);
+      F->mass[k] = mkL / (sL - sM) * sM;
+    }
+    F->mom[0] = rhoStar * sM * sM + pStar;
+    F->mom[1] = rhoStar * vY * sM;
+    F->mom[2] = rhoStar * vZ * sM;
+    F->energMix = (rhoStar * EStar + pStar) * sM;
+  } else {
+    double vY = R->m.u[1], vZ = R->m.u[2];
+    double Et = R->m.e + 0.5 * sqnorm(R->m.u);
+    double rhoStar = mR / (sR - sM);
+    double EStar = Et + (sM - uR) * (sM + pR / mR);
+    double pStar = mR * (sM - uR) + pR;
+    for (int k = 0; k < np; k++) {
+      double mkR = R->ph[k].alpha * R->ph[k].rho * (sR - uR);
+      F->mass[k] = mkR / (sR - sM) * sM;
+    }
+    F->mom[0] = rhoStar * sM * sM + pStar;
+    F->mom[1] = rhoStar * vY * sM;
+    F->mom[2] = rhoStar * vZ * sM;
+    F->energMix = (rhoStar * EStar + pStar) * sM;
+  }
+  F->sM = sM;
+  F->uStar = 0.;
+}
+
 /* ------------------------------------------------------------------------------ flux accumulation */
 /* FluxUEq::addFlux/subtractFlux src/Models/UEq/FluxUEq.cpp:61,85 ;
  * FluxPUEq::addNonCons/subtractNonCons src/Models/PUEq/FluxPUEq.cpp:44,56 ;
@@ -447,6 +558,12 @@ static void acc_add(const ecgo_sim* S, OFlux* acc, const OFlux* F, double cA, co
   }
   if (S->c.model == ECGO_MODEL_EULER) {
     acc->mass[0] += cA * F->mass[0];
+    for (int d = 0; d < 3; d++) acc->mom[d] += cA * F->mom[d];
+    acc->energMix += cA * F->energMix;
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) { /* FluxPTUEq::addFlux src/Models/PTUEq/FluxPTUEq.cpp:55 */
+    for (int k = 0; k < S->np; k++) acc->mass[k] += cA * F->mass[k];
     for (int d = 0; d < 3; d++) acc->mom[d] += cA * F->mom[d];
     acc->energMix += cA * F->energMix;
     return;
@@ -476,6 +593,12 @@ static void acc_sub(const ecgo_sim* S, OFlux* acc, const OFlux* F, double cA, co
     acc->energMix -= cA * F->energMix;
     return;
   }
+  if (S->c.model == ECGO_MODEL_PTUEQ) { /* FluxPTUEq::subtractFlux :79 */
+    for (int k = 0; k < S->np; k++) acc->mass[k] -= cA * F->mass[k];
+    for (int d = 0; d < 3; d++) acc->mom[d] -= cA * F->mom[d];
+    acc->energMix -= cA * F->energMix;
+    return;
+  }
   for (int k = 0; k < S->np; k++) {
     acc->alpha[k] -= cA * F->alpha[k];
     acc->mass[k] -= cA * F->mass[k];
@@ -498,6 +621,12 @@ static void build_cons(const ecgo_sim* S, const OSt* st, OFlux* U) { /* FluxUEq:
     U->mass[0] = ph->rho;
     for (int d = 0; d < 3; d++) U->mom[d] = U->mass[0] * ph->u[d];
     U->energMix = U->mass[0] * ph->E;
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) { /* FluxPTUEq::buildCons src/Models/PTUEq/FluxPTUEq.cpp:109 */
+    for (int k = 0; k < S->np; k++) U->mass[k] = st->ph[k].alpha * st->ph[k].rho;
+    for (int d = 0; d < 3; d++) U->mom[d] = st->m.rho * st->m.u[d];
+    U->energMix = st->m.rho * st->m.E;
     return;
   }
   for (int k = 0; k < S->np; k++) {
@@ -547,6 +676,48 @@ static void build_prim(const ecgo_sim* S, OFlux* U, OSt* st) { /* FluxUEq::build
     ph->p = eos_p(q, eps, U->mass[0], ei);
     ph->c = eos_c(q, eps, U->mass[0], ph->p);
     ph->T = eos_T(q, eps, U->mass[0], ph->p);
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) {
+    /* FluxPTUEq::buildPrim src/Models/PTUEq/FluxPTUEq.cpp:125-160 with MixPTUEq::computePressure
+     * (:93-122, analytic p of two IG/SG phases, Le Martelot 2013) and computeTemperature (:126-145) */
+    double rhoMel = 0.;
+    for (int k = 0; k < 2; k++) rhoMel += U->mass[k];
+    st->m.u[0] = U->mom[0] / rhoMel;
+    st->m.u[1] = U->mom[1] / rhoMel;
+    st->m.u[2] = U->mom[2] / rhoMel;
+    for (int d = 0; d < 3; d++)
+      if (fabs(st->m.u[d]) < 1.e-8) st->m.u[d] = 0.;
+    double ie = U->energMix / rhoMel - 0.5 * (st->m.u[0] * st->m.u[0] + st->m.u[1] * st->m.u[1] + st->m.u[2] * st->m.u[2]);
+    const ecgo_eos* E1 = &S->c.eos[0];
+    const ecgo_eos* E2 = &S->c.eos[1];
+    double gamma1 = E1->gamma, pInf1 = eos_pinf(E1), cv1 = E1->cv, e01 = E1->eref, Y1 = U->mass[0] / rhoMel;
+    double gamma2 = E2->gamma, pInf2 = eos_pinf(E2), cv2 = E2->cv, e02 = E2->eref, Y2 = U->mass[1] / rhoMel;
+    double q = Y1 * e01 + Y2 * e02;
+    double cvMel = Y1 * cv1 + Y2 * cv2;
+    double A1 = Y1 * (gamma1 - 1.) * cv1 / cvMel * (rhoMel * (ie - q) - pInf1);
+    double A2 = Y2 * (gamma2 - 1.) * cv2 / cvMel * (rhoMel * (ie - q) - pInf2);
+    double pressure = 0.5 * (A1 + A2 - (pInf1 + pInf2)) +
+                      sqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
+    double temperature = 0.;
+    for (int k = 0; k < 2; k++) {
+      const ecgo_eos* E = &S->c.eos[k];
+      temperature += U->mass[k] / rhoMel * (E->gamma - 1.) * E->cv / (pressure + eos_pinf(E));
+    }
+    temperature = 1. / (temperature * rhoMel);
+    st->m.p = pressure;
+    st->m.T = temperature;
+    for (int k = 0; k < 2; k++) {
+      OPh* ph = &st->ph[k];
+      ph->p = pressure;
+      ph->rho = eos_rho_pT(&S->c.eos[k], eps, pressure, temperature);
+      ph->alpha = U->mass[k] / ph->rho;
+      ph->T = temperature;
+      ph->e = eos_e(&S->c.eos[k], eps, ph->rho, ph->p);
+      ph->c = eos_c(&S->c.eos[k], eps, ph->rho, ph->p);
+    }
+    ptueq_mixture_vars(S, st);
+    st->m.E = U->energMix / rhoMel;
     return;
   }
   int np = S->np;
@@ -811,7 +982,7 @@ static void relax_pt(ecgo_sim* S, OSt* st) {
 }
 
 static void relaxations(ecgo_sim* S, OSt* st) { /* Model::relaxations src/Models/Model.cpp:74 */
-  if (S->c.model == ECGO_MODEL_EULER) return;
+  if (S->c.model != ECGO_MODEL_KAPILA) return;
   relax_pinf(S, st);
   if (S->c.ptmu) relax_ptmu(S, st);
   if (S->c.pt) relax_pt(S, st);
@@ -983,6 +1154,7 @@ static void riemann(ecgo_sim* S, OSt* L, OSt* R, const OFace* F, double dxL, dou
   proj_local(vel_of(S, &l), F->n, F->t, F->b);
   proj_local(vel_of(S, &r), F->n, F->t, F->b);
   if (S->c.model == ECGO_MODEL_EULER) hllc_euler(S, &l, &r, dxL, dxR, dtMax, out);
+  else if (S->c.model == ECGO_MODEL_PTUEQ) hllc_ptueq(S, &l, &r, dxL, dxR, dtMax, out);
   else hllc_ueq(S, &l, &r, dxL, dxR, dtMax, out);
   for (int k = 0; k < S->c.ntr; k++) /* Transport::solveRiemann src/Transport/Transport.cpp: upwind by sM */
     out->tr[k] = (out->sM > 0.) ? l.tr[k] * out->sM : r.tr[k] * out->sM;
@@ -1002,6 +1174,13 @@ static void compute_slopes(ecgo_sim* S, OSt* st) {
       sl->rho[0] = (R->ph[0].rho - L->ph[0].rho) / dist;
       sl->p[0] = (R->ph[0].p - L->ph[0].p) / dist;
       for (int d = 0; d < 3; d++) sl->u[d] = (R->ph[0].u[d] - L->ph[0].u[d]) / dist;
+      continue;
+    }
+    if (S->c.model == ECGO_MODEL_PTUEQ) { /* PhasePTUEq::computeSlopesPhase :233, MixPTUEq::computeSlopesMixture :347 */
+      for (int k = 0; k < S->np; k++) sl->alpha[k] = (R->ph[k].alpha - L->ph[k].alpha) / dist;
+      sl->pm = (R->m.p - L->m.p) / dist;
+      sl->Tm = (R->m.T - L->m.T) / dist;
+      for (int d = 0; d < 3; d++) sl->u[d] = (R->m.u[d] - L->m.u[d]) / dist;
       continue;
     }
     for (int k = 0; k < S->np; k++) {
@@ -1058,6 +1237,13 @@ static void local_slopes(ecgo_sim* S, int cell, int face, double alphaCell, doub
   if (S->c.model == ECGO_MODEL_EULER) {
     out->rho[0] = ecgo_limiter(lim, s1.rho[0], s2.rho[0]);
     out->p[0] = ecgo_limiter(lim, s1.p[0], s2.p[0]);
+    for (int d = 0; d < 3; d++) out->u[d] = ecgo_limiter(lim, s1.u[d], s2.u[d]);
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) { /* PhasePTUEq::limitSlopes :256, MixPTUEq::limitSlopes :376 */
+    for (int k = 0; k < np; k++) out->alpha[k] = ecgo_limiter(limv, s1.alpha[k], s2.alpha[k]);
+    out->pm = ecgo_limiter(lim, s1.pm, s2.pm);
+    out->Tm = ecgo_limiter(lim, s1.Tm, s2.Tm);
     for (int d = 0; d < 3; d++) out->u[d] = ecgo_limiter(lim, s1.u[d], s2.u[d]);
     return;
   }
@@ -1149,6 +1335,20 @@ static void extrapolate(ecgo_sim* S, OSt* b, const OSlope* sl, double dist, doub
     if (ph->rho < 1.e-10) ph->rho = 1.e-10;
     eos_fix_p(&S->c.eos[0], &ph->p);
     eos_rho_max(&S->c.eos[0], &ph->rho);
+    return;
+  }
+  if (S->c.model == ECGO_MODEL_PTUEQ) {
+    /* PhasePTUEq::extrapolate + verifyAndCorrectPhase (:291: alpha in [1e-10, 1 - 1e-10]; its density and
+     * pressure corrections act on values fulfillState overwrites), MixPTUEq::extrapolate (:366) */
+    for (int k = 0; k < S->np; k++) {
+      OPh* ph = &b->ph[k];
+      ph->alpha += (sign * sl->alpha[k]) * dist;
+      if (ph->alpha < 1e-10) ph->alpha = 1e-10;
+      if (ph->alpha > 1. - 1e-10) ph->alpha = 1. - 1e-10;
+    }
+    b->m.p += (sign * sl->pm) * dist;
+    b->m.T += (sign * sl->Tm) * dist;
+    for (int d = 0; d < 3; d++) b->m.u[d] = b->m.u[d] + (sign * sl->u[d]) * dist;
     return;
   }
   for (int k = 0; k < S->np; k++) {
@@ -1247,7 +1447,7 @@ static void flux_pass(ecgo_sim* S, OSt* prim, int o2, double* dtMax) {
 }
 
 static void solve_relaxations(ecgo_sim* S) { /* Run::solveRelaxations src/Run.cpp:771 */
-  if (S->c.model == ECGO_MODEL_EULER) return;
+  if (S->c.model != ECGO_MODEL_KAPILA) return; /* Euler and PTUEq have no relaxation (advancingProcedure :596) */
   for (int i = 0; i < S->n; i++) relaxations(S, &S->s[i]);
   for (int i = 0; i < S->n; i++) {
     correction_energy(S, &S->s[i]);
@@ -1284,7 +1484,7 @@ static void step_o2(ecgo_sim* S, double dt, double* dtMax) {
     for (int k = 0; k < S->c.ntr; k++) /* CellO2::predictionOrdre2 :121-125 */
       S->s2[i].tr[k] = S->s[i].tr[k] + S->cons[i].tr[k] * (0.5 * dt);
     relaxations(S, &S->s2[i]);
-    if (S->c.model != ECGO_MODEL_EULER) correction_energy(S, &S->s2[i]);
+    if (S->c.model == ECGO_MODEL_KAPILA) correction_energy(S, &S->s2[i]);
     fulfill(S, &S->s2[i]);
   }
   memset(S->cons, 0, sizeof(OFlux) * (size_t)S->n);
@@ -1303,9 +1503,19 @@ static void step_o2(ecgo_sim* S, double dt, double* dtMax) {
 
 /* -------------------------------------------------------------------------------------------- API */
 
-ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u,
-                      const double* tr) {
+static ecgo_sim* create_impl(const ecgo_case* c, const double* alpha, const double* rho, const double* T,
+                             const double* p, const double* u, const double* tr) {
   if (c->ntr < 0 || c->ntr > NT_MAX || (c->ntr > 0 && !tr)) return NULL;
+  if ((c->model == ECGO_MODEL_PTUEQ) != (T != NULL)) return NULL;
+  if (c->model == ECGO_MODEL_PTUEQ && c->nphases != 2) return NULL;
+  /* ModPTUEq has no transport Riemann solver: the reference reports "solveRiemannTransportIntern not
+   * available for required model" (src/Models/Model.h:185) at every face */
+  if (c->model == ECGO_MODEL_PTUEQ && c->ntr > 0) return NULL;
+  /* MUSCL symmetry sides set phase velocity slopes (BoundCondWallO2Cartesian::computeSlopes :92-112), which
+   * PhasePTUEq does not have: the reference stops there (Phase::setU, src/Models/Phase.h:159) */
+  if (c->model == ECGO_MODEL_PTUEQ && c->order == 2)
+    for (int i = 0; i < 6; i++)
+      if (c->bc[i] == ECGO_BC_SYMMETRY) return NULL;
   ecgo_sim* S = (ecgo_sim*)calloc(1, sizeof(ecgo_sim));
   S->c = *c;
   S->np = (c->model == ECGO_MODEL_EULER) ? 1 : c->nphases;
@@ -1327,6 +1537,14 @@ ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho
       st->ph[0].alpha = 1.;
       for (int d = 0; d < 3; d++) st->ph[0].u[d] = u[d * n + i];
       euler_extended(S, &st->ph[0]);
+    } else if (c->model == ECGO_MODEL_PTUEQ) {
+      /* PhasePTUEq / MixPTUEq states (alpha_k; p, T, u), then Cell::completeFulfillState */
+      for (int k = 0; k < S->np; k++) st->ph[k].alpha = alpha[k * n + i];
+      st->m.p = p[i];
+      st->m.T = T[i];
+      for (int d = 0; d < 3; d++) st->m.u[d] = u[d * n + i];
+      fulfill(S, st);
+      st->m.E = st->m.e + 0.5 * sqnorm(st->m.u); /* MixPTUEq::computeTotalEnergy :316 */
     } else {
       for (int k = 0; k < S->np; k++) {
         st->ph[k].alpha = alpha[k * n + i];
@@ -1349,6 +1567,16 @@ ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho
     S->pcrit = pc;
   }
   return S;
+}
+
+ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u,
+                      const double* tr) {
+  return create_impl(c, alpha, rho, NULL, p, u, tr);
+}
+
+ecgo_sim* ecgo_create_ptueq(const ecgo_case* c, const double* alpha, const double* T, const double* p,
+                            const double* u, const double* tr) {
+  return create_impl(c, alpha, NULL, T, p, u, tr);
 }
 
 void ecgo_destroy(ecgo_sim* S) {

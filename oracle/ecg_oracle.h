@@ -8,6 +8,8 @@
  * reference itself is pinned by tests that run the reference binary built from
  * the reference sources (oracle/Makefile, oracle/refrun.py) on the same cases.
  *
+ * (The temperature-pressure-velocity equilibrium model, PTUEq, is restated too.)
+ *
  * Layout of state arrays passed across this interface (n = number of cells,
  * cell index i + j*nx + k*nx*ny, reference src/Meshes/MeshCartesian.cpp:141):
  *   alpha[k*n + c], rho[k*n + c] for k < nphases, p[c], u[d*n + c] (d < 3), E[c], tr[k*n + c] (k < ntr)
@@ -22,7 +24,7 @@ extern "C" {
 enum { ECGO_EOS_IG = 0, ECGO_EOS_SG = 1, ECGO_EOS_NASG = 2 };
 enum { ECGO_LIM_NONE = 0, ECGO_LIM_MINMOD = 1, ECGO_LIM_VANLEER = 2, ECGO_LIM_VANALBADA = 3,
        ECGO_LIM_SUPERBEE = 4, ECGO_LIM_MC = 5, ECGO_LIM_THINC = 6 };
-enum { ECGO_MODEL_KAPILA = 0, ECGO_MODEL_EULER = 1 };
+enum { ECGO_MODEL_KAPILA = 0, ECGO_MODEL_EULER = 1, ECGO_MODEL_PTUEQ = 2 };
 /* Boundary conditions per side Xm, Xp, Ym, Yp, Zm, Zp: non-reflecting, or symmetry (also an
  * inviscid "wall", src/InputOutput/Input.cpp:1146-1180). */
 enum { ECGO_BC_NONREFLECTING = 0, ECGO_BC_SYMMETRY = 1 };
@@ -63,6 +65,11 @@ typedef struct ecgo_sim ecgo_sim;
  * completed as in Cell::completeFulfillState (src/Order1/Cell.cpp:344). */
 ecgo_sim* ecgo_create(const ecgo_case* c, const double* alpha, const double* rho, const double* p, const double* u,
                       const double* tr);
+/* Temperature-pressure-velocity equilibrium model (ModPTUEq, two IG/SG phases): the initial state is
+ * alpha_k and the mixture p, T and velocity (src/Models/PTUEq/PhasePTUEq.cpp:42, MixPTUEq.cpp:44); phase
+ * densities follow from (p, T).  ecgo_get returns the mixture temperature as every phase's T. */
+ecgo_sim* ecgo_create_ptueq(const ecgo_case* c, const double* alpha, const double* T, const double* p,
+                            const double* u, const double* tr);
 void ecgo_destroy(ecgo_sim* s);
 /* Advance nsteps time steps.  *dt is the step to take first (1e-15 at start,
  * src/Run.cpp:38); on return it holds the next step cfl*dtMax (src/Run.cpp:439). */

@@ -61,6 +61,8 @@ def lib():
         dp = C.POINTER(C.c_double)
         L.ecgo_create.restype = C.c_void_p
         L.ecgo_create.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
+        L.ecgo_create_ptueq.restype = C.c_void_p
+        L.ecgo_create_ptueq.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
         L.ecgo_get_transports.argtypes = [C.c_void_p, dp]
         L.ecgo_destroy.argtypes = [C.c_void_p]
         L.ecgo_step.argtypes = [C.c_void_p, C.c_int, dp, dp, C.POINTER(Stats)]
@@ -85,7 +87,7 @@ def make_case(case) -> Case:
     """Convert an ``ecogen_b200.cases.Case`` into the oracle's case record."""
     c = Case()
     euler = case.model.upper() == "EULER"
-    c.model = 1 if euler else 0
+    c.model = 1 if euler else (2 if getattr(case, "ptueq", False) else 0)
     c.nphases = case.nphases
     c.alpha_null = 1 if case.alpha_null else 0
     c.order = 2 if case.second_order else 1
@@ -156,13 +158,15 @@ def _belongs(d, X, Y, Z) -> np.ndarray:
 
 
 def initial_fields(case) -> Dict[str, np.ndarray]:
-    """Initial (alpha_k, rho_k, p, u) of a case, filled domain by domain like the reference."""
+    """Initial (alpha_k, rho_k, p, u) of a case, filled domain by domain like the reference; the
+    temperature-pressure equilibrium model adds the mixture temperature "T" (phase densities from (p, T))."""
     X, Y, Z = cell_centres(case)
     n = X.size
     npf = case.nphases
     alpha = np.zeros((npf, n))
     rho = np.zeros((npf, n))
     p = np.zeros(n)
+    T = np.zeros(n)
     u = np.zeros((3, n))
     names = list(case.transports or [])
     tr = np.zeros((len(names), n))
@@ -172,18 +176,25 @@ def initial_fields(case) -> Dict[str, np.ndarray]:
         st = states[d.state]
         for k, ph in enumerate(st.phases):
             e = case.eos[k]
-            if ph.temperature is not None:
+            if getattr(case, "ptueq", False):
+                r = e.density_from_pT(st.pressure, st.temperature)
+            elif ph.temperature is not None:
                 r = e.density_from_pT(st.pressure, ph.temperature)
             else:
                 r = ph.density
             alpha[k, m] = ph.alpha
             rho[k, m] = r
         p[m] = st.pressure
+        if getattr(st, "temperature", None) is not None:
+            T[m] = st.temperature
         for dd in range(3):
             u[dd, m] = st.velocity[dd]
         for j, name in enumerate(names):  # a state without the transport leaves 0 (Input.cpp:1034-1050)
             tr[j, m] = (st.transports or {}).get(name, 0.0)
-    return {"alpha": alpha, "rho": rho, "p": p, "u": u, "tr": tr}
+    out = {"alpha": alpha, "rho": rho, "p": p, "u": u, "tr": tr}
+    if getattr(case, "ptueq", False):
+        out["T"] = T
+    return out
 
 
 class Sim:
@@ -202,7 +213,12 @@ class Sim:
         self.ntr = self.c.ntr
         tr = np.ascontiguousarray(f.get("tr", np.zeros((self.ntr, self.n))), dtype=np.float64)
         self._tr = tr
-        self.h = lib().ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u), _p(tr) if self.ntr else None)
+        if self.c.model == 2:
+            T = np.ascontiguousarray(f["T"], dtype=np.float64)
+            self._T = T
+            self.h = lib().ecgo_create_ptueq(C.byref(self.c), _p(a), _p(T), _p(p), _p(u), _p(tr) if self.ntr else None)
+        else:
+            self.h = lib().ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u), _p(tr) if self.ntr else None)
         if not self.h:
             raise ValueError("ecgo_create refused the case")
         self.dt = C.c_double(1e-15)

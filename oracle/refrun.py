@@ -116,13 +116,20 @@ def _transports(fields: Dict[str, np.ndarray]):
 
 
 def reference_prim(fields: Dict[str, np.ndarray], nphases: int):
-    """Map reference output names to (alpha[k], rho[k], p, u[3], E, tr) arrays (PUEq or Euler output)."""
+    """Map reference output names to (alpha[k], rho[k], p, u[3], E, tr) arrays (PUEq, PTUEq or Euler output)."""
     if "Pressure_Mixture" not in fields:  # Euler: PhaseEuler scalars + velocity (no total energy written)
         get = lambda pre: [v for n, v in fields.items() if n.startswith(pre)][0]
         rho = get("F0_Density")
         return {"alpha": np.ones((1, rho.size)), "rho": rho[None, :], "p": get("F0_Pressure"),
                 "u": get("F0_Velocity").T.copy(), "E": None, "rho_mix": rho, "T": get("F0_Temperature")[None, :],
                 "tr": _transports(fields)}
+    if "Temperature_Mixture" in fields:  # PTUEq: PhasePTUEq (Alpha, Density), MixPTUEq (rho, p, T, velocity)
+        alpha = np.stack([[v for n, v in fields.items() if n.startswith(f"F{k}_Alpha")][0] for k in range(nphases)])
+        rho = np.stack([[v for n, v in fields.items() if n.startswith(f"F{k}_Density")][0] for k in range(nphases)])
+        Tm = fields["Temperature_Mixture"]
+        return {"alpha": alpha, "rho": rho, "p": fields["Pressure_Mixture"],
+                "u": fields["Velocity_Mixture_norm"].T.copy(), "E": None, "rho_mix": fields["Density_Mixture"],
+                "T": np.stack([Tm] * nphases), "Tm": Tm, "tr": _transports(fields)}
     alpha, rho = [], []
     for k in range(nphases):
         a = [v for n, v in fields.items() if n.startswith(f"F{k}_Alpha")]

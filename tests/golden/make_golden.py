@@ -102,6 +102,19 @@ def golden_cases():
     c.pt_relaxation = True
     g["bubble2d_pt"] = c
     g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
+    # temperature-pressure-velocity equilibrium model (ModPTUEq)
+    g["ptueq_tube_o2"] = cases.ptueq_shock_tube_1d(ncells=200, iterations=60)
+    g["ptueq_tube_o1"] = cases.ptueq_shock_tube_1d(ncells=300, iterations=None, total_time=1.0e-4, order=None,
+                                                   name="ptueqTubeO1")
+    g["ptueq_tube_wall_o1"] = cases.ptueq_shock_tube_1d(ncells=120, iterations=150, order=None, x_interface=0.75,
+                                                        name="ptueqTubeWall", boundaries=["wall", "symmetry"])
+    g["ptueq_bubble2d_o2"] = cases.ptueq_bubble_2d(n=24, iterations=10)
+    g["ptueq_bubble2d_o1_sym"] = cases.ptueq_bubble_2d(n=20, ny=16, iterations=8, limiter=None, name="ptueqBubbleSym",
+                                                       boundaries=["symmetry", "nonReflecting", "wall", "symmetry"])
+    c = cases.ptueq_bubble_2d(n=20, iterations=8, limiter="minmod", name="ptueqBubbleTHINC")
+    c.interface_limiter, c.interface_vf_limiter = "superbee", "THINC"
+    g["ptueq_bubble2d_thinc"] = c
+    g["ptueq_bubble3d_o2"] = cases.ptueq_bubble_2d(n=10, nz=6, iterations=4, name="ptueqBubble3D")
     return g
 
 

@@ -14,7 +14,8 @@ KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_
         "expansion2d_ptmu", "euler1d_o1", "euler1d_o2", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2",
         "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc",
         "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2", "tube1d_pt_o1",
-        "bubble2d_pt"]
+        "bubble2d_pt", "ptueq_tube_o2", "ptueq_tube_o1", "ptueq_tube_wall_o1",
+        "ptueq_bubble2d_o2", "ptueq_bubble2d_o1_sym", "ptueq_bubble2d_thinc", "ptueq_bubble3d_o2"]
 
 
 @pytest.mark.parametrize("key", KEYS)
@@ -36,9 +37,12 @@ def test_oracle_matches_reference(key, golden_cases):
         if name in ("alpha", "rho") and got.ndim == 2 and ref.ndim == 2:
             pass
         assert np.array_equal(got, ref), f"{key}: field {name} differs from the reference"
+    if "final_Tm" in g:  # PTUEq mixture temperature (MixPTUEq "Temperature_Mixture")
+        assert np.array_equal(o["T"][0], g["final_Tm"]), f"{key}: temperature differs from the reference"
 
 
-@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "cavity3d_o2", "expansion2d_ptmu", "euler1d_o1"])
+@pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "cavity3d_o2", "expansion2d_ptmu", "euler1d_o1",
+                                 "ptueq_bubble2d_o2", "ptueq_bubble3d_o2"])
 def test_initial_fill_matches_reference(key, golden_cases):
     _, g = load_golden(key)
     case = golden_cases[key]
