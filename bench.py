@@ -87,9 +87,14 @@ def pass_bytes_per_cell(case) -> dict:
 
 
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch / cells, 2D two-phase MUSCL at 1536^2; profiles/k_kapila_step_shock_bubble_1536.md);
-# the kernels stream the state once, so traffic scales with the cell count.
-NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 195.72, ("kapila", 2, 2, True, "pass1"): 124.96}
+# of one launch / cells: 2D two-phase MUSCL at 1536^2, profiles/k_kapila_step_shock_bubble_1536.md; 3D
+# three-phase MUSCL at 128^3, profiles/k_kapila_step_cavity3d_128.md); the kernels stream the state once,
+# so traffic scales with the cell count.
+NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2, True, "pass1"): 125.14,
+                        ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89}
+# Batched tubes (2048 cases, profiles/k_batch_shock_tubes_2048.md): predictor + corrector DRAM bytes per
+# cell-update.
+NCU_BATCH_BYTES_PER_CELL_UPDATE = 94.98 + 153.87
 
 
 class ClockSampler:
@@ -295,7 +300,9 @@ def bench_batch(args, rank, world, local):
                 "config": {"workload": f"batched 1D shock tubes, Kapila 2-phase, MUSCL + van Leer, {len(recs)} cases",
                            "cells": total, "tile": tile.value, "parallelism": f"replicas{world}"},
                 "roofline": {"bound": "hbm", "achieved": B * value / 1e9, "peak": peak, "unit": "GB/s",
-                             "frac": B * value / 1e9 / peak, "traffic": None, "peak_kind": kind},
+                             "frac": B * value / 1e9 / peak, "traffic": None, "peak_kind": kind,
+                             "kernel": "k_batch (predictor + corrector of one step)",
+                             "ncu_bytes_per_cell_update": NCU_BATCH_BYTES_PER_CELL_UPDATE},
                 "gpu_launches": args.steps * 3, "clocks": clk.summary(),
                 "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max}}
         if seeded is not None:

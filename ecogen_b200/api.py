@@ -17,7 +17,7 @@ LIB_PATH = os.environ.get("ECG_LIB", os.path.join(HERE, "libecg.so"))
 ECG_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported case", 3: "CUDA error", 4: "case input error",
           5: "physics check failed", 6: "out of memory", 7: "size above the stated maximum", 8: "device wait timed out"}
-MODEL_KAPILA, MODEL_EULER = 0, 1
+MODEL_KAPILA, MODEL_EULER, MODEL_PTUEQ = 0, 1, 2
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
@@ -153,14 +153,18 @@ def _field_ptrs(arrs: Sequence[np.ndarray]):
 
 
 def nfields(case: Case) -> int:
-    return (6 if case.model == MODEL_EULER else 2 * case.nphases + 5) + case.ntransports
+    if case.model == MODEL_EULER:
+        return 6 + case.ntransports
+    if case.model == MODEL_PTUEQ:  # + the mixture temperature
+        return 2 * case.nphases + 6 + case.ntransports
+    return 2 * case.nphases + 5 + case.ntransports
 
 
 def case_from_spec(spec) -> Case:
     """ABI case record of an ``ecogen_b200.cases.Case`` description."""
     c = Case()
     euler = spec.model.upper() == "EULER"
-    c.model = MODEL_EULER if euler else MODEL_KAPILA
+    c.model = MODEL_EULER if euler else (MODEL_PTUEQ if getattr(spec, "ptueq", False) else MODEL_KAPILA)
     c.nphases = spec.nphases
     c.alpha_null = 1 if spec.alpha_null else 0
     c.order = 2 if spec.second_order else 1
@@ -245,8 +249,14 @@ class Context:
             return {"alpha": np.ones((1, self.n)), "rho": f[0][None, :], "p": f[1], "u": np.stack(f[2:5]),
                     "E": f[5], "tr": np.array(f[6:6 + nt]).reshape(nt, self.n)}
         k = self.case.nphases
-        return {"alpha": np.stack(f[:k]), "rho": np.stack(f[k:2 * k]), "p": f[2 * k], "u": np.stack(f[2 * k + 1:2 * k + 4]),
-                "E": f[2 * k + 4], "tr": np.array(f[2 * k + 5:2 * k + 5 + nt]).reshape(nt, self.n)}
+        out = {"alpha": np.stack(f[:k]), "rho": np.stack(f[k:2 * k]), "p": f[2 * k],
+               "u": np.stack(f[2 * k + 1:2 * k + 4]), "E": f[2 * k + 4]}
+        if self.case.model == MODEL_PTUEQ:
+            out["Tm"] = f[2 * k + 5]
+            out["tr"] = np.zeros((0, self.n))
+        else:
+            out["tr"] = np.array(f[2 * k + 5:2 * k + 5 + nt]).reshape(nt, self.n)
+        return out
 
     def derived(self):
         k = self.case.nphases

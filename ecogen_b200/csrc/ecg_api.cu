@@ -29,6 +29,8 @@ cudaError_t kapila_launch(int np, int dim, bool ptmu, int pass, const StepParams
                           const ecg_eos* eos, double eps, cudaStream_t s, bool prepare);
 cudaError_t euler_launch(int dim, int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
                          cudaStream_t s, bool prepare);
+cudaError_t ptueq_launch(int dim, int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, cudaStream_t s,
+                         bool prepare);
 
 __global__ void k_finalize(DevScalars* s) {
   // Run::solver src/Run.cpp:417-440: t += dt, iteration++, stop test, dt = cfl * dtMax
@@ -65,6 +67,27 @@ __global__ void k_derived(const double* __restrict__ S, int64_t n, int np, int d
     EosParams q{eos[k].type, eos[k].gamma, eos[k].pinf, eos[k].b, eos[k].cv, eos[k].eref, eos[k].sref};
     if (T) T[(int64_t)k * n + i] = eos_T(q, eps, r[k], pk[k]);
     if (Y) Y[(int64_t)k * n + i] = a[k] * r[k] / dmax(rho, eps);
+  }
+}
+
+// Temperature-pressure equilibrium model: phase densities computeDensity(p, T) (EosIG.cpp:85, EosSG.cpp:87),
+// every phase's temperature (the mixture's) and mass fractions, from the state alpha_0, alpha_1, p, T, ...
+__global__ void k_ptueq_derived(const double* __restrict__ S, int64_t n, ecg_eos e0, ecg_eos e1, double* rho,
+                                double* T, double* Y) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const ecg_eos eos[2] = {e0, e1};
+  const double p = S[2 * n + i], Tm = S[3 * n + i];
+  double r[2], mix = 0.;
+  for (int k = 0; k < 2; k++) {
+    const double den = dmax(((eos[k].gamma - 1.) * eos[k].cv * Tm), 0.);
+    r[k] = eos[k].type == ECG_EOS_IG ? p / den : (p + eos[k].pinf) / den;
+    mix += S[(int64_t)k * n + i] * r[k];
+  }
+  for (int k = 0; k < 2; k++) {
+    if (rho) rho[(int64_t)k * n + i] = r[k];
+    if (T) T[(int64_t)k * n + i] = Tm;
+    if (Y) Y[(int64_t)k * n + i] = S[(int64_t)k * n + i] * r[k] / mix;
   }
 }
 
@@ -120,7 +143,19 @@ ecg_status cuda_fail(cudaError_t e, const char* what) {
 
 ecg_status validate_case(const ecg_case* c) {
   if (!c) { set_error("null case"); return ECG_ERR_INVALID; }
-  if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER) { set_error("unknown model"); return ECG_ERR_INVALID; }
+  if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER && c->model != ECG_MODEL_PTUEQ) { set_error("unknown model"); return ECG_ERR_INVALID; }
+  if (c->model == ECG_MODEL_PTUEQ) {
+    // MixPTUEq::computePressure: two phases, IG or SG (src/Models/PTUEq/MixPTUEq.cpp:96-99)
+    if (c->nphases != 2) { set_error("the temperature-pressure equilibrium model has two phases"); return ECG_ERR_UNSUPPORTED; }
+    for (int k = 0; k < 2; k++)
+      if (c->eos[k].type == ECG_EOS_NASG) { set_error("Only IG and SG permitted in thermal equilibrium model"); return ECG_ERR_UNSUPPORTED; }
+    if (c->ntransports) { set_error("solveRiemannTransportIntern not available for the temperature-pressure equilibrium model"); return ECG_ERR_UNSUPPORTED; }
+    if (c->ptmu || c->pt_relaxation) { set_error("relaxations of the temperature-pressure equilibrium model"); return ECG_ERR_UNSUPPORTED; }
+    if (c->alpha_null) { set_error("alphaNull is not an option of the temperature-pressure equilibrium model"); return ECG_ERR_INVALID; }
+    if (c->order == 2)
+      for (int i = 0; i < 6; i++)  // BoundCondWallO2Cartesian::computeSlopes sets phase velocity slopes PhasePTUEq lacks
+        if (c->bc[i] == ECG_BC_SYMMETRY) { set_error("MUSCL symmetry sides of the temperature-pressure equilibrium model (setU not available)"); return ECG_ERR_UNSUPPORTED; }
+  }
   if (c->model == ECG_MODEL_KAPILA && (c->nphases < 2 || c->nphases > 3)) { set_error("Kapila needs 2 or 3 phases"); return ECG_ERR_UNSUPPORTED; }
   if (c->model == ECG_MODEL_EULER && c->nphases != 1) { set_error("Euler has one phase"); return ECG_ERR_INVALID; }
   if (c->order != 1 && c->order != 2) { set_error("order must be 1 or 2"); return ECG_ERR_INVALID; }
@@ -191,8 +226,10 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   double* sn = x->state[parity];
   double* s1 = x->state[1 - parity];
   const bool euler = x->c.model == ECG_MODEL_EULER;
+  const bool ptueq = x->c.model == ECG_MODEL_PTUEQ;
   auto run = [&](int pass) -> cudaError_t {
     if (euler) return euler_launch(x->dim, pass, P, x->geo, x->c.eos, x->eps, x->stream, false);
+    if (ptueq) return ptueq_launch(x->dim, pass, P, x->geo, x->c.eos, x->stream, false);
     return kapila_launch(x->np, x->dim, x->c.ptmu != 0, pass, P, x->geo, x->c.eos, x->eps, x->stream, false);
   };
   cudaError_t e;
@@ -399,7 +436,9 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   x->n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
   x->eps = c->alpha_null ? 1.e-15 : 0.;
   const bool euler = c->model == ECG_MODEL_EULER;
-  x->nstate = euler ? (3 + x->dim) : (2 * x->np + 2 + x->dim);  // Euler: rho, p, u, E
+  const bool ptueq = c->model == ECG_MODEL_PTUEQ;
+  // Euler: rho, p, u, E ; PTUEq: alpha_0, alpha_1, p, T, u, E ; Kapila: alpha_k, rho_k, p, u, E
+  x->nstate = euler ? (3 + x->dim) : (ptueq ? 5 + x->dim : 2 * x->np + 2 + x->dim);
   x->nq = x->nstate - 1;
   auto fail_free = [&](ecg_status s) {
     ecg_destroy(x);
@@ -420,7 +459,7 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
     e = cudaMalloc(&x->half, sizeof(double) * (size_t)(x->nstate + c->ntransports) * (size_t)x->n);
     if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(half)"));
   }
-  e = cudaMalloc(&x->tmp, sizeof(double) * (size_t)x->n);
+  e = cudaMalloc(&x->tmp, sizeof(double) * (size_t)(ptueq ? 2 : 1) * (size_t)x->n);  // download scratch
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(tmp)"));
   std::vector<double> h;
   distance_tables(*c, h);
@@ -473,8 +512,9 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   for (int pass = 0; pass < 3; pass++) {
     StepParams P{};
     P.ntr = c->ntransports;
-    cudaError_t pe = euler ? euler_launch(x->dim, pass, P, x->geo, c->eos, x->eps, x->stream, true)
-                           : kapila_launch(x->np, x->dim, c->ptmu != 0, pass, P, x->geo, c->eos, x->eps, x->stream, true);
+    cudaError_t pe = euler   ? euler_launch(x->dim, pass, P, x->geo, c->eos, x->eps, x->stream, true)
+                     : ptueq ? ptueq_launch(x->dim, pass, P, x->geo, c->eos, x->stream, true)
+                             : kapila_launch(x->np, x->dim, c->ptmu != 0, pass, P, x->geo, c->eos, x->eps, x->stream, true);
     if (pe == cudaErrorNotSupported) {
       set_error("no kernel built for this model / phases / dimension");
       ecg_destroy(x);
@@ -527,6 +567,23 @@ static ecg_status upload_impl(ecg_ctx* x, const double* const* f, int64_t ncells
   const size_t fb = sizeof(double) * (size_t)n;
   double* S = x->state[x->cur];
   const bool euler = x->c.model == ECG_MODEL_EULER;
+  if (x->c.model == ECG_MODEL_PTUEQ) {
+    // ABI: alpha_0 alpha_1 rho_0 rho_1 p u_x u_y u_z E T -> device: alpha_0 alpha_1 p T u_0..u_{dim-1} E
+    // (the phase densities are computeDensity(p, T); the uploaded ones are not read)
+    for (int i = 0; i < 2; i++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)i * n, f[i], fb, kind, x->stream));
+    ECG_CUDA(cudaMemcpyAsync(S + (size_t)2 * n, f[4], fb, kind, x->stream));
+    ECG_CUDA(cudaMemcpyAsync(S + (size_t)3 * n, f[9], fb, kind, x->stream));
+    for (int d = 0; d < x->dim; d++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)(4 + d) * n, f[5 + d], fb, kind, x->stream));
+    ECG_CUDA(cudaMemcpyAsync(S + (size_t)(4 + x->dim) * n, f[8], fb, kind, x->stream));
+    if (kind == cudaMemcpyHostToDevice)
+      for (int d = x->dim; d < 3; d++)
+        for (int64_t i = 0; i < n; i++)
+          if (f[5 + d][i] != 0.) {
+            set_error("non-zero velocity component along an axis with one cell is not supported");
+            return ECG_ERR_UNSUPPORTED;
+          }
+    return ECG_OK;
+  }
   // ABI: [alpha_k, rho_k] p u_x u_y u_z E  -> device: [alpha_k, rho_k] p u_0..u_{dim-1} E
   const int pre = euler ? 2 : 2 * x->np + 1;  // fields up to and including p
   for (int i = 0; i < pre; i++) ECG_CUDA(cudaMemcpyAsync(S + (size_t)i * n, f[i], fb, kind, x->stream));
@@ -568,6 +625,26 @@ static ecg_status download_impl(ecg_ctx* x, double* const* f, int64_t ncells, cu
   const size_t fb = sizeof(double) * (size_t)n;
   const double* S = x->state[x->cur];
   const bool euler = x->c.model == ECG_MODEL_EULER;
+  if (x->c.model == ECG_MODEL_PTUEQ) {
+    k_ptueq_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, x->c.eos[0], x->c.eos[1], x->tmp,
+                                                                       nullptr, nullptr);
+    ECG_CUDA(cudaGetLastError());
+    for (int i = 0; i < 2; i++) {
+      ECG_CUDA(cudaMemcpyAsync(f[i], S + (size_t)i * n, fb, kind, x->stream));
+      ECG_CUDA(cudaMemcpyAsync(f[2 + i], x->tmp + (size_t)i * n, fb, kind, x->stream));
+    }
+    ECG_CUDA(cudaMemcpyAsync(f[4], S + (size_t)2 * n, fb, kind, x->stream));
+    for (int d = 0; d < 3; d++) {
+      if (d < x->dim) ECG_CUDA(cudaMemcpyAsync(f[5 + d], S + (size_t)(4 + d) * n, fb, kind, x->stream));
+      else if (kind == cudaMemcpyDeviceToHost) {
+        ECG_CUDA(cudaStreamSynchronize(x->stream));
+        std::memset(f[5 + d], 0, fb);
+      } else ECG_CUDA(cudaMemsetAsync(f[5 + d], 0, fb, x->stream));
+    }
+    ECG_CUDA(cudaMemcpyAsync(f[8], S + (size_t)(4 + x->dim) * n, fb, kind, x->stream));
+    ECG_CUDA(cudaMemcpyAsync(f[9], S + (size_t)3 * n, fb, kind, x->stream));
+    return ECG_OK;
+  }
   if (euler) {
     for (int i = 0; i < 2; i++) ECG_CUDA(cudaMemcpyAsync(f[i], S + (size_t)i * n, fb, kind, x->stream));
   } else {
@@ -618,6 +695,9 @@ extern "C" ecg_status ecg_download_derived(ecg_ctx* x, double* T, double* Y, int
   if (x->c.model == ECG_MODEL_EULER) {
     k_euler_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, x->c.eos[0], x->eps, dT);
     cudaMemsetAsync(dY, 0, sizeof(double) * n, x->stream);
+  } else if (x->c.model == ECG_MODEL_PTUEQ) {
+    k_ptueq_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, x->c.eos[0], x->c.eos[1], nullptr, dT,
+                                                                       dY);
   } else {
     k_derived<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(S, n, np, x->dim, x->c.eos[0], x->c.eos[1],
                                                                  x->c.eos[2], x->eps, nullptr, dT, dY);

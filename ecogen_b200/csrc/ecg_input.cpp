@@ -29,6 +29,7 @@ struct StateIC {
   std::string name;
   double alpha[ECG_MAX_PHASES], rho[ECG_MAX_PHASES];
   double p = 0.;
+  double T = 0.;            // mixture temperature (temperature-pressure equilibrium model)
   double u[3] = {0., 0., 0.};
   double tr[2] = {0., 0.};  // passive transports (0 unless the state gives them)
 };
@@ -66,6 +67,20 @@ double eos_density_pT(const ecg_eos& q, double eps, double p, double T) {  // co
   if (q.type == ECG_EOS_IG) return p / std::max((q.gamma - 1.) * q.cv * T, eps);
   if (q.type == ECG_EOS_SG) return (p + q.pinf) / std::max((q.gamma - 1.) * q.cv * T, eps);
   return (p + q.pinf) / std::max((q.gamma - 1.) * q.cv * T + q.b * (p + q.pinf), eps);
+}
+
+// Total energy of a temperature-pressure equilibrium cell from the ABI fields alpha_k (0, 1), rho_k (2, 3),
+// p (4), u (5-7): ModPTUEq::fulfillState (e_k), MixPTUEq::computeMixtureVariables (e = sum Y_k e_k) and
+// computeTotalEnergy (E = e + |u|^2 / 2).
+double ptueq_total_energy(const ecg_case& c, double* const* f, int64_t i) {
+  double rho = 0., e = 0., ek[2];
+  for (int k = 0; k < 2; k++) {
+    ek[k] = ecg::host_eos_e(c.eos[k], 0., f[2 + k][i], f[4][i]);
+    rho += f[k][i] * f[2 + k][i];
+  }
+  for (int k = 0; k < 2; k++) e += f[k][i] * f[2 + k][i] / rho * ek[k];
+  const double u0 = f[5][i], u1 = f[6][i], u2 = f[7][i];
+  return e + 0.5 * (u0 * u0 + u1 * u1 + u2 * u2);
 }
 
 ecg_status read_eos(const std::string& dir, const std::string& name, ecg_eos* e) {
@@ -244,8 +259,14 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
     if (!fm->get_bool("alphaNull", &alpha_null)) return bail(ECG_ERR_XML, "model.xml: alphaNull missing");
     if (c.nphases < 2 || c.nphases > ECG_MAX_PHASES)
       return bail(ECG_ERR_UNSUPPORTED, "Kapila runs need 2 or 3 phases");
+  } else if (model == "TEMPERATUREPRESSUREVELOCITYEQ") {  // Input.cpp:642, ModPTUEq (no alphaNull attribute)
+    c.model = ECG_MODEL_PTUEQ;
+    if (!fm->get_int("numberPhases", &c.nphases)) return bail(ECG_ERR_XML, "model.xml: numberPhases missing");
+    if (c.nphases != 2)
+      return bail(ECG_ERR_UNSUPPORTED, "more than two phases not permitted in thermal equilibrium model");
   } else {
-    return bail(ECG_ERR_UNSUPPORTED, "flow model " + model + " is not supported (Euler, PressureVelocityEq)");
+    return bail(ECG_ERR_UNSUPPORTED, "flow model " + model +
+                                         " is not supported (Euler, PressureVelocityEq, TemperaturePressureVelocityEq)");
   }
   c.alpha_null = alpha_null ? 1 : 0;
   if (const Node* lm = modx->child("lowMach")) {
@@ -267,6 +288,14 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   if (modx->child("additionalPhysic")) return bail(ECG_ERR_UNSUPPORTED, "additional physics are not supported");
   if (modx->child("symmetryTerm")) return bail(ECG_ERR_UNSUPPORTED, "symmetry terms are not supported");
   if (modx->child("sourceTerms")) return bail(ECG_ERR_UNSUPPORTED, "source terms are not supported");
+  if (c.model == ECG_MODEL_PTUEQ) {
+    for (int k = 0; k < c.nphases; k++)  // MixPTUEq::computePressure (:97-99)
+      if (c.eos[k].type == ECG_EOS_NASG)
+        return bail(ECG_ERR_UNSUPPORTED, "Only IG and SG permitted in thermal equilibrium model");
+    if (ntr > 0)  // no transport Riemann solver (src/Models/Model.h:185)
+      return bail(ECG_ERR_UNSUPPORTED, "passive transports are not available for the thermal equilibrium model");
+    if (modx->child("relaxation")) return bail(ECG_ERR_UNSUPPORTED, "relaxations of the thermal equilibrium model");
+  }
   for (const Node* r : modx->all("relaxation")) {
     std::string t = upper(r->attr("type"));
     if (t == "PTMU") {
@@ -326,11 +355,14 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
       StateIC S;
       S.name = sn->attr("name");
       int k = 0;
-      if (c.model == ECG_MODEL_KAPILA) {
+      if (c.model == ECG_MODEL_KAPILA || c.model == ECG_MODEL_PTUEQ) {
         const Node* mix = sn->child("mixture");
         const Node* dmx = mix ? mix->child("dataMix") : nullptr;
         const Node* vel = mix ? mix->child("velocity") : nullptr;
         if (!mix || !dmx || !dmx->get_double("pressure", &S.p)) return bail(ECG_ERR_XML, "state " + st + ": mixture pressure missing");
+        // MixPTUEq::MixPTUEq src/Models/PTUEq/MixPTUEq.cpp:44-73: pressure and temperature
+        if (c.model == ECG_MODEL_PTUEQ && !dmx->get_double("temperature", &S.T))
+          return bail(ECG_ERR_XML, "state " + st + ": mixture temperature missing");
         if (!vel || !vel->get_double("x", &S.u[0]) || !vel->get_double("y", &S.u[1]) || !vel->get_double("z", &S.u[2]))
           return bail(ECG_ERR_XML, "state " + st + ": mixture velocity missing");
       }
@@ -343,7 +375,11 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
         if (!df) return bail(ECG_ERR_XML, "state " + st + ": <dataFluid> missing");
         double rho = 0., T = 0., p = 0.;
         bool hr = df->get_double("density", &rho), hT = df->get_double("temperature", &T);
-        if (c.model == ECG_MODEL_KAPILA) {
+        if (c.model == ECG_MODEL_PTUEQ) {
+          // PhasePTUEq::PhasePTUEq src/Models/PTUEq/PhasePTUEq.cpp:42-52: alpha only
+          if (!df->get_double("alpha", &S.alpha[k])) return bail(ECG_ERR_XML, "state " + st + ": alpha missing");
+          S.rho[k] = eos_density_pT(c.eos[k], 0., S.p, S.T);
+        } else if (c.model == ECG_MODEL_KAPILA) {
           // PhasePUEq::PhasePUEq src/Models/PUEq/PhasePUEq.cpp:41-73
           if (!df->get_double("alpha", &S.alpha[k])) return bail(ECG_ERR_XML, "state " + st + ": alpha missing");
           if (hr && hT) return bail(ECG_ERR_XML, "only one of following is required : density, temperature");
@@ -505,6 +541,11 @@ extern "C" ecg_status ecg_restart_fill(const ecg_case* cp, double* const* fields
   const double eps = c.alpha_null ? 1.e-15 : 0.;
   const int np = c.nphases;
   for (int64_t i = 0; i < n; i++) {
+    if (c.model == ECG_MODEL_PTUEQ) {  // ModPTUEq::fulfillState: rho_k from (p, T), then the total energy
+      for (int k = 0; k < 2; k++) fields[2 + k][i] = eos_density_pT(c.eos[k], 0., fields[4][i], fields[9][i]);
+      fields[8][i] = ptueq_total_energy(c, fields, i);
+      continue;
+    }
     if (c.model == ECG_MODEL_EULER) {
       const double u0 = fields[2][i], u1 = fields[3][i], u2 = fields[4][i];
       fields[5][i] = ecg::host_eos_e(c.eos[0], eps, fields[0][i], fields[1][i]) + 0.5 * (u0 * u0 + u1 * u1 + u2 * u2);
@@ -604,7 +645,16 @@ extern "C" ecg_status ecg_input_fill(const ecg_input* in, double* const* fields,
     if (!S) S = &in->states[in->domains[0].state];
     // Cell::completeFulfillState: fulfillState then E = e + |u|^2 / 2 (MixUEq::computeTotalEnergy)
     double E;
-    if (c.model == ECG_MODEL_KAPILA) {
+    if (c.model == ECG_MODEL_PTUEQ) {
+      for (int k = 0; k < 2; k++) {
+        fields[k][i] = S->alpha[k];
+        fields[2 + k][i] = S->rho[k];
+      }
+      fields[4][i] = S->p;
+      for (int dd = 0; dd < 3; dd++) fields[5 + dd][i] = S->u[dd];
+      fields[9][i] = S->T;
+      fields[8][i] = ptueq_total_energy(c, fields, i);
+    } else if (c.model == ECG_MODEL_KAPILA) {
       double rho = 0., e = 0.;
       double ek[ECG_MAX_PHASES];
       for (int k = 0; k < np; k++) {

@@ -11,7 +11,9 @@ void set_error(const std::string& msg);
 
 // Number of field pointers in the ABI layout of a case (see include/ecogen_b200.h).
 inline int abi_nfields(const ecg_case& c) {
-  return (c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5) + c.ntransports;
+  if (c.model == ECG_MODEL_EULER) return 6 + c.ntransports;
+  if (c.model == ECG_MODEL_PTUEQ) return 2 * c.nphases + 6 + c.ntransports;  // + the mixture temperature
+  return 2 * c.nphases + 5 + c.ntransports;
 }
 
 // EOS internal energy e(rho, p), same expression as the kernels and the reference EOS classes.

@@ -237,6 +237,13 @@ std::vector<double> grad_rho(const ecg_case& c, const std::vector<double>& rho) 
   return g;
 }
 
+// Number of field pointers of the ABI layout (include/ecogen_b200.h).
+int abi_fields(const ecg_case& c) {
+  if (c.model == ECG_MODEL_EULER) return 6 + c.ntransports;
+  if (c.model == ECG_MODEL_PTUEQ) return 2 * c.nphases + 6 + c.ntransports;
+  return 2 * c.nphases + 5 + c.ntransports;
+}
+
 struct Output {
   std::string dir;
   const ecg_input* in;
@@ -260,7 +267,7 @@ struct Output {
   bool write(ecg_ctx* ctx) {
     const int np = c.nphases;
     const bool euler = c.model == ECG_MODEL_EULER;
-    const int nf = (euler ? 6 : 2 * np + 5) + c.ntransports;
+    const int nf = abi_fields(c);
     std::vector<std::vector<double>> f(nf, std::vector<double>((size_t)n));
     std::vector<double*> ptr;
     for (auto& v : f) ptr.push_back(v.data());
@@ -295,6 +302,25 @@ struct Output {
       write_array(o, "F0_Velocity_" + e, u, 3, binary);
       write_transports(o, f, 6);
       write_array(o, "gradRho", grad_rho(c, f[0]), 1, binary);
+    } else if (c.model == ECG_MODEL_PTUEQ) {
+      // PhasePTUEq scalars Alpha, Density (src/Models/PTUEq/PhasePTUEq.cpp:118-150, no display clamp) and
+      // MixPTUEq scalars Density, Pressure, Temperature and vector Velocity (MixPTUEq.cpp:236-270)
+      for (int k = 0; k < np; k++) {
+        std::string e = strip_xml(ecg_input_eos_name(in, k));
+        write_array(o, "F" + std::to_string(k) + "_Alpha_" + e, f[k], 1, binary);
+        write_array(o, "F" + std::to_string(k) + "_Density_" + e, f[np + k], 1, binary);
+      }
+      std::vector<double> rho((size_t)n, 0.);
+      for (int k = 0; k < np; k++)
+        for (int64_t i = 0; i < n; i++) rho[i] += f[k][i] * f[np + k][i];
+      write_array(o, "Density_Mixture", rho, 1, binary);
+      write_array(o, "Pressure_Mixture", f[2 * np], 1, binary);
+      write_array(o, "Temperature_Mixture", f[2 * np + 5], 1, binary);
+      std::vector<double> u((size_t)3 * n);
+      for (int64_t i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) u[3 * i + d] = f[2 * np + 1 + d][i];
+      write_array(o, "Velocity_Mixture_norm", u, 3, binary);
+      write_array(o, "gradRho", grad_rho(c, rho), 1, binary);
     } else {
       for (int k = 0; k < np; k++) {  // PhasePUEq scalars (src/Models/PUEq/PhasePUEq.cpp:60-110)
         std::string e = strip_xml(ecg_input_eos_name(in, k));
@@ -351,7 +377,7 @@ int run_case(const std::string& work, const std::string& rel) {
   }
   int32_t binary = 1, precision = 0, restart = 0;
   ecg_input_output_control(in, &binary, &precision, &restart);
-  const int nf = (c.model == ECG_MODEL_EULER ? 6 : 2 * c.nphases + 5) + c.ntransports;
+  const int nf = abi_fields(c);
   std::vector<std::vector<double>> f(nf, std::vector<double>((size_t)n));
   std::vector<double*> ptr;
   for (auto& v : f) ptr.push_back(v.data());
@@ -391,7 +417,8 @@ int run_case(const std::string& work, const std::string& rel) {
       // phase scalars then vectors, mixture scalars then vectors (OutputXML::ReadPhysicalDataXML :194)
       const int np = c.nphases;
       const bool euler = c.model == ECG_MODEL_EULER;
-      const size_t base = euler ? 4 : (size_t)4 * np + 4;
+      const bool ptueq = c.model == ECG_MODEL_PTUEQ;
+      const size_t base = euler ? 4 : (ptueq ? (size_t)2 * np + 4 : (size_t)4 * np + 4);
       const size_t need = base + c.ntransports;  // then the transports T1, T2, ...
       bool ok = arrays.size() >= need;
       for (size_t a = 0; ok && a < need; a++) {
@@ -400,6 +427,15 @@ int run_case(const std::string& work, const std::string& rel) {
       }
       if (!ok) {
         fail_msg = "restart: result file does not hold this case's fields";
+      } else if (ptueq) {  // F<k> alpha, density; mixture density, pressure, temperature, velocity
+        for (int k = 0; k < np; k++) {
+          f[k] = arrays[2 * k];
+          f[np + k] = arrays[2 * k + 1];
+        }
+        f[2 * np] = arrays[2 * np + 1];
+        f[2 * np + 5] = arrays[2 * np + 2];
+        for (int64_t i = 0; i < n; i++)
+          for (int d = 0; d < 3; d++) f[2 * np + 1 + d][i] = arrays[2 * np + 3][3 * i + d];
       } else if (euler) {  // F0 density, pressure, temperature, velocity
         f[0] = arrays[0];
         f[1] = arrays[1];

@@ -1,7 +1,7 @@
 /*
  * ecogen_b200 — C ABI of the B200 (sm_100a) explicit finite-volume step of ECOGEN.
  *
- * The library replaces, for Cartesian non-AMR Euler / Kapila (PUEq) cases, the part of the
+ * The library replaces, for Cartesian non-AMR Euler / Kapila (PUEq) / PTUEq cases, the part of the
  * reference CPU run loop that advances the solution by one time step:
  *   Run::solveHyperbolic / Run::solveHyperbolicO2 + Run::solveRelaxations
  *   (src/Run.cpp:696, :627, :771) and the dt update of Run::solver (src/Run.cpp:406-440).
@@ -14,9 +14,13 @@
  * field, in the order
  *   alpha_0 .. alpha_{N-1}, rho_0 .. rho_{N-1}, p, u_x, u_y, u_z, E, T_0 .. T_{M-1}  (Kapila, N phases)
  *   rho, p, u_x, u_y, u_z, E, T_0 .. T_{M-1}                                       (Euler)
+ *   alpha_0, alpha_1, rho_0, rho_1, p, u_x, u_y, u_z, E, temperature               (PTUEq)
  * each pointing at n doubles, M = ecg_case.ntransports.  For Kapila, p is the mixture pressure
  * sum_k alpha_k p_k as the reference writes it ("Pressure_Mixture", src/Models/UEq/MixUEq.cpp:201);
- * E is the specific total energy ("Total_energy_Mixture"); T_j are the passive transports.
+ * E is the specific total energy ("Total_energy_Mixture"); T_j are the passive transports.  The
+ * temperature-pressure-velocity equilibrium model (PTUEq, src/Models/PTUEq) has one pressure and one
+ * temperature; its phase densities are computeDensity(p, temperature) of each EOS, so an upload reads
+ * alpha_k, p, u, E and the temperature and a download returns the densities it derives.
  */
 #ifndef ECOGEN_B200_H
 #define ECOGEN_B200_H
@@ -40,7 +44,9 @@ typedef enum {
   ECG_ERR_TIMEOUT = 8       /* a bounded device-side wait gave up */
 } ecg_status;
 
-enum { ECG_MODEL_KAPILA = 0, ECG_MODEL_EULER = 1 };
+/* Flow models: Kapila = PressureVelocityEq (ModPUEq), Euler (ModEuler), PTUEq =
+ * TemperaturePressureVelocityEq (ModPTUEq: two IG/SG phases, no transports, first-order symmetry sides). */
+enum { ECG_MODEL_KAPILA = 0, ECG_MODEL_EULER = 1, ECG_MODEL_PTUEQ = 2 };
 enum { ECG_EOS_IG = 0, ECG_EOS_SG = 1, ECG_EOS_NASG = 2 };
 enum {
   ECG_LIM_NONE = 0, ECG_LIM_MINMOD = 1, ECG_LIM_VANLEER = 2, ECG_LIM_VANALBADA = 3,
@@ -61,7 +67,7 @@ typedef struct {
 /* A case as the four ECOGEN XML files describe it (Input::readInputXML src/InputOutput/Input.cpp:54). */
 typedef struct {
   int32_t model;                /* ECG_MODEL_* */
-  int32_t nphases;              /* Kapila: 2..3 ; Euler: 1 */
+  int32_t nphases;              /* Kapila: 2..3 ; Euler: 1 ; PTUEq: 2 */
   int32_t alpha_null;           /* model.xml alphaNull */
   int32_t order;                /* 1 first order, 2 MUSCL-Hancock (secondOrder) */
   int32_t limiter[4];           /* global, interface, global vol.-fraction, interface vol.-fraction */
@@ -126,7 +132,8 @@ ecg_status ecg_input_fill(const ecg_input* in, double* const* fields, int64_t nc
  * Kapila: every phase takes the mixture pressure and is corrected (ModPUEq::fulfillStateRestart
  * src/Models/PUEq/ModPUEq.cpp:76, PhaseUEq::verifyAndCorrectPhase), then the total energy is rebuilt
  * (Cell::completeFulfillState src/Order1/Cell.cpp:344); Euler: the total energy only.  alpha_k and rho_k
- * are corrected in place and E is overwritten; p and u are kept.  Host-only, no GPU work. */
+ * are corrected in place and E is overwritten; p and u are kept.  PTUEq: the phase densities are recomputed
+ * from p and the temperature (ModPTUEq::fulfillState) and E is rebuilt.  Host-only, no GPU work. */
 ecg_status ecg_restart_fill(const ecg_case* c, double* const* fields, int64_t ncells);
 
 /* ------------------------------------------------------------------ one case on one GPU */
