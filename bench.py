@@ -46,6 +46,8 @@ def make_case(config: str, size: int | None):
         return cases.cavity_collapse_3d(n=size or 256, iterations=10 ** 6)
     if config == "c5":
         return cases.expansion_tube_2d(n=size or 1024, iterations=10 ** 6)
+    if config == "p2":
+        return cases.ptueq_bubble_2d(n=size or 2048, iterations=10 ** 6)
     if config == "c4":
         # one case of the batched workload (its per-case reference timing)
         return cases.shock_tube_1d(ncells=1000, iterations=10 ** 6, order="vanleer")
@@ -63,7 +65,10 @@ def seed_model_path(config: str, nphases: int) -> str:
 
 
 def state_fields(case) -> int:
-    """Doubles per cell of the stored state: (alpha_k, rho_k)_k, p, u (d components), E."""
+    """Doubles per cell of the stored state: (alpha_k, rho_k)_k, p, u (d components), E; for the
+    temperature-pressure equilibrium model alpha_k, p, T, u, E."""
+    if getattr(case, "ptueq", False):
+        return case.nphases + 3 + case.dim
     per_phase = 1 if case.model.upper() == "EULER" else 2
     return per_phase * case.nphases + 2 + case.dim
 
@@ -319,7 +324,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "p2"])
     ap.add_argument("--no-seeded", action="store_true", help="skip the learned-seed measurement")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -330,7 +335,9 @@ def main():
                 "c1": "1D water/air shock tube, Kapila, first order",
                 "c2": "2D shock-bubble, Kapila 2-phase, MUSCL + van Leer",
                 "c3": "3D three-phase cavity collapse, Kapila, MUSCL + minmod",
-                "c5": "2D liquid/vapour expansion, Kapila + p-T-mu relaxation, MUSCL + van Leer"}[args.config]
+                "c5": "2D liquid/vapour expansion, Kapila + p-T-mu relaxation, MUSCL + van Leer",
+                "p2": "2D air bubble in water, PTUEq (temperature-pressure-velocity equilibrium), MUSCL + van Leer"}[
+        args.config]
     config = {"workload": f"{workload}, {'x'.join(str(n) for n in case.cells if n > 1)} cells, FP64",
               "cells": case.ncells, "phases": case.nphases, "dim": case.dim, "order": 2 if case.second_order else 1,
               "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas{args.gpus}"}
@@ -394,7 +401,7 @@ def main():
     # ---- learned seed: same workload, relaxation Newton started from the installed MLP
     seeded = None
     model_path = seed_model_path(args.config, case.nphases)
-    if not args.no_seeded and os.path.exists(model_path):
+    if not args.no_seeded and os.path.exists(model_path) and not case.ptueq:  # PTUEq has no relaxation to seed
         from ecogen_b200 import seed as seedmod
         model = seedmod.SeedModel.load(model_path)
         ref_ctx = api.Context(inp.case)
@@ -467,7 +474,7 @@ def main():
         top = max(pb, key=lambda k: pass_ms[0 if k == "pass1" else 1])
         top_ms = pass_ms[0 if top == "pass1" else 1]
         achieved = pb[top] * case.ncells / (top_ms * 1e-3) / 1e9
-        tkey = ("euler" if case.model.upper() == "EULER" else "kapila", case.nphases, case.dim,
+        tkey = ("euler" if case.model.upper() == "EULER" else ("ptueq" if case.ptueq else "kapila"), case.nphases, case.dim,
                 bool(case.second_order), top)
         traffic = NCU_TRAFFIC_PER_CELL.get(tkey)
         kname = {"pass1": "MUSCL predictor" if case.second_order else "first-order step",

@@ -18,6 +18,18 @@
 #include "ecg_internal.h"
 #include "ecg_kapila_cell.cuh"
 
+// Register budget of the batched kernels: ECG_BATCH_SM_THREADS > 0 asks the compiler to fit
+// ECG_BATCH_SM_THREADS / TB blocks of TB threads on an SM (more resident warps, fewer registers a
+// thread); 0 leaves the register count to the compiler.
+#ifndef ECG_BATCH_SM_THREADS
+#define ECG_BATCH_SM_THREADS 0
+#endif
+#if ECG_BATCH_SM_THREADS > 0
+#define ECG_BATCH_BOUNDS(TB) __launch_bounds__(TB, (ECG_BATCH_SM_THREADS / (TB) > 0 ? ECG_BATCH_SM_THREADS / (TB) : 1))
+#else
+#define ECG_BATCH_BOUNDS(TB) __launch_bounds__(TB)
+#endif
+
 namespace ecg {
 
 struct BatchCase {
@@ -53,7 +65,7 @@ struct BatchTile {
 };
 
 template <int NP, int TB, int PASS, int TYPES>
-__global__ void __launch_bounds__(TB) k_batch(BatchParams B, Model<NP> M0) {
+__global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
   const Model<NP> M = specialize_eos<NP, TYPES>(M0);  // EOS types compiled in for the shipped workload
   using FL = Fields<NP, 1>;
   using K = BatchTile<NP, TB, PASS>;
