@@ -93,13 +93,15 @@ def pass_bytes_per_cell(case) -> dict:
 
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / cells: 2D two-phase MUSCL at 1536^2, profiles/k_kapila_step_shock_bubble_1536.md; 3D
-# three-phase MUSCL at 128^3, profiles/k_kapila_step_cavity3d_128.md); the kernels stream the state once,
+# three-phase MUSCL at 128^3, profiles/k_kapila_step_cavity3d_128.md; 2D PTUEq MUSCL at 1536^2,
+# profiles/k_ptueq_step_bubble_1536.md); the kernels stream the state once,
 # so traffic scales with the cell count.
 NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2, True, "pass1"): 125.14,
-                        ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89}
+                        ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89,
+                        ("ptueq", 2, 2, True, "pass2"): 150.78, ("ptueq", 2, 2, True, "pass1"): 91.56}
 # Batched tubes (2048 cases, profiles/k_batch_shock_tubes_2048.md): predictor + corrector DRAM bytes per
 # cell-update.
-NCU_BATCH_BYTES_PER_CELL_UPDATE = 94.98 + 153.87
+NCU_BATCH_BYTES_PER_CELL_UPDATE = 99.20 + 158.35
 
 
 class ClockSampler:
@@ -495,7 +497,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": traffic * case.ncells if traffic is not None else None,
-                         "peak_kind": peak_kind, "kernel": f"{'k_euler_step' if tkey[0] == 'euler' else 'k_kapila_step'} ({kname})",
+                         "peak_kind": peak_kind, "kernel": f"{ {'euler': 'k_euler_step', 'ptueq': 'k_ptueq_step'}.get(tkey[0], 'k_kapila_step')} ({kname})",
                          "algorithmic_bytes_per_cell": pb[top], "launch_ms": top_ms,
                          "step_bytes_per_cell_update": B,
                          "step_frac": B * case.ncells / (step_ms * 1e-3) / 1e9 / peak},

@@ -20,9 +20,12 @@
 
 // Register budget of the batched kernels: ECG_BATCH_SM_THREADS > 0 asks the compiler to fit
 // ECG_BATCH_SM_THREADS / TB blocks of TB threads on an SM (more resident warps, fewer registers a
-// thread); 0 leaves the register count to the compiler.
+// thread); 0 leaves the register count to the compiler.  Measured on 4096 batched two-phase tubes
+// (cell-updates/s, tile chosen by the autotuner): no budget (168 registers, 12 warps per SM) 1168 M;
+// 512 threads 1448 M; 640: 1464 M; 896 (85 registers at 256-cell tiles, 24 warps) 1628-1658 M;
+// 1024: 1599 M; 1152: 1602 M.
 #ifndef ECG_BATCH_SM_THREADS
-#define ECG_BATCH_SM_THREADS 0
+#define ECG_BATCH_SM_THREADS 896
 #endif
 #if ECG_BATCH_SM_THREADS > 0
 #define ECG_BATCH_BOUNDS(TB) __launch_bounds__(TB, (ECG_BATCH_SM_THREADS / (TB) > 0 ? ECG_BATCH_SM_THREADS / (TB) : 1))

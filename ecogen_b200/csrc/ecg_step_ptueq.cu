@@ -146,9 +146,18 @@ __device__ __forceinline__ void hllc_pt(const PtSide& L, const double ul[3], con
   }
 }
 
+// Register budget: the resident-block target of the tile shape (TileShape::MINB), as the Kapila
+// kernels; ECG_PTUEQ_NO_MINB leaves the register count to the compiler.  Measured on the 2D bubble at
+// 2048^2 (MUSCL + van Leer): compiler's choice (94 registers, 20 warps per SM) 1170 M cell-updates/s,
+// 7 blocks of 128 threads (72 registers, 28 warps) 1536 M.
+#ifndef ECG_PTUEQ_NO_MINB
+#define ECG_PTUEQ_BOUNDS(DIM, PASS) __launch_bounds__(PtStep<DIM, PASS>::NTH, TileShape<DIM>::MINB)
+#else
+#define ECG_PTUEQ_BOUNDS(DIM, PASS) __launch_bounds__(PtStep<DIM, PASS>::NTH)
+#endif
+
 template <int DIM, int PASS>
-__global__ void __launch_bounds__(PtStep<DIM, PASS>::NTH)
-    k_ptueq_step(StepParams P, Geometry G, PtEos M) {
+__global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry G, PtEos M) {
   using K = PtStep<DIM, PASS>;
   using TS = TileShape<DIM>;
   if (*P.done) return;

@@ -166,38 +166,48 @@ def restart_case(restart_file=None):
     return c
 
 
-def make_restart_golden():
-    """restart2d.npz/.json: the reference's result file 2 and infoCalcul.out of a 30-iteration run, and the
+def restart_case_ptueq(restart_file=None):
+    """2D PTUEq bubble printed every 10 iterations as ASCII with 17 digits."""
+    c = cases.ptueq_bubble_2d(n=20, ny=16, iterations=30, name="restartPTUEq")
+    c.output_binary, c.output_precision, c.print_freq, c.restart_file = False, 17, 10, restart_file
+    return c
+
+
+def make_restart_golden(key="restart2d", make_case=None):
+    """<key>.npz/.json: the reference's result file 2 and infoCalcul.out of a 30-iteration run, and the
     final file of the reference restarted from file 2 (Run::restartSimulation src/Run.cpp:345)."""
-    work = os.path.join(ROOT, "_work", "runs", "golden", "restart2d")
+    make_case = make_case or restart_case
+    work = os.path.join(ROOT, "_work", "runs", "golden", key)
     shutil.rmtree(work, ignore_errors=True)
-    c = restart_case()
+    c = make_case()
     d = c.write(work)
     cases.write_ecogen_list(work, [d])
     r = refrun.run(work)
     if r.returncode != 0:
-        raise SystemExit("restart2d: reference failed\n" + r.stdout[-3000:])
+        raise SystemExit(key + ": reference failed\n" + r.stdout[-3000:])
     with open(os.path.join(work, "results", c.name, "infoCalcul.out")) as f:
         info_lines = [ln.rstrip("\n") for ln in f if ln.strip()]
     src = refrun.read_vtr_ordered(refrun.result_file(work, c.name, 2, binary=False))
-    c2 = restart_case(2)
+    c2 = make_case(2)
     d = c2.write(work)  # same case folder, now restarting from file 2
     r = refrun.run(work)
     if r.returncode != 0:
-        raise SystemExit("restart2d: reference restart failed\n" + r.stdout[-3000:])
+        raise SystemExit(key + ": reference restart failed\n" + r.stdout[-3000:])
     fin = refrun.read_vtr(refrun.result_file(work, c.name, 3, binary=False))
     arrays = {f"in{i:02d}": np.asarray(a) for i, (_, a) in enumerate(src)}
     arrays.update({"final_" + k: np.asarray(v) for k, v in
                    refrun.reference_prim(fin, c.nphases).items() if v is not None})
-    np.savez_compressed(os.path.join(OUT, "restart2d.npz"), **arrays)
-    with open(os.path.join(OUT, "restart2d.json"), "w") as fh:
+    np.savez_compressed(os.path.join(OUT, key + ".npz"), **arrays)
+    with open(os.path.join(OUT, key + ".json"), "w") as fh:
         json.dump({"info_lines": info_lines[:4], "names": [n for n, _ in src], "restart_file": 2,
                    "case": case_meta(c)}, fh, indent=1)
-    print("restart2d", info_lines[:4])
+    print(key, info_lines[:4])
 
 
 if __name__ == "__main__":
     if sys.argv[1:] == ["restart2d"]:
         make_restart_golden()
+    elif sys.argv[1:] == ["restart_ptueq"]:
+        make_restart_golden("restart_ptueq", restart_case_ptueq)
     else:
         main()

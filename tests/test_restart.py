@@ -20,16 +20,16 @@ import pytest
 from ecogen_b200 import api, cases
 from oracle import oracle, refrun
 from tests.conftest import display, rel_l1
-from tests.golden.make_golden import restart_case
+from tests.golden.make_golden import restart_case, restart_case_ptueq
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 
 
-def _fixture():
-    with open(os.path.join(HERE, "golden", "restart2d.json")) as f:
+def _fixture(key="restart2d"):
+    with open(os.path.join(HERE, "golden", key + ".json")) as f:
         meta = json.load(f)
-    g = dict(np.load(os.path.join(HERE, "golden", "restart2d.npz")))
+    g = dict(np.load(os.path.join(HERE, "golden", key + ".npz")))
     arrays = [g[f"in{i:02d}"] for i in range(len(meta["names"]))]
     return meta, g, arrays
 
@@ -43,6 +43,17 @@ def _abi_fields(case, arrays):
     vel = arrays[4 * k + 3].reshape(-1, 3)
     f += [vel[:, d] for d in range(3)]
     f.append(arrays[4 * k + 2])
+    return [np.ascontiguousarray(x, dtype=np.float64) for x in f]
+
+
+def _abi_fields_ptueq(case, arrays):
+    """PTUEq ABI layout (alpha_k, rho_k, p, u_x, u_y, u_z, E, T) from a PTUEq result file in file order:
+    per phase alpha, density; mixture density, pressure, temperature, velocity.  E is left to
+    ecg_restart_fill."""
+    f = [arrays[0], arrays[2], arrays[1], arrays[3], arrays[5]]
+    vel = arrays[7].reshape(-1, 3)
+    f += [vel[:, d] for d in range(3)]
+    f += [np.zeros(case.ncells), arrays[6]]
     return [np.ascontiguousarray(x, dtype=np.float64) for x in f]
 
 
@@ -116,3 +127,46 @@ def test_driver_restart_matches_reference_restart(tmp_path):
         lines = [ln.split() for ln in fh if ln.strip()]
     assert [ln[0] for ln in lines] == ["1", "0", "1", "2", "3"]
     assert lines[-1][1] == "30"
+
+
+def test_ptueq_restart_fill_and_oracle_match_reference_restart():
+    """PTUEq restart (fixture restart_ptueq): densities from (p, T) and the total energy rebuilt by
+    ecg_restart_fill, then the oracle continues bit for bit on the reference's restarted run."""
+    meta, g, arrays = _fixture("restart_ptueq")
+    assert meta["names"][:2] == ["F0_Alpha_IG_air", "F0_Density_IG_air"]
+    case = restart_case_ptueq()
+    f = _abi_fields_ptueq(case, arrays)
+    api.check(api.lib().ecg_restart_fill(C.byref(api.case_from_spec(case)), api._field_ptrs(f), case.ncells),
+              "ecg_restart_fill")
+    assert np.array_equal(f[2], arrays[1]) and np.array_equal(f[3], arrays[3])  # computeDensity(p, T)
+    sim = oracle.Sim(case, {"alpha": np.stack(f[:2]), "rho": np.stack(f[2:4]), "p": f[4], "T": f[9],
+                            "u": np.stack(f[5:8])})
+    assert np.array_equal(sim.fields()["E"], f[8])
+    it, t, dt = _info(meta)
+    assert it == 20
+    sim.t.value, sim.dt.value = t, dt
+    sim.step(10)
+    o = sim.fields()
+    for name in ("alpha", "rho", "p", "u"):
+        assert np.array_equal(o[name], g["final_" + name]), name
+    assert np.array_equal(o["T"][0], g["final_Tm"])
+
+
+@pytest.mark.gpu
+def test_driver_ptueq_restart_matches_reference_restart(tmp_path):
+    meta, g, arrays = _fixture("restart_ptueq")
+    case = restart_case_ptueq(meta["restart_file"])
+    work = str(tmp_path)
+    d = case.write(work)
+    cases.write_ecogen_list(work, [d])
+    res = os.path.join(work, "results", case.name)
+    os.makedirs(os.path.join(res, "datasets"))
+    with open(os.path.join(res, "infoCalcul.out"), "w") as fh:
+        fh.write("\n".join(meta["info_lines"]) + "\n")
+    _write_reference_layout(refrun.result_file(work, case.name, 2, binary=False), meta["names"], arrays, case)
+    exe = os.path.join(ROOT, "ecogen_b200", "ecogen-b200")
+    r = subprocess.run([exe, work + "/"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    got = refrun.reference_prim(refrun.read_vtr(refrun.result_file(work, case.name, 3, binary=False)), case.nphases)
+    for name in ("alpha", "rho", "p", "u", "Tm"):
+        assert rel_l1(got[name], g["final_" + name]) <= 1e-12, name
