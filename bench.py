@@ -101,7 +101,7 @@ NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2
                         ("ptueq", 2, 2, True, "pass2"): 150.78, ("ptueq", 2, 2, True, "pass1"): 91.56}
 # Batched tubes (2048 cases, profiles/k_batch_shock_tubes_2048.md): predictor + corrector DRAM bytes per
 # cell-update.
-NCU_BATCH_BYTES_PER_CELL_UPDATE = 99.20 + 158.35
+NCU_BATCH_BYTES_PER_CELL_UPDATE = 98.05 + 157.17
 
 
 class ClockSampler:
@@ -305,7 +305,8 @@ def bench_batch(args, rank, world, local):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": f"batched 1D shock tubes, Kapila 2-phase, MUSCL + van Leer, {len(recs)} cases",
-                           "cells": total, "tile": tile.value, "parallelism": f"replicas{world}"},
+                           "cells": total, "tile": tile.value, "cells_per_item": tile.value - 1,
+                           "parallelism": f"replicas{world}"},
                 "roofline": {"bound": "hbm", "achieved": B * value / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": B * value / 1e9 / peak, "traffic": None, "peak_kind": kind,
                              "kernel": "k_batch (predictor + corrector of one step)",

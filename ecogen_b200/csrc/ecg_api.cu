@@ -115,6 +115,10 @@ struct ecg_ctx {
   double* tmp = nullptr;      // download scratch (mixture pressure)
   DevScalars* scal = nullptr;
   DevStats* stats = nullptr;
+  // pinned host staging of the scalars and counters an ecg_step call exchanges (asynchronous copies,
+  // one synchronisation per call)
+  DevScalars* h_scal = nullptr;
+  DevStats* h_stats = nullptr;
   int cur = 0;
   int newton_cap = 100;
   MlpDev* mlp = nullptr;
@@ -499,6 +503,8 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   e = cudaMalloc(&x->scal, sizeof(DevScalars));
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(scalars)"));
   e = cudaMalloc(&x->stats, sizeof(DevStats));
+  if (e == cudaSuccess) e = cudaMallocHost(&x->h_scal, sizeof(DevScalars));
+  if (e == cudaSuccess) e = cudaMallocHost(&x->h_stats, sizeof(DevStats));
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(stats)"));
   DevScalars s0{};
   s0.dt = 1.e-15;
@@ -539,6 +545,8 @@ extern "C" void ecg_destroy(ecg_ctx* x) {
   cudaFree(x->tmp);
   cudaFree(x->scal);
   cudaFree(x->stats);
+  cudaFreeHost(x->h_scal);
+  cudaFreeHost(x->h_stats);
   cudaFree(x->mlp);
   cudaFree(x->rec_x);
   cudaFree(x->rec_y);
@@ -727,7 +735,8 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
   h.max_it = x->c.max_iterations;
   h.mode = mode;
   h.done = (mode == 1 && h.it >= h.max_it) || (mode == 2 && h.t >= h.t_end);
-  ECG_CUDA(cudaMemcpyAsync(x->scal, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+  *x->h_scal = h;  // the previous call synchronised, so the staging buffer is free
+  ECG_CUDA(cudaMemcpyAsync(x->scal, x->h_scal, sizeof(h), cudaMemcpyHostToDevice, x->stream));
   ECG_CUDA(cudaMemsetAsync(x->stats, 0, sizeof(DevStats), x->stream));
   const int cur0 = x->cur;  // a step that finds the stop flag set writes nothing, so the state that
                             // holds the result is decided by the number of steps actually taken
@@ -764,11 +773,11 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
       if (r.done) break;
     }
   }
-  DevScalars r{};
-  DevStats ds{};
-  ECG_CUDA(cudaMemcpyAsync(&r, x->scal, sizeof(r), cudaMemcpyDeviceToHost, x->stream));
-  ECG_CUDA(cudaMemcpyAsync(&ds, x->stats, sizeof(ds), cudaMemcpyDeviceToHost, x->stream));
+  ECG_CUDA(cudaMemcpyAsync(x->h_scal, x->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, x->stream));
+  ECG_CUDA(cudaMemcpyAsync(x->h_stats, x->stats, sizeof(DevStats), cudaMemcpyDeviceToHost, x->stream));
   ECG_CUDA(cudaStreamSynchronize(x->stream));
+  const DevScalars r = *x->h_scal;
+  const DevStats ds = *x->h_stats;
   done_steps = r.it - h.it;
   x->cur = cur0 ^ (int)(done_steps & 1);
   *dt = r.dt;

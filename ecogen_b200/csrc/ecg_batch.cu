@@ -27,6 +27,13 @@
 #ifndef ECG_BATCH_SM_THREADS
 #define ECG_BATCH_SM_THREADS 896
 #endif
+// Cells of one work item for TB threads: TB - ECG_BATCH_ITEM_TRIM.  With a trim of 1 the item's
+// TB faces take one round of the block; with 0 the item has TB + 1 faces and one warp computes two
+// while the block waits at the next barrier.  Measured on 4096 batched tubes: trim 0 1657 M, trim 1
+// 2066 M cell-updates/s.
+#ifndef ECG_BATCH_ITEM_TRIM
+#define ECG_BATCH_ITEM_TRIM 1
+#endif
 #if ECG_BATCH_SM_THREADS > 0
 #define ECG_BATCH_BOUNDS(TB) __launch_bounds__(TB, (ECG_BATCH_SM_THREADS / (TB) > 0 ? ECG_BATCH_SM_THREADS / (TB) : 1))
 #else
@@ -58,12 +65,13 @@ struct BatchParams {
 
 template <int NP, int TB, int PASS>
 struct BatchTile {
+  static constexpr int TC = TB - ECG_BATCH_ITEM_TRIM;  // cells of one work item
   static constexpr int H = (PASS == PASS_O1) ? 1 : 2;
-  static constexpr int RL = TB + 2 * H;
+  static constexpr int RL = TC + 2 * H;
   static constexpr int NQ = Fields<NP, 1>::NQ + ((PASS == PASS_CORR) ? 1 : 0);
-  static constexpr int NS = (PASS == PASS_O1) ? 0 : TB + 3;
+  static constexpr int NS = (PASS == PASS_O1) ? 0 : TC + 3;
   static constexpr size_t smem_bytes() {
-    return sizeof(double) * ((size_t)RL * NQ + (size_t)NS * Fields<NP, 1>::NSL + (size_t)(TB + 1) * Fields<NP, 1>::NFL);
+    return sizeof(double) * ((size_t)RL * NQ + (size_t)NS * Fields<NP, 1>::NSL + (size_t)(TC + 1) * Fields<NP, 1>::NFL);
   }
 };
 
@@ -73,9 +81,10 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
   using FL = Fields<NP, 1>;
   using K = BatchTile<NP, TB, PASS>;
   constexpr bool O2 = (PASS != PASS_O1);
+  constexpr int TC = K::TC;
   constexpr int RS = K::RL;
   constexpr int SS = O2 ? K::NS : 1;
-  constexpr int FS = TB + 1;
+  constexpr int FS = TC + 1;
   extern __shared__ double smem[];
   double* sq = smem;
   double* sa0 = sq + (size_t)FL::NQ * RS;
@@ -131,7 +140,7 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
       __syncthreads();
     }
     double dtmax = 1.e10;
-    for (int j = tid; j <= TB; j += TB) {
+    for (int j = tid; j <= TC; j += TB) {
       int gl = org + j - 1;
       if (gl < 0 || gl + 1 >= n) continue;
       int rl = j - 1 + K::H, rr = rl + 1;
@@ -173,8 +182,9 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
     }
     __syncthreads();
     const int g = org + tid;
+    const bool own = tid < TC && g < n;  // this thread's cell of the item
     CellPrim<NP, 1> cp;
-    if (g < n) {
+    if (own) {
       const int64_t cell = C.off + g;
       double an[NP], rn[NP], pn[NP], aa[NP], am[NP], ae[NP], amom[1] = {0.}, aE = 0.;
       double p0 = P.sn[(int64_t)FL::P * nn + cell];
@@ -210,8 +220,8 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
     }
     SeedGate<NP> sg;
     const bool seeded = P.mlp != nullptr;  // uniform over the launch
-    if (seeded) seed_gate<NP, 1>(P, M, g < n, cp, sg);
-    if (g < n) {
+    if (seeded) seed_gate<NP, 1>(P, M, own, cp, sg);
+    if (own) {
       const int64_t cell = C.off + g;
       CellCounters cc;
       if (seeded)
@@ -359,7 +369,7 @@ void drop_graphs(ecg_batch* b) {
 ecg_status build_items(ecg_batch* b, int tile) {
   std::vector<int2> it;
   for (int c = 0; c < b->ncases; c++)
-    for (int s = 0; s < b->hcases[c].n; s += tile) it.push_back(make_int2(c, s));
+    for (int s = 0; s < b->hcases[c].n; s += tile - ECG_BATCH_ITEM_TRIM) it.push_back(make_int2(c, s));
   cudaFree(b->items);
   b->items = nullptr;
   BCUDA(cudaMalloc(&b->items, sizeof(int2) * it.size()));

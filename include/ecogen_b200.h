@@ -255,7 +255,8 @@ ecg_status ecg_batch_download_prim(ecg_batch* b, double* const* fields, int64_t 
 /* Advance every case nsteps steps (each with its own dt); dt/t arrays of ncases (may be NULL). */
 ecg_status ecg_batch_step(ecg_batch* b, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats);
 ecg_status ecg_batch_set_seed_model(ecg_batch* b, const ecg_mlp* mlp);
-/* Tile size (cells per work item) and threads per block; 0 = autotuned. */
+/* Tile = threads per block (64, 128 or 256; 0 = autotuned); a work item covers tile - 1 cells of one
+ * case, so its tile faces take one round of the block.  threads must be 0 or equal to tile. */
 ecg_status ecg_batch_set_shape(ecg_batch* b, int32_t tile, int32_t threads);
 ecg_status ecg_batch_autotune(ecg_batch* b, int32_t* tile, int32_t* threads);
 int64_t ecg_batch_total_cells(const ecg_batch* b);
