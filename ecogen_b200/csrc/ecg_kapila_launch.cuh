@@ -41,9 +41,10 @@ cudaError_t kapila_launch_tr(int np, int dim, bool ptmu, int pass, const StepPar
                              const ecg_eos* eos, double eps, cudaStream_t s, bool prepare);
 constexpr int KAPILA_MAX_TRANSPORTS = 2;
 
-// The EOS combination of the shipped workloads (SG liquid first, ideal gases after) has kernels
-// (plain and seeded) with the types compiled in and no THINC or PT-relaxation code; every other
-// case (other EOS, THINC, PT relaxation, passive transports, p-T-mu) runs the generic kernels.
+// The EOS combination of the shipped workloads (SG liquid first, ideal gases after; two stiffened
+// gases with p-T-mu relaxation) has kernels (plain and seeded) with the types compiled in and no
+// THINC or PT-relaxation code; every other case (other EOS, THINC, PT relaxation, passive
+// transports) runs the generic kernels.
 template <int NP>
 constexpr int eos_fast_types() {
   return NP == 2 ? eos_types_code<2>(ECG_EOS_SG, ECG_EOS_IG) : eos_types_code<3>(ECG_EOS_SG, ECG_EOS_IG, ECG_EOS_IG);
@@ -54,10 +55,15 @@ template <int NP>
 constexpr int eos_fast_limiter() {
   return NP == 2 ? ECG_LIM_VANLEER : ECG_LIM_MINMOD;
 }
-template <int NP>
+// With p-T-mu relaxation the shipped workload has a stiffened-gas liquid and a stiffened-gas vapour.
+template <int NP, bool PTMU>
+constexpr int workload_types() {
+  return PTMU ? eos_types_code<NP>(ECG_EOS_SG, ECG_EOS_SG) : eos_fast_types<NP>();
+}
+template <int NP, bool PTMU = false>
 inline bool eos_is_fast(const ecg_eos* eos) {
   int t[3] = {eos[0].type, eos[1].type, NP > 2 ? eos[2].type : 0};
-  return eos_types_code<NP>(t[0], t[1], t[2]) == eos_fast_types<NP>();
+  return eos_types_code<NP>(t[0], t[1], t[2]) == workload_types<NP, PTMU>();
 }
 
 template <int NP, int DIM, bool PTMU>
@@ -66,7 +72,7 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
   // kernels with the learned seed are separate variants, so that the plain kernels carry none of
   // its registers; with prepare both are configured
 #ifndef ECG_NO_EOS_SPECIALIZATION
-  constexpr bool kFast = !PTMU;
+  constexpr bool kFast = true;
 #else
   constexpr bool kFast = false;
 #endif
@@ -75,8 +81,8 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
     return kapila_launch_tr(NP, DIM, PTMU, pass, P, G, eos, eps, s, prepare);
   }
   // EOS types compiled in (limiters at run time), and EOS types plus the workload's limiter
-  constexpr int kEos = kFast ? fast_code(eos_fast_types<NP>(), -1) : EOS_DYNAMIC;
-  constexpr int kEosLim = kFast ? fast_code(eos_fast_types<NP>(), eos_fast_limiter<NP>()) : EOS_DYNAMIC;
+  constexpr int kEos = kFast ? fast_code(workload_types<NP, PTMU>(), -1) : EOS_DYNAMIC;
+  constexpr int kEosLim = kFast ? fast_code(workload_types<NP, PTMU>(), eos_fast_limiter<NP>()) : EOS_DYNAMIC;
   if (prepare) {
     cudaError_t e = launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, false, kEos>(pass, P, G, eos, eps, s, true);
@@ -87,7 +93,7 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEosLim>(pass, P, G, eos, eps, s, true);
     return e;
   }
-  const bool fast_eos = kFast && !P.thinc && !P.pt && eos_is_fast<NP>(eos);
+  const bool fast_eos = kFast && !P.thinc && !P.pt && eos_is_fast<NP, PTMU>(eos);
   const int L = eos_fast_limiter<NP>();
   const bool fast_lim = P.lim[0] == L && P.lim[1] == L && P.lim[2] == L && P.lim[3] == L;
   if (P.mlp != nullptr) {  // the seeded kernels get the same compile-time configurations as the plain ones
