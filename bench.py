@@ -7,7 +7,10 @@ the library's own XML reader.  One "step" is one full time step of the whole gri
 (predictor + corrector + relaxations + dt update).  The state (2048^2 x 8 doubles = 268 MB per
 copy) is larger than L2, so no L2 flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p2]
+
+Other workloads' lines say in config.l2 whether their data exceeds L2 (the 1D tube of 1000 cells is
+L2-resident: a latency-bound configuration, not a bandwidth measurement).
 
 Multi-GPU: the path does not shard (one case per GPU; a single large domain would need halo
 exchange, which this workload does not use), so N ranks run N independent replicas ("replicas
@@ -71,6 +74,22 @@ def state_fields(case) -> int:
         return case.nphases + 3 + case.dim
     per_phase = 1 if case.model.upper() == "EULER" else 2
     return per_phase * case.nphases + 2 + case.dim
+
+
+L2_BYTES = 126 * 2 ** 20
+
+
+def l2_note(case) -> str:
+    """Whether one step's data (the state read, the state written, the MUSCL half-step state) exceeds L2."""
+    state = 8 * state_fields(case) * case.ncells
+    ws = state * (3 if case.second_order else 2)
+    if state > L2_BYTES:
+        return f"state {state / 1e6:.0f} MB per copy, larger than the 126 MB L2 (no flush needed)"
+    if ws > L2_BYTES:
+        return (f"state {state / 1e6:.0f} MB per copy, {ws / 1e6:.0f} MB touched per step, more than the 126 MB L2; "
+                "no flush between steps (part of the state stays L2-resident)")
+    return (f"state {state / 1e6:.2f} MB: L2-resident, no flush between steps (a latency-bound configuration, "
+            "not a bandwidth measurement)")
 
 
 def bytes_per_cell_update(case) -> int:
@@ -371,7 +390,7 @@ def main():
         args.config]
     config = {"workload": f"{workload}, {'x'.join(str(n) for n in case.cells if n > 1)} cells, FP64",
               "cells": case.ncells, "phases": case.nphases, "dim": case.dim, "order": 2 if case.second_order else 1,
-              "l2": "state larger than L2 (no flush needed)", "parallelism": f"replicas{args.gpus}"}
+              "l2": l2_note(case), "parallelism": f"replicas{args.gpus}"}
 
     if args.impl == "reference":
         if rank != 0:
