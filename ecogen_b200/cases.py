@@ -515,3 +515,19 @@ def ptueq_bubble_2d(n: int = 64, iterations: int = 20, limiter: Optional[str] = 
     return Case(name, [AIR_IG, WATER_SG300], (L, L, L if nz > 1 else 1.0), (n, ny or n, nz), states, domains,
                 model=PTUEQ,
                 cfl=0.6, iterations=iterations, second_order=limiter, boundaries=boundaries)
+
+
+def euler_blast_2d(n: int = 64, ny: Optional[int] = None, nz: int = 1, iterations: int = 20,
+                   order: Optional[str] = "vanleer", name: str = "eulerBlast2D",
+                   boundaries: Optional[List[str]] = None) -> Case:
+    """Single-phase air (Euler model) on a 1 m square (a 1 m cube with ``nz`` > 1): a dense,
+    high-pressure disc (a cylinder along z in 3D) off the centre, moving air left of x = 0.2 m."""
+    states = [State("ambient", [PhaseState(1.0, 1.0)], 1.0e5),
+              State("blast", [PhaseState(1.0, 5.0)], 1.0e6),
+              State("inflow", [PhaseState(1.0, 1.5)], 2.0e5, (80.0, 20.0, 0.0))]
+    domains = [Domain("base", "ambient", "entireDomain"),
+               Domain("blast", "blast", "disc", {"axis1": "x", "axis2": "y", "radius": 0.15,
+                                                "center": (0.55, 0.45, 0.5)}),
+               Domain("inflow", "inflow", "halfSpace", {"axis": "x", "origin": 0.2, "direction": "negative"})]
+    return Case(name, [AIR_IG], (1.0, 1.0, 1.0 if nz > 1 else 0.1), (n, ny or n, nz), states, domains,
+                model="Euler", cfl=0.6, iterations=iterations, second_order=order, boundaries=boundaries)

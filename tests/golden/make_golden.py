@@ -102,6 +102,13 @@ def golden_cases():
     c.pt_relaxation = True
     g["bubble2d_pt"] = c
     g["euler1d_o2"] = cases.euler_shock_tube(ncells=200, iterations=40, order="vanleer", name="eulerO2")
+    # Euler model on 2D and 3D meshes
+    g["euler2d_o2_walls"] = cases.euler_blast_2d(n=24, ny=20, iterations=12,
+                                                 boundaries=["nonReflecting", "wall", "symmetry", "nonReflecting"])
+    g["euler2d_o1"] = cases.euler_blast_2d(n=20, iterations=10, order=None, name="eulerBlastO1")
+    g["euler3d_o2"] = cases.euler_blast_2d(n=10, ny=8, nz=6, iterations=5, order="minmod", name="eulerBlast3D",
+                                           boundaries=["wall", "nonReflecting", "nonReflecting", "symmetry",
+                                                       "wall", "nonReflecting"])
     # temperature-pressure-velocity equilibrium model (ModPTUEq)
     g["ptueq_tube_o2"] = cases.ptueq_shock_tube_1d(ncells=200, iterations=60)
     g["ptueq_tube_o1"] = cases.ptueq_shock_tube_1d(ncells=300, iterations=None, total_time=1.0e-4, order=None,

@@ -17,7 +17,8 @@ KAPILA_KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1
                "expansion2d_ptmu", "tube1d_wall_o1", "tube1d_wall_o2", "bubble2d_sym_o2", "bubble2d_sym_o1",
                "cavity3d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc", "tube1d_transport_o2", "bubble2d_transport",
                "tube1d_transport_o1", "tube1d_pt_o1", "bubble2d_pt"]
-EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2", "euler1d_transport_o2"]
+EULER_KEYS = ["euler1d_o1", "euler1d_o2", "euler1d_wall_o2", "euler1d_transport_o2", "euler2d_o2_walls", "euler2d_o1",
+              "euler3d_o2"]
 
 
 def _compare(key, got, g):
@@ -184,3 +185,23 @@ def test_driver_writes_reference_results(key, golden_cases, tmp_path):
         assert rel_l1(got[name], ref) <= TOL, name
     # |grad rho| of the output (finite differences of the density: differences amplify the 1e-12)
     assert rel_l1(raw["gradRho"], g["final_gradRho"]) <= 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_gpu_euler_matches_oracle_multid(dim, tmp_path):
+    """Euler model on meshes of several tiles per axis (ragged), symmetry and open sides."""
+    from ecogen_b200 import cases
+    if dim == 2:
+        case = cases.euler_blast_2d(n=70, ny=45, iterations=20, name="eulerBlast70",
+                                    boundaries=["wall", "nonReflecting", "symmetry", "nonReflecting"])
+    else:
+        case = cases.euler_blast_2d(n=13, ny=9, nz=7, iterations=5, name="eulerBlast13",
+                                    boundaries=["nonReflecting", "wall", "symmetry", "nonReflecting", "wall", "wall"])
+    out = gpu_run(case, tmp_path)
+    sim = oracle.Sim(case)
+    sim.step(case.iterations)
+    o = sim.fields()
+    for name in ("rho", "p", "u", "E"):
+        assert rel_l1(out[name], o[name]) <= TOL, name
+    assert out["dt"] == pytest.approx(sim.dt.value, rel=1e-12)

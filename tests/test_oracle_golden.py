@@ -15,7 +15,8 @@ KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_
         "bubble2d_sym_o1", "cavity3d_wall_o2", "euler1d_wall_o2", "tube1d_thinc_o2", "bubble2d_thinc",
         "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2", "tube1d_pt_o1",
         "bubble2d_pt", "ptueq_tube_o2", "ptueq_tube_o1", "ptueq_tube_wall_o1",
-        "ptueq_bubble2d_o2", "ptueq_bubble2d_o1_sym", "ptueq_bubble2d_thinc", "ptueq_bubble3d_o2"]
+        "ptueq_bubble2d_o2", "ptueq_bubble2d_o1_sym", "ptueq_bubble2d_thinc", "ptueq_bubble3d_o2",
+        "euler2d_o2_walls", "euler2d_o1", "euler3d_o2"]
 
 
 @pytest.mark.parametrize("key", KEYS)
