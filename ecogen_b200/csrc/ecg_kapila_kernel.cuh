@@ -48,7 +48,8 @@ __device__ __forceinline__ bool iface_detect(double aCell, double aOther, double
 }
 
 template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES, int NTM = 0>
-__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH, TileShape<DIM>::MINB)
+__global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
+                                  (PTMU && DIM == 2 && ECG_PTMU_MINB > 0) ? ECG_PTMU_MINB : TileShape<DIM>::MINB)
     k_kapila_step(StepParams P, Geometry G, Model<NP> M0) {
   const Model<NP> M = specialize_eos<NP, TYPES>(M0);
   using K = KapilaStep<NP, DIM, PASS, NTM>;

@@ -54,6 +54,13 @@ enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
 #ifndef ECG_TILE3D_MINB
 #define ECG_TILE3D_MINB 2
 #endif
+// Resident blocks asked for the 2D p-T-mu kernels (0: the tile shape's MINB).  Their saturation
+// solve makes them larger than the other Kapila kernels: at 7 blocks (72 registers) they spilled
+// 1.4 KB a thread and wrote 4-6x the algorithmic bytes to DRAM.  Measured on the 1024^2 expansion
+// (cell-updates/s): 7 blocks 360 M, 6 370 M, 5 388 M, 4 (128 registers) 389 M.
+#ifndef ECG_PTMU_MINB
+#define ECG_PTMU_MINB 4
+#endif
 template <int DIM>
 struct TileShape;
 template <>
