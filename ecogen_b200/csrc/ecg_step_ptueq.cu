@@ -147,11 +147,16 @@ __device__ __forceinline__ void hllc_pt(const PtSide& L, const double ul[3], con
 }
 
 // Register budget: the resident-block target of the tile shape (TileShape::MINB), as the Kapila
-// kernels; ECG_PTUEQ_NO_MINB leaves the register count to the compiler.  Measured on the 2D bubble at
-// 2048^2 (MUSCL + van Leer): compiler's choice (94 registers, 20 warps per SM) 1170 M cell-updates/s,
-// 7 blocks of 128 threads (72 registers, 28 warps) 1536 M.
+// kernels, with 8 blocks in 2D (ECG_PTUEQ_MINB2D); ECG_PTUEQ_NO_MINB leaves the register count to the
+// compiler.  Measured on the 2D bubble at 2048^2 (MUSCL + van Leer, cell-updates/s): compiler's choice
+// (94 registers, 20 warps per SM) 1170 M; blocks of 128 threads per SM: 5 1182 M, 6 1362 M,
+// 7 (72 registers) 1540 M, 8 (64 registers, 32 warps) 1572 M, 9 1468 M, 10 1385 M.
+#ifndef ECG_PTUEQ_MINB2D
+#define ECG_PTUEQ_MINB2D 8
+#endif
 #ifndef ECG_PTUEQ_NO_MINB
-#define ECG_PTUEQ_BOUNDS(DIM, PASS) __launch_bounds__(PtStep<DIM, PASS>::NTH, TileShape<DIM>::MINB)
+#define ECG_PTUEQ_BOUNDS(DIM, PASS) \
+  __launch_bounds__(PtStep<DIM, PASS>::NTH, DIM == 2 ? ECG_PTUEQ_MINB2D : TileShape<DIM>::MINB)
 #else
 #define ECG_PTUEQ_BOUNDS(DIM, PASS) __launch_bounds__(PtStep<DIM, PASS>::NTH)
 #endif
