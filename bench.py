@@ -7,7 +7,7 @@ the library's own XML reader.  One "step" is one full time step of the whole gri
 (predictor + corrector + relaxations + dt update).  The state (2048^2 x 8 doubles = 268 MB per
 copy) is larger than L2, so no L2 flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p2]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p2|e2]
 
 Other workloads' lines say in config.l2 whether their data exceeds L2 (the 1D tube of 1000 cells is
 L2-resident: a latency-bound configuration, not a bandwidth measurement).
@@ -51,6 +51,8 @@ def make_case(config: str, size: int | None):
         return cases.expansion_tube_2d(n=size or 1024, iterations=10 ** 6)
     if config == "p2":
         return cases.ptueq_bubble_2d(n=size or 2048, iterations=10 ** 6)
+    if config == "e2":
+        return cases.euler_blast_2d(n=size or 2048, iterations=10 ** 6)
     if config == "c4":
         # one case of the batched workload (its per-case reference timing)
         return cases.shock_tube_1d(ncells=1000, iterations=10 ** 6, order="vanleer")
@@ -376,7 +378,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "p2"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "p2", "e2"])
     ap.add_argument("--no-seeded", action="store_true", help="skip the learned-seed measurement")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -388,7 +390,8 @@ def main():
                 "c2": "2D shock-bubble, Kapila 2-phase, MUSCL + van Leer",
                 "c3": "3D three-phase cavity collapse, Kapila, MUSCL + minmod",
                 "c5": "2D liquid/vapour expansion, Kapila + p-T-mu relaxation, MUSCL + van Leer",
-                "p2": "2D air bubble in water, PTUEq (temperature-pressure-velocity equilibrium), MUSCL + van Leer"}[
+                "p2": "2D air bubble in water, PTUEq (temperature-pressure-velocity equilibrium), MUSCL + van Leer",
+                "e2": "2D blast in air, Euler (single phase), MUSCL + van Leer"}[
         args.config]
     config = {"workload": f"{workload}, {'x'.join(str(n) for n in case.cells if n > 1)} cells, FP64",
               "cells": case.ncells, "phases": case.nphases, "dim": case.dim, "order": 2 if case.second_order else 1,

@@ -100,8 +100,17 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
   }
 }
 
+// Register budget: ECG_EULER_MINB2D > 0 asks the compiler for that many resident blocks per SM in 2D;
+// 0 leaves the register count to the compiler.  Measured on a 2048^2 blast (MUSCL + van Leer,
+// cell-updates/s): compiler's choice (80 registers, 6 blocks of 128 threads) 2449 M; 6 blocks 2721 M;
+// 7 (72 registers) 2909 M; 8 (64 registers) 2754 M.
+#ifndef ECG_EULER_MINB2D
+#define ECG_EULER_MINB2D 7
+#endif
+
 template <int DIM, int PASS, int NTM = 0>
-__global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH)
+__global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
+                                  (DIM == 2 && ECG_EULER_MINB2D > 0) ? ECG_EULER_MINB2D : 1)
     k_euler_step(StepParams P, Geometry G, EosParams q, double eps) {
   using K = EulerStep<DIM, PASS, NTM>;
   using TS = TileShape<DIM>;
