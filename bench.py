@@ -115,13 +115,15 @@ def pass_bytes_per_cell(case) -> dict:
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / cells: 2D two-phase MUSCL at 1536^2, profiles/k_kapila_step_shock_bubble_1536.md; 3D
 # three-phase MUSCL at 128^3, profiles/k_kapila_step_cavity3d_128.md; 2D PTUEq MUSCL at 1536^2,
-# profiles/k_ptueq_step_bubble_1536.md; 2D p-T-mu at 1536^2, profiles/k_kapila_step_ptmu_expansion_1536.md);
+# profiles/k_ptueq_step_bubble_1536.md; 2D p-T-mu at 1536^2, profiles/k_kapila_step_ptmu_expansion_1536.md;
+# 2D Euler at 2048^2, profiles/k_euler_step_blast_2048.md);
 # the kernels stream the state once,
 # so traffic scales with the cell count.
 NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2, True, "pass1"): 125.14,
                         ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89,
                         ("ptueq", 2, 2, True, "pass2"): 150.78, ("ptueq", 2, 2, True, "pass1"): 91.56,
-                        ("kapila_ptmu", 2, 2, True, "pass2"): 181.05, ("kapila_ptmu", 2, 2, True, "pass1"): 112.08}
+                        ("kapila_ptmu", 2, 2, True, "pass2"): 181.05, ("kapila_ptmu", 2, 2, True, "pass1"): 112.08,
+                        ("euler", 1, 2, True, "pass2"): 98.52, ("euler", 1, 2, True, "pass1"): 64.92}
 # Batched tubes (2048 cases, profiles/k_batch_shock_tubes_2048.md): predictor + corrector DRAM bytes per
 # cell-update.
 NCU_BATCH_BYTES_PER_CELL_UPDATE = 98.05 + 157.17
