@@ -34,8 +34,11 @@ enum { PASS_O1 = 0, PASS_PRED = 1, PASS_CORR = 2 };
 // two-phase MUSCL step (cell-updates/s): 16x15 / 256 threads / 2 blocks (128 registers) 652 M;
 // 16x15 / 256 / 3 (80) 825 M; 16x15 / 256 / 4 (64) 790 M; 8x14 / 128 / 6 (80) 849 M;
 // 8x14 / 128 / 7 (72) 949 M; 8x14 / 128 / 8 (64) 883 M; 16x7 / 128 / 7 868 M; 8x7 / 64 / 14 719 M.
+// 1D single cases (the 1000-cell tube of the reference's CPU-sized configuration) run a few blocks
+// and are latency-bound: fewer spills matter more than resident warps.  Measured on that tube
+// (cell-updates/s): 3 blocks per SM (80 registers) 48.6 M, 2 (128 registers) 51.8 M, 1 52.8 M.
 #ifndef ECG_TILE1D_MINB
-#define ECG_TILE1D_MINB 3
+#define ECG_TILE1D_MINB 2
 #endif
 #ifndef ECG_TILE2D_X
 #define ECG_TILE2D_X 8
