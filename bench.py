@@ -1,16 +1,24 @@
 """Benchmark: cell-updates/s of the ECOGEN Cartesian FV step on one B200 (or N replicas).
 
-Default workload (the configuration the headline metric is quoted on): 2D shock-bubble
-interaction, Kapila 2-phase, MUSCL-Hancock + van Leer, FP64, 2048 x 2048 cells on 1 x 1 cm,
-CFL 0.6 — seeded synthetic input generated by ecogen_b200.cases.shock_bubble_2d and read through
-the library's own XML reader.  One "step" is one full time step of the whole grid
-(predictor + corrector + relaxations + dt update).  The state (2048^2 x 8 doubles = 268 MB per
+Default workload (the largest single-GPU configuration of the metric, the one the learned-seed target
+is quoted on): 3D three-phase cavity collapse, Kapila model, MUSCL-Hancock + minmod, FP64, 256^3 cells,
+64 seeded spherical gas inclusions (two ideal gases in a stiffened-gas liquid), CFL 0.6 -- seeded
+synthetic input generated by ecogen_b200.cases.cavity_collapse_3d and read through the library's own
+XML reader.  The line reports the plain FP64 path (`value`) and the same workload with the learned
+pressure-relaxation seed installed (`mlp_seeded`).  One "step" is one full time step of the whole
+grid (predictor + corrector + relaxations + dt update).  The state (256^3 x 11 doubles = 1.48 GB per
 copy) is larger than L2, so no L2 flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p2|e2]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c3|c2|c1|c4|c5|p2|e2]
 
+c2 is the 2D shock-bubble (Kapila 2-phase, MUSCL + van Leer, 2048^2), c1 the 1000-cell first-order
+tube, c4 4096 batched 1D tubes, c5 the 1024^2 p-T-mu expansion, p2 / e2 the PTUEq and Euler models.
 Other workloads' lines say in config.l2 whether their data exceeds L2 (the 1D tube of 1000 cells is
 L2-resident: a latency-bound configuration, not a bandwidth measurement).
+
+Two rooflines are reported for the dominant kernel: HBM (algorithmic bytes over the measured copy
+bandwidth) and FP64 (FP64 thread instructions per cell, counted by ncu on one launch, over the FP64
+pipe rate measured live by a DFMA-throughput probe).
 
 Multi-GPU: the path does not shard (one case per GPU; a single large domain would need halo
 exchange, which this workload does not use), so N ranks run N independent replicas ("replicas
@@ -113,19 +121,15 @@ def pass_bytes_per_cell(case) -> dict:
 
 
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch / cells: 2D two-phase MUSCL at 1536^2, profiles/k_kapila_step_shock_bubble_1536.md; 3D
-# three-phase MUSCL at 128^3, profiles/k_kapila_step_cavity3d_128.md; 2D PTUEq MUSCL at 1536^2,
-# profiles/k_ptueq_step_bubble_1536.md; 2D p-T-mu at 1536^2, profiles/k_kapila_step_ptmu_expansion_1536.md;
-# 2D Euler at 2048^2, profiles/k_euler_step_blast_2048.md);
-# the kernels stream the state once,
-# so traffic scales with the cell count.
+# of one launch / cells: 2D two-phase MUSCL at 1536^2, 3D three-phase MUSCL at 128^3, 2D PTUEq MUSCL at
+# 1536^2, 2D p-T-mu at 1536^2, 2D Euler at 2048^2).  The kernels stream the state once, so traffic
+# scales with the cell count.
 NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2, True, "pass1"): 125.14,
                         ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89,
                         ("ptueq", 2, 2, True, "pass2"): 150.78, ("ptueq", 2, 2, True, "pass1"): 91.56,
                         ("kapila_ptmu", 2, 2, True, "pass2"): 181.05, ("kapila_ptmu", 2, 2, True, "pass1"): 112.08,
                         ("euler", 1, 2, True, "pass2"): 98.52, ("euler", 1, 2, True, "pass1"): 64.92}
-# Batched tubes (2048 cases, profiles/k_batch_shock_tubes_2048.md): predictor + corrector DRAM bytes per
-# cell-update.
+# Batched tubes (2048 cases): predictor + corrector DRAM bytes per cell-update.
 NCU_BATCH_BYTES_PER_CELL_UPDATE = 98.05 + 157.17
 
 
@@ -189,6 +193,30 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def fp64_pipe_peak(device_index: int):
+    """FP64 pipe rate of this GPU in thread instructions per second, measured live by the DFMA
+    throughput probe (ecogen_b200/libecg_probe.so), with the SM clock sampled meanwhile."""
+    import ctypes as C
+    path = os.path.join(ROOT, "ecogen_b200", "libecg_probe.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.ecg_probe_fp64.argtypes = [C.c_int, C.c_longlong, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    rate, ms = C.c_double(), C.c_double()
+    with ClockSampler(device_index) as clk:
+        rc = lib.ecg_probe_fp64(8, 1 << 19, 5, C.byref(rate), C.byref(ms))
+    if rc != 0:
+        return None
+    return {"dfma_per_s": rate.value, "launch_ms": ms.value, "clocks": clk.summary(),
+            "how": "148 SMs x 8 blocks x 256 threads, 8 independent DFMA chains per thread, best of 5 launches"}
+
+
+# FP64 thread instructions per cell of one launch of a step kernel, counted by ncu
+# (smsp__sass_thread_inst_executed_op_fp64_pred_on.sum / cells), keyed like NCU_TRAFFIC_PER_CELL.  The
+# count does not depend on the mesh size beyond boundary cells (measured at 512^2 in 2D, 64^3 in 3D).
+NCU_FP64_PER_CELL: dict = {}
+
+
 def max_over_ranks(value: float, device: str) -> float:
     """Max of a per-rank device time over all ranks of the default process group (if any)."""
     import torch
@@ -203,20 +231,44 @@ def max_over_ranks(value: float, device: str) -> float:
 # ----------------------------------------------------------------------------------- reference arm
 
 
-def reference_sample(steps: int, warmup: int, size: int = 256, iters: int = 4, procs: int | None = None,
-                     config: str = "c2"):
+# Per-process mesh of the reference sample of each workload: large enough that the step dominates the
+# reference's set-up, small enough that a sample of a few iterations takes seconds on one core
+# (reference, one core: 2D 256^2 MUSCL ~0.9 s per step, 3D 32^3 three-phase MUSCL ~0.7 s per step).
+REF_SAMPLE_SIZE = {"c1": 1000, "c3": 32, "c4": None}
+# iterations of a sample's long run (the 1D tubes take milliseconds per step)
+REF_SAMPLE_ITERS = {"c1": 200, "c4": 200}
+REF_SAMPLE_BUDGET_S = 150.0
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_sample(steps: int, warmup: int, iters: int | None = None, procs: int | None = None,
+                     config: str = "c3", budget_s: float = REF_SAMPLE_BUDGET_S):
     """Time the reference CPU solver (oracle/_ref/ECOGEN, built from the reference sources).
 
-    Each sample runs `procs` independent reference processes concurrently (one per host core) on a
-    `size`^2 version of the workload for `iters` iterations, and once for 1 iteration; the
-    difference removes initialisation and output, giving cell-updates/s over all cores.
+    Each sample runs `procs` independent reference processes concurrently (one per host core; the
+    reference has no threads and no MPI exists on the box) on a reduced mesh of the workload
+    (REF_SAMPLE_SIZE) for `iters` iterations, and once for 1 iteration; the difference removes
+    initialisation and output, giving cell-updates/s over all cores.  Samples stop after
+    `warmup + steps` or once `budget_s` seconds have passed with at least one timed sample.
     """
     from ecogen_b200 import cases
     from oracle import refrun
     if not refrun.available():
         return None
     procs = procs or len(os.sched_getaffinity(0))
-    base = tempfile.mkdtemp(prefix="ecg_ref_", dir=os.path.join(ROOT, "_work") if os.path.isdir(os.path.join(ROOT, "_work")) else None)
+    size = REF_SAMPLE_SIZE.get(config, 256)
+    iters = iters or REF_SAMPLE_ITERS.get(config, 4)
+    base = tempfile.mkdtemp(prefix="ecg_ref_")
 
     def prepare(nit):
         dirs = []
@@ -242,15 +294,20 @@ def reference_sample(steps: int, warmup: int, size: int = 256, iters: int = 4, p
     c = make_case(config, size)
     cells = c.ncells
     samples = []
+    start = time.perf_counter()
     for i in range(warmup + steps):
         t1 = run_all(d1)
         tn = run_all(dn)
         if i >= warmup:
             samples.append(procs * cells * (iters - 1) / max(tn - t1, 1e-9))
+        if samples and time.perf_counter() - start > budget_s:
+            break
     shutil.rmtree(base, ignore_errors=True)
-    return {"value": statistics.median(samples), "cores": procs,
-            "sample": f"{procs} concurrent reference processes, {size}^2 cells each, {iters}-1 iterations "
-                      f"(time of an {iters}-iteration run minus a 1-iteration run)", "samples": samples}
+    mesh = "x".join(str(n) for n in c.cells if n > 1)
+    return {"value": statistics.median(samples), "cores": procs, "cpu": cpu_model(),
+            "sample": f"{procs} concurrent reference processes (one per core of a {cpu_model()}), {mesh} cells each, "
+                      f"{iters}-1 iterations (time of an {iters}-iteration run minus a 1-iteration run); "
+                      f"{len(samples)} timed samples, median", "samples": samples}
 
 
 # ------------------------------------------------------------------------------------ batched mode
@@ -380,7 +437,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "p2", "e2"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "p2", "e2"])
     ap.add_argument("--no-seeded", action="store_true", help="skip the learned-seed measurement")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -410,7 +467,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
                 "cpu_baseline": {"value": r["value"], "unit": "cell-updates/s", "cores": r["cores"],
-                                 "kind": "reference", "sample": r["sample"]},
+                                 "kind": "reference", "cpu": r["cpu"], "sample": r["sample"]},
                 "e2e": {"value": r["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -539,9 +596,21 @@ def main():
         traffic = NCU_TRAFFIC_PER_CELL.get(tkey)
         kname = {"pass1": "MUSCL predictor" if case.second_order else "first-order step",
                  "pass2": "MUSCL corrector"}[top]
+        # FP64 roofline of the same kernel: its FP64 thread instructions (ncu count per cell) over the
+        # FP64 pipe rate measured now by the DFMA probe
+        fp64 = None
+        pk64 = fp64_pipe_peak(local)
+        if pk64 is not None:
+            per_cell = NCU_FP64_PER_CELL.get(tkey)
+            ach64 = per_cell * case.ncells / (top_ms * 1e-3) if per_cell else None
+            fp64 = {"bound": "fp64", "unit": "FP64 thread-instructions/s (one DFMA = 2 flops)",
+                    "peak": pk64["dfma_per_s"], "peak_kind": "measured (DFMA probe, this run)",
+                    "peak_how": pk64["how"], "peak_clocks": pk64["clocks"],
+                    "instructions_per_cell": per_cell, "achieved": ach64,
+                    "frac": ach64 / pk64["dfma_per_s"] if ach64 else None}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = reference_sample(steps=2, warmup=0, config=args.config)
+            cpu = reference_sample(steps=3, warmup=1, config=args.config, budget_s=60.0)
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -558,7 +627,8 @@ def main():
                          "peak_kind": peak_kind, "kernel": f"{ {'euler': 'k_euler_step', 'ptueq': 'k_ptueq_step'}.get(tkey[0], 'k_kapila_step')} ({kname})",
                          "algorithmic_bytes_per_cell": pb[top], "launch_ms": top_ms,
                          "step_bytes_per_cell_update": B,
-                         "step_frac": B * case.ncells / (step_ms * 1e-3) / 1e9 / peak},
+                         "step_frac": B * case.ncells / (step_ms * 1e-3) / 1e9 / peak,
+                         "fp64": fp64},
             "kernels_ms": {"pass1": pass_ms[0], "pass2": pass_ms[1], "update": pass_ms[2]},
             "gpu_launches": args.steps * (3 if case.second_order else 2),
             "clocks": clk.summary(),
@@ -569,7 +639,7 @@ def main():
             line["mlp_seeded"] = seeded
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "cell-updates/s", "cores": cpu["cores"],
-                                    "kind": "reference", "sample": cpu["sample"]}
+                                    "kind": "reference", "cpu": cpu["cpu"], "sample": cpu["sample"]}
         print(json.dumps(line))
     ctx.close()
     shutil.rmtree(work, ignore_errors=True)

@@ -20,6 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.environ.get("ECG_BUILD_DIR", os.path.join(HERE, "_build"))
 LIB = os.environ.get("ECG_LIB_OUT", os.path.join(HERE, "libecg.so"))
 DRIVER = os.path.join(HERE, "ecogen-b200")
+PROBE_LIB = os.path.join(HERE, "libecg_probe.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -69,6 +70,15 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    # measurement probe (FP64 pipe peak for the bench's FP64 roofline), its own library
+    probe_src = os.path.join(HERE, "probe", "ecg_fp64_peak.cu")
+    if os.path.exists(probe_src):
+        pobj = _compile(probe_src)
+        if not os.path.exists(PROBE_LIB) or os.path.getmtime(pobj) > os.path.getmtime(PROBE_LIB):
+            cmd = [_nvcc()] + ARCH + ["-shared", "-o", PROBE_LIB, pobj, "-lcudart"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     main_src = os.path.join(CSRC, "ecogen_main.cpp")
     if os.path.exists(main_src):
         mobj = _compile(main_src)
