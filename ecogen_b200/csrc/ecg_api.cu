@@ -145,6 +145,11 @@ ecg_status cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
   } while (0)
 
+}  // namespace
+
+namespace ecg {
+
+// Checks a case against what the library runs (ecg_create and ecg_step_noalloc accept the same cases).
 ecg_status validate_case(const ecg_case* c) {
   if (!c) { set_error("null case"); return ECG_ERR_INVALID; }
   if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER && c->model != ECG_MODEL_PTUEQ) { set_error("unknown model"); return ECG_ERR_INVALID; }
@@ -180,12 +185,23 @@ ecg_status validate_case(const ecg_case* c) {
       if (c->eos[k].type == ECG_EOS_NASG) { set_error("PT relaxation needs IG or SG phases"); return ECG_ERR_UNSUPPORTED; }
   }
   if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
+  if (c->ptmu) {
+    if (c->ptmu_liquid < 0 || c->ptmu_liquid > 1 || c->ptmu_vapor < 0 || c->ptmu_vapor > 1 ||
+        c->ptmu_liquid == c->ptmu_vapor) { set_error("PTMu liquid / vapour phase indices"); return ECG_ERR_INVALID; }
+    // Mixture::computeTsat (src/Models/Mixture.cpp:62-63): IG and SG phases only
+    for (int k = 0; k < 2; k++)
+      if (c->eos[k].type == ECG_EOS_NASG) { set_error("Only IG and SG permitted in thermal equilibrium model: MixPTUEq::computeTsat"); return ECG_ERR_UNSUPPORTED; }
+  }
   int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
   if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
   int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
   if (n > (int64_t)1 << 31) { set_error("more than 2^31 cells"); return ECG_ERR_TOO_LARGE; }
   return ECG_OK;
 }
+
+}  // namespace ecg
+
+namespace {
 
 // Distances of the MUSCL reconstruction per axis, with the reference's arithmetic: cell centres
 // (i + 0.5) * d, face position centre + 0.5 * d, lengths as Coord::norm of a difference

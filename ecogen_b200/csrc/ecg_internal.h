@@ -9,6 +9,10 @@ namespace ecg {
 
 void set_error(const std::string& msg);
 
+// Checks a case against what the library runs; ECG_OK, or the status and message of the first
+// violation (ecg_create and ecg_step_noalloc accept the same cases).
+ecg_status validate_case(const ecg_case* c);
+
 // Number of field pointers in the ABI layout of a case (see include/ecogen_b200.h).
 inline int abi_nfields(const ecg_case& c) {
   if (c.model == ECG_MODEL_EULER) return 6 + c.ntransports;

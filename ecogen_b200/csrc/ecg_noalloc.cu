@@ -115,31 +115,31 @@ using namespace ecg;
 
 extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in, double* state_out, double dt,
                                        double* dt_next, ecg_step_stats* stats, void* stream) {
-  if (!c || !state_in || !state_out || state_in == state_out) {
-    set_error("ecg_step_noalloc: null or aliased state buffers");
-    return ECG_ERR_INVALID;
-  }
-  if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER) {
-    set_error("unknown model");
-    return ECG_ERR_INVALID;
-  }
-  if (c->order != 1 && c->order != 2) {
-    set_error("order must be 1 or 2");
-    return ECG_ERR_INVALID;
+  // the cases ecg_create accepts, less the ones this entry point has no scratch or kernels for
+  ecg_status vs = validate_case(c);
+  if (vs != ECG_OK) return vs;
+  if (c->model == ECG_MODEL_PTUEQ) {
+    set_error("ecg_step_noalloc runs the Kapila and Euler models; use ecg_create / ecg_step for PTUEq");
+    return ECG_ERR_UNSUPPORTED;
   }
   if (c->ntransports != 0) {
     set_error("ecg_step_noalloc runs without passive transports");
     return ECG_ERR_UNSUPPORTED;
   }
-  for (int a = 0; a < 3; a++)
-    if (c->ncells[a] < 1 || !(c->length[a] > 0.)) {
-      set_error("bad mesh");
-      return ECG_ERR_INVALID;
-    }
   const int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
   if (n > kMaxCells) {
     set_error("ecg_step_noalloc: more than ECG_NOALLOC_MAX_CELLS (65536) cells; use ecg_create / ecg_step");
     return ECG_ERR_TOO_LARGE;
+  }
+  // the two states, nstate fields of n doubles each (the layout of ecg_create), must not overlap: the
+  // kernels read neighbours of the input while they write the output
+  const int dim0 = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
+  const int64_t nstate = c->model == ECG_MODEL_EULER ? 3 + dim0 : 2 * c->nphases + 2 + dim0;
+  const uintptr_t ib = reinterpret_cast<uintptr_t>(state_in), ob = reinterpret_cast<uintptr_t>(state_out);
+  const uintptr_t bytes = (uintptr_t)(nstate * n) * sizeof(double);
+  if (!state_in || !state_out || (ib < ob + bytes && ob < ib + bytes)) {
+    set_error("ecg_step_noalloc: null or overlapping state buffers");
+    return ECG_ERR_INVALID;
   }
   NoallocScratch* S = nullptr;
   ecg_status st = noalloc_scratch(&S);

@@ -182,13 +182,18 @@ ecg_status ecg_download_prim_device(ecg_ctx* ctx, double* const* dfields, int64_
  *   - state_in / state_out: device arrays in the library's device layout, fields of ncells doubles
  *     back to back: alpha_0..alpha_{N-1}, rho_0..rho_{N-1}, p, u_0..u_{dim-1}, E (Kapila) or
  *     rho, p, u_0..u_{dim-1}, E (Euler), where dim counts the axes with more than one cell; this is
- *     what ecg_upload_prim stores.  They must not alias.
+ *     what ecg_upload_prim stores.  The two ranges must not overlap (ECG_ERR_INVALID).
+ *   - The case is checked as ecg_create checks it; PTUEq cases and passive transports are refused
+ *     with ECG_ERR_UNSUPPORTED.
  *   - dt: the step to take; *dt_next (optional) receives cfl * dtMax.  stats may be NULL.
  *   - stream: a cudaStream_t (NULL = legacy default stream); the call returns after the step ran.
- *   - The first call on a device looks up the scratch's device address; make it before any stream
- *     capture.  All calls share the scratch and the last call's contents stay in it; every call
- *     re-initialises what must start at zero.  Calls that overlap on the GPU (other streams, other
- *     host threads) race on the scratch and must be serialised by the caller. */
+ *   - The first call on a device does the set-up: it looks up the scratch's device address, and with
+ *     CUDA's lazy module loading (the default) that first touch also loads the library's device code,
+ *     which is when the scratch array itself is allocated.  Make that first call before the time loop
+ *     and before any stream capture (or set CUDA_MODULE_LOADING=EAGER); later calls allocate nothing.
+ *     All calls share the scratch and the last call's contents stay in it; every call re-initialises
+ *     what must start at zero.  Calls that overlap on the GPU (other streams, other host threads)
+ *     race on the scratch and must be serialised by the caller. */
 #define ECG_NOALLOC_MAX_CELLS 65536
 ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in, double* state_out, double dt, double* dt_next,
                             ecg_step_stats* stats, void* stream);

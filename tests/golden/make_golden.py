@@ -13,6 +13,7 @@ import json
 import os
 import shutil
 import sys
+import tempfile
 
 import numpy as np
 
@@ -134,7 +135,7 @@ def case_meta(c) -> dict:
 def main():
     if not refrun.available():
         sys.exit("reference binary missing: run `make -C oracle ref` first")
-    work = os.path.join(ROOT, "_work", "runs", "golden")
+    work = tempfile.mkdtemp(prefix="ecg_golden_")
     only = set(sys.argv[1:])
     for key, c in golden_cases().items():
         if only and key not in only:
@@ -163,6 +164,7 @@ def main():
         with open(os.path.join(OUT, f"{key}.json"), "w") as fh:
             json.dump(meta, fh, indent=1)
         print(key, "iterations", it, "t", t)
+    shutil.rmtree(work, ignore_errors=True)
 
 
 def restart_case(restart_file=None):
@@ -184,8 +186,7 @@ def make_restart_golden(key="restart2d", make_case=None):
     """<key>.npz/.json: the reference's result file 2 and infoCalcul.out of a 30-iteration run, and the
     final file of the reference restarted from file 2 (Run::restartSimulation src/Run.cpp:345)."""
     make_case = make_case or restart_case
-    work = os.path.join(ROOT, "_work", "runs", "golden", key)
-    shutil.rmtree(work, ignore_errors=True)
+    work = tempfile.mkdtemp(prefix=f"ecg_golden_{key}_")
     c = make_case()
     d = c.write(work)
     cases.write_ecogen_list(work, [d])
@@ -209,6 +210,7 @@ def make_restart_golden(key="restart2d", make_case=None):
         json.dump({"info_lines": info_lines[:4], "names": [n for n, _ in src], "restart_file": 2,
                    "case": case_meta(c)}, fh, indent=1)
     print(key, info_lines[:4])
+    shutil.rmtree(work, ignore_errors=True)
 
 
 if __name__ == "__main__":
