@@ -120,15 +120,64 @@ def pass_bytes_per_cell(case) -> dict:
     return {"pass1": 16 * ns}
 
 
+# Per-kernel slots of ecg_step_profiled_kernels: pass 1 (first order or MUSCL predictor) X / Y / Z face
+# kernels and cell kernel, pass 2 (MUSCL corrector) the same, time-step update.  In fused form a
+# pass is one kernel, timed in its cell-kernel slot.
+KERNEL_SLOTS = ["pass1_faces_x", "pass1_faces_y", "pass1_faces_z", "pass1_cells",
+                "pass2_faces_x", "pass2_faces_y", "pass2_faces_z", "pass2_cells", "update"]
+
+
+def kernel_bytes_per_cell(case, form: str, slot: str) -> int:
+    """Algorithmic bytes per cell of one launch of a step kernel.
+
+    Fused form: the pass's bytes (pass_bytes_per_cell).  Split form, face kernel of one axis: read the
+    pass's input state (NS - 1 fields; the corrector also the time-n alpha_0), write one flux
+    (3N + d + 3 doubles) per face; cell kernel: read the d faces' fluxes per cell, S^n (NS), write the
+    output state (NS, the predictor NS - 1)."""
+    ns = state_fields(case)
+    pb = pass_bytes_per_cell(case)
+    if form != "split" or case.dim < 2:
+        return pb["pass2" if slot.startswith("pass2") else "pass1"]
+    nfl = 3 * case.nphases + case.dim + 3
+    corr = slot.startswith("pass2")
+    pred = slot.startswith("pass1") and case.second_order
+    if "_faces_" in slot:
+        return 8 * ((ns - 1) + (1 if corr else 0) + nfl)
+    return 8 * (case.dim * nfl + ns + (ns - 1 if pred else ns))
+
+
+def kernel_label(case, form: str, slot: str) -> str:
+    euler, ptueq = case.model.upper() == "EULER", getattr(case, "ptueq", False)
+    base = "k_euler_step" if euler else ("k_ptueq_step" if ptueq else "k_kapila_step")
+    pas = ("MUSCL corrector" if slot.startswith("pass2") else
+           ("MUSCL predictor" if case.second_order else "first-order step"))
+    if form == "split" and case.dim >= 2 and not euler and not ptueq:
+        if "_faces_" in slot:
+            return f"k_kapila_faces, {slot[-1].upper()} faces ({pas})"
+        return f"k_kapila_cells ({pas})"
+    return f"{base} ({pas})"
+
+
+def launches_per_step(case, form: str) -> int:
+    passes = 2 if case.second_order else 1
+    per_pass = (case.dim + 1) if (form == "split" and case.dim >= 2) else 1
+    return passes * per_pass + 1
+
+
 # DRAM bytes per cell of the step kernels measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / cells: 2D two-phase MUSCL at 1536^2, 3D three-phase MUSCL at 128^3, 2D PTUEq MUSCL at
 # 1536^2, 2D p-T-mu at 1536^2, 2D Euler at 2048^2).  The kernels stream the state once, so traffic
 # scales with the cell count.
-NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "pass2"): 190.96, ("kapila", 2, 2, True, "pass1"): 125.14,
-                        ("kapila", 3, 3, True, "pass2"): 250.27, ("kapila", 3, 3, True, "pass1"): 155.89,
-                        ("ptueq", 2, 2, True, "pass2"): 150.78, ("ptueq", 2, 2, True, "pass1"): 91.56,
-                        ("kapila_ptmu", 2, 2, True, "pass2"): 181.05, ("kapila_ptmu", 2, 2, True, "pass1"): 112.08,
-                        ("euler", 1, 2, True, "pass2"): 98.52, ("euler", 1, 2, True, "pass1"): 64.92}
+NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "fused", "pass2_cells"): 190.96,
+                        ("kapila", 2, 2, True, "fused", "pass1_cells"): 125.14,
+                        ("kapila", 3, 3, True, "fused", "pass2_cells"): 250.27,
+                        ("kapila", 3, 3, True, "fused", "pass1_cells"): 155.89,
+                        ("ptueq", 2, 2, True, "fused", "pass2_cells"): 150.78,
+                        ("ptueq", 2, 2, True, "fused", "pass1_cells"): 91.56,
+                        ("kapila_ptmu", 2, 2, True, "fused", "pass2_cells"): 181.05,
+                        ("kapila_ptmu", 2, 2, True, "fused", "pass1_cells"): 112.08,
+                        ("euler", 1, 2, True, "fused", "pass2_cells"): 98.52,
+                        ("euler", 1, 2, True, "fused", "pass1_cells"): 64.92}
 # Batched tubes (2048 cases): predictor + corrector DRAM bytes per cell-update.
 NCU_BATCH_BYTES_PER_CELL_UPDATE = 98.05 + 157.17
 
@@ -441,6 +490,8 @@ def main():
     ap.add_argument("--no-seeded", action="store_true", help="skip the learned-seed measurement")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="default", choices=["default", "split", "fused"],
+                    help="form of the 2D / 3D Kapila passes (ecg_set_step_form); default: the library's")
     args = ap.parse_args()
     rank, world, local = env_rank()
     case = make_case(args.config, args.size)
@@ -492,7 +543,14 @@ def main():
     d = case.write(work)
     inp = api.Input(d, os.path.join(work, "libEOS"))
     fields0 = inp.fill()
-    ctx = api.Context(inp.case)
+
+    def new_context():
+        c = api.Context(inp.case)
+        if args.form != "default":
+            c.set_step_form(api.FORM_SPLIT if args.form == "split" else api.FORM_FUSED)
+        return c
+
+    ctx = new_context()
     ctx.upload(fields0)
     ctx.step(args.warmup)
     stream = torch.cuda.ExternalStream(api.lib().ecg_stream(ctx.h))
@@ -518,9 +576,9 @@ def main():
     if not args.no_seeded and os.path.exists(model_path) and not case.ptueq:  # PTUEq has no relaxation to seed
         from ecogen_b200 import seed as seedmod
         model = seedmod.SeedModel.load(model_path)
-        ref_ctx = api.Context(inp.case)
+        ref_ctx = new_context()
         ref_ctx.upload(fields0)
-        ctx3 = api.Context(inp.case)
+        ctx3 = new_context()
         ctx3.upload(fields0)
         model.install(ctx3)
         ref_ctx.step(args.warmup)
@@ -546,10 +604,11 @@ def main():
         ctx3.close()
 
     # ---- per-kernel attribution (separate launches, events between kernels)
-    st_p, kms = ctx.step_profiled(max(2, min(args.steps, 10)))
     nprof = max(2, min(args.steps, 10))
+    st_p, kms = ctx.step_profiled_kernels(nprof)
     step_ms = sum(kms) / nprof
-    pass_ms = [k / nprof for k in kms]
+    kernel_ms = {name: v / nprof for name, v in zip(KERNEL_SLOTS, kms) if v > 0.0}
+    form = "split" if ctx.step_form == api.FORM_SPLIT else "fused"
 
     # ---- end to end through the C ABI with host buffers: upload from pinned host memory, one
     #      ecg_step call per step (host -> device dt/t, device -> host dt/t/counters), download
@@ -558,7 +617,7 @@ def main():
     pinned_out = [torch.empty(case.ncells, dtype=torch.float64).pin_memory() for _ in range(nf)]
     in_np = [p.numpy() for p in pinned_in]
     out_np = [p.numpy() for p in pinned_out]
-    ctx2 = api.Context(inp.case)
+    ctx2 = new_context()
     ctx2.upload(in_np)
     ctx2.step(args.warmup)
     torch.cuda.synchronize()
@@ -584,18 +643,16 @@ def main():
     if rank == 0:
         peak, peak_kind = measured_peak()
         B = bytes_per_cell_update(case)
-        pb = pass_bytes_per_cell(case)
-        top = max(pb, key=lambda k: pass_ms[0 if k == "pass1" else 1])
-        top_ms = pass_ms[0 if top == "pass1" else 1]
-        achieved = pb[top] * case.ncells / (top_ms * 1e-3) / 1e9
+        top = max((k for k in kernel_ms if k != "update"), key=lambda k: kernel_ms[k])
+        top_ms = kernel_ms[top]
+        top_bytes = kernel_bytes_per_cell(case, form, top)
+        achieved = top_bytes * case.ncells / (top_ms * 1e-3) / 1e9
         model_key = "euler" if case.model.upper() == "EULER" else ("ptueq" if case.ptueq else "kapila")
         if model_key == "kapila" and case.ptmu is not None:
             model_key = "kapila_ptmu"
-        tkey = (model_key, case.nphases, case.dim,
-                bool(case.second_order), top)
+        tkey = (model_key, case.nphases, case.dim, bool(case.second_order), form, top)
         traffic = NCU_TRAFFIC_PER_CELL.get(tkey)
-        kname = {"pass1": "MUSCL predictor" if case.second_order else "first-order step",
-                 "pass2": "MUSCL corrector"}[top]
+        kname = kernel_label(case, form, top)
         # FP64 roofline of the same kernel: its FP64 thread instructions (ncu count per cell) over the
         # FP64 pipe rate measured now by the DFMA probe
         fp64 = None
@@ -624,13 +681,13 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": traffic * case.ncells if traffic is not None else None,
-                         "peak_kind": peak_kind, "kernel": f"{ {'euler': 'k_euler_step', 'ptueq': 'k_ptueq_step'}.get(tkey[0], 'k_kapila_step')} ({kname})",
-                         "algorithmic_bytes_per_cell": pb[top], "launch_ms": top_ms,
+                         "peak_kind": peak_kind, "kernel": kname, "form": form,
+                         "algorithmic_bytes_per_cell": top_bytes, "launch_ms": top_ms,
                          "step_bytes_per_cell_update": B,
                          "step_frac": B * case.ncells / (step_ms * 1e-3) / 1e9 / peak,
                          "fp64": fp64},
-            "kernels_ms": {"pass1": pass_ms[0], "pass2": pass_ms[1], "update": pass_ms[2]},
-            "gpu_launches": args.steps * (3 if case.second_order else 2),
+            "kernels_ms": kernel_ms,
+            "gpu_launches": args.steps * launches_per_step(case, form),
             "clocks": clk.summary(),
             "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max,
                        "fallback": st.newton_fallback, "hist": list(st.newton_hist)},

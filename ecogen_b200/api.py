@@ -18,6 +18,7 @@ ECG_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported case", 3: "CUDA error", 4: "case input error",
           5: "physics check failed", 6: "out of memory", 7: "size above the stated maximum", 8: "device wait timed out"}
 MODEL_KAPILA, MODEL_EULER, MODEL_PTUEQ = 0, 1, 2
+FORM_FUSED, FORM_SPLIT = 0, 1
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
@@ -99,6 +100,10 @@ def lib():
     L.ecg_step.argtypes = [vp, C.c_int32, dp, dp, P(StepStats)]
     L.ecg_run.argtypes = [vp, dp, dp, P(C.c_int32), P(StepStats)]
     L.ecg_step_profiled.argtypes = [vp, C.c_int32, dp, dp, P(StepStats), dp]
+    L.ecg_step_profiled_kernels.argtypes = [vp, C.c_int32, dp, dp, P(StepStats), dp]
+    L.ecg_set_step_form.argtypes = [vp, C.c_int32]
+    L.ecg_step_form.restype = C.c_int32
+    L.ecg_step_form.argtypes = [vp]
     L.ecg_step_noalloc.argtypes = [P(Case), vp, vp, C.c_double, dp, P(StepStats), vp]
     L.ecg_ncells.restype = C.c_int64
     L.ecg_ncells.argtypes = [vp]
@@ -281,6 +286,24 @@ class Context:
               "ecg_step_profiled")
         self.iteration += nsteps
         return st, list(ms)
+
+    def step_profiled_kernels(self, nsteps: int = 1):
+        """Steps with every kernel timed separately: (stats, 9 times in ms) -- pass 1 X / Y / Z face
+        kernels and cell kernel, pass 2 the same, update (ecg_step_profiled_kernels)."""
+        st = StepStats()
+        ms = (C.c_double * 9)(*([0.0] * 9))
+        check(lib().ecg_step_profiled_kernels(self.h, nsteps, C.byref(self.dt), C.byref(self.t), C.byref(st), ms),
+              "ecg_step_profiled_kernels")
+        self.iteration += nsteps
+        return st, list(ms)
+
+    def set_step_form(self, form: int):
+        """FORM_FUSED or FORM_SPLIT (ecg_set_step_form)."""
+        check(lib().ecg_set_step_form(self.h, form), "ecg_set_step_form")
+
+    @property
+    def step_form(self) -> int:
+        return int(lib().ecg_step_form(self.h))
 
     def run(self) -> StepStats:
         st = StepStats()

@@ -113,6 +113,8 @@ struct ecg_ctx {
   double* half = nullptr;     // MUSCL half-step primitives
   double* dist = nullptr;     // distance tables (3 axes x 3 tables)
   double* tmp = nullptr;      // download scratch (mixture pressure)
+  double* flux[3] = {nullptr, nullptr, nullptr};  // face arrays of the split form (Kapila 2D / 3D)
+  bool split = false;         // step passes in split form (face kernels + cell kernel)
   DevScalars* scal = nullptr;
   DevStats* stats = nullptr;
   // pinned host staging of the scalars and counters an ecg_step call exchanges (asynchronous copies,
@@ -243,6 +245,7 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.ptmu_liq = x->c.ptmu_liquid;
   P.ptmu_vap = x->c.ptmu_vapor;
   P.pcrit = x->pcrit;
+  for (int a = 0; a < 3; a++) P.flux[a] = x->split ? x->flux[a] : nullptr;
   double* sn = x->state[parity];
   double* s1 = x->state[1 - parity];
   const bool euler = x->c.model == ECG_MODEL_EULER;
@@ -258,6 +261,7 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
     P.q = sn;
     P.sn = sn;
     P.out = s1;
+    P.split_ev = (ev && x->split) ? ev + 4 : nullptr;
     e = run(PASS_O1);
     if (e != cudaSuccess) return cuda_fail(e, "step kernel");
     if (ev) cudaEventRecord(ev[1], x->stream);
@@ -265,11 +269,13 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
     P.q = sn;
     P.sn = sn;
     P.out = x->half;
+    P.split_ev = (ev && x->split) ? ev + 4 : nullptr;  // after each axis' face kernel (profiling)
     e = run(PASS_PRED);
     if (e != cudaSuccess) return cuda_fail(e, "predictor kernel");
     if (ev) cudaEventRecord(ev[1], x->stream);
     P.q = x->half;
     P.out = s1;
+    P.split_ev = (ev && x->split) ? ev + 7 : nullptr;
     e = run(PASS_CORR);
     if (e != cudaSuccess) return cuda_fail(e, "corrector kernel");
   }
@@ -481,6 +487,16 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
   }
   e = cudaMalloc(&x->tmp, sizeof(double) * (size_t)(ptueq ? 2 : 1) * (size_t)x->n);  // download scratch
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(tmp)"));
+  if (!euler && !ptueq && x->dim >= 2 && c->ntransports == 0) {
+    // face arrays of the split form: 3N + d + 3 flux components per face, faces of each axis including
+    // the domain sides
+    const int nfl = 3 * x->np + x->dim + 3;
+    for (int a = 0; a < x->dim; a++) {
+      e = cudaMalloc(&x->flux[a], sizeof(double) * (size_t)nfl * (size_t)split_nfaces(c->ncells, a));
+      if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(face fluxes)"));
+    }
+    x->split = true;
+  }
   std::vector<double> h;
   distance_tables(*c, h);
   e = cudaMalloc(&x->dist, sizeof(double) * h.size());
@@ -559,6 +575,7 @@ extern "C" void ecg_destroy(ecg_ctx* x) {
   cudaFree(x->half);
   cudaFree(x->dist);
   cudaFree(x->tmp);
+  for (int a = 0; a < 3; a++) cudaFree(x->flux[a]);
   cudaFree(x->scal);
   cudaFree(x->stats);
   cudaFreeHost(x->h_scal);
@@ -573,6 +590,16 @@ extern "C" void ecg_destroy(ecg_ctx* x) {
 
 extern "C" int64_t ecg_ncells(const ecg_ctx* x) { return x ? x->n : 0; }
 extern "C" void* ecg_stream(const ecg_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+extern "C" ecg_status ecg_set_step_form(ecg_ctx* x, int32_t form) {
+  if (!x || (form != ECG_FORM_FUSED && form != ECG_FORM_SPLIT)) { set_error("bad step form"); return ECG_ERR_INVALID; }
+  if (form == ECG_FORM_SPLIT && !x->flux[0]) { set_error("no split form for this case (1D, Euler, PTUEq or transports)"); return ECG_ERR_UNSUPPORTED; }
+  x->split = form == ECG_FORM_SPLIT;
+  x->graph_dirty = true;
+  return ECG_OK;
+}
+
+extern "C" int32_t ecg_step_form(const ecg_ctx* x) { return (x && x->split) ? ECG_FORM_SPLIT : ECG_FORM_FUSED; }
 
 extern "C" ecg_status ecg_set_newton_cap(ecg_ctx* x, int32_t cap) {
   if (!x || cap < 1 || cap > 100000) { set_error("bad Newton cap"); return ECG_ERR_INVALID; }
@@ -737,8 +764,11 @@ extern "C" ecg_status ecg_download_derived(ecg_ctx* x, double* T, double* Y, int
   return ECG_OK;
 }
 
+// kernel_ms (profiled steps, every kernel launched separately): with nms = 3 the pass-1, pass-2 and
+// update times; with nms = 9 per kernel: pass 1 X, Y, Z face kernels and cell kernel (the whole pass
+// in fused form), pass 2 the same, update.
 static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, double* t, int32_t* iterations,
-                              ecg_step_stats* stats, double* kernel_ms = nullptr) {
+                              ecg_step_stats* stats, double* kernel_ms = nullptr, int nms = 3) {
   // host values of dt and t seed the device scalars (the caller owns the time loop state)
   DevScalars h{};
   h.dt = *dt;
@@ -758,22 +788,44 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
                             // holds the result is decided by the number of steps actually taken
   int64_t done_steps = 0;
   if (kernel_ms) {
-    cudaEvent_t ev[4];
-    for (int i = 0; i < 4; i++) ECG_CUDA(cudaEventCreate(&ev[i]));
+    // ev[0..3]: step start, after pass 1, after pass 2, after the update; ev[4..6] / ev[7..9]: after
+    // the X, Y, Z face kernels of pass 1 / pass 2 (split form)
+    cudaEvent_t ev[10];
+    for (int i = 0; i < 10; i++) ECG_CUDA(cudaEventCreate(&ev[i]));
+    auto ms = [&](int a, int b) {
+      float v = 0.f;
+      cudaEventElapsedTime(&v, ev[a], ev[b]);
+      return (double)v;
+    };
+    const bool two = x->c.order == 2;
     for (int i = 0; i < nsteps; i++) {
       ecg_status s = launch_step(x, x->cur, ev);
       if (s != ECG_OK) return s;
       x->cur = 1 - x->cur;
       ECG_CUDA(cudaEventSynchronize(ev[3]));
-      float a = 0.f, b = 0.f, c = 0.f;
-      cudaEventElapsedTime(&a, ev[0], ev[1]);
-      cudaEventElapsedTime(&b, ev[1], ev[2]);
-      cudaEventElapsedTime(&c, ev[2], ev[3]);
-      kernel_ms[0] += a;
-      kernel_ms[1] += b;
-      kernel_ms[2] += c;
+      if (nms < 9) {
+        kernel_ms[0] += ms(0, 1);
+        kernel_ms[1] += ms(1, 2);
+        kernel_ms[2] += ms(2, 3);
+        continue;
+      }
+      for (int pass = 0; pass < (two ? 2 : 1); pass++) {
+        const int start = pass == 0 ? 0 : 1, end = pass == 0 ? 1 : 2, base = pass == 0 ? 4 : 7;
+        double* o = kernel_ms + 4 * pass;
+        if (x->split) {
+          int prev = start;
+          for (int a = 0; a < x->dim; a++) {
+            o[a] += ms(prev, base + a);
+            prev = base + a;
+          }
+          o[3] += ms(prev, end);
+        } else {
+          o[3] += ms(start, end);
+        }
+      }
+      kernel_ms[8] += ms(2, 3);
     }
-    for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 10; i++) cudaEventDestroy(ev[i]);
   } else if (mode == 0) {
     ecg_status s = advance(x, nsteps);
     if (s != ECG_OK) return s;
@@ -815,7 +867,13 @@ extern "C" ecg_status ecg_step(ecg_ctx* x, int32_t nsteps, double* dt, double* t
 extern "C" ecg_status ecg_step_profiled(ecg_ctx* x, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats,
                                         double* kernel_ms) {
   if (!x || !dt || !t || nsteps < 0 || !kernel_ms) { set_error("bad argument"); return ECG_ERR_INVALID; }
-  return step_common(x, 0, nsteps, dt, t, nullptr, stats, kernel_ms);
+  return step_common(x, 0, nsteps, dt, t, nullptr, stats, kernel_ms, 3);
+}
+
+extern "C" ecg_status ecg_step_profiled_kernels(ecg_ctx* x, int32_t nsteps, double* dt, double* t,
+                                                ecg_step_stats* stats, double* kernel_ms) {
+  if (!x || !dt || !t || nsteps < 0 || !kernel_ms) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  return step_common(x, 0, nsteps, dt, t, nullptr, stats, kernel_ms, 9);
 }
 
 extern "C" ecg_status ecg_run(ecg_ctx* x, double* dt, double* t, int32_t* iterations, ecg_step_stats* stats) {

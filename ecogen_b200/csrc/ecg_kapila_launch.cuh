@@ -1,7 +1,7 @@
 // Launch templates of the Kapila step kernels; explicit instantiations live in ecg_kapila_*.cu so
 // that the (large) kernel variants compile in parallel.
 #pragma once
-#include "ecg_kapila_kernel.cuh"
+#include "ecg_kapila_split.cuh"
 
 namespace ecg {
 
@@ -25,13 +25,29 @@ cudaError_t launch_one(const StepParams& P, const Geometry& G, const ecg_eos* eo
   return cudaGetLastError();
 }
 
+// One pass of one kernel variant: the split form (face kernels + cell kernel) for 2D and 3D cases whose
+// context holds face arrays, the fused kernel otherwise (1D, passive transports, the allocation-free
+// entry point).  With prepare both forms are configured.
+template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES, int NTM>
+cudaError_t launch_form(const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps, cudaStream_t s,
+                        bool prepare) {
+  constexpr bool kSplit = DIM >= 2 && NTM == 0;
+  if (prepare) {
+    cudaError_t e = launch_one<NP, DIM, PASS, PTMU, SEED, TYPES, NTM>(P, G, eos, eps, s, true);
+    if (kSplit && e == cudaSuccess) e = launch_split<NP, DIM, PASS, PTMU, SEED, TYPES>(P, G, eos, eps, s, true);
+    return e;
+  }
+  if (kSplit && P.flux[0] != nullptr) return launch_split<NP, DIM, PASS, PTMU, SEED, TYPES>(P, G, eos, eps, s, false);
+  return launch_one<NP, DIM, PASS, PTMU, SEED, TYPES, NTM>(P, G, eos, eps, s, false);
+}
+
 template <int NP, int DIM, bool PTMU, bool SEED, int TYPES = EOS_DYNAMIC, int NTM = 0>
 cudaError_t launch_pass_seed(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
                              cudaStream_t s, bool prepare) {
   switch (pass) {
-    case PASS_O1: return launch_one<NP, DIM, PASS_O1, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
-    case PASS_PRED: return launch_one<NP, DIM, PASS_PRED, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
-    default: return launch_one<NP, DIM, PASS_CORR, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    case PASS_O1: return launch_form<NP, DIM, PASS_O1, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    case PASS_PRED: return launch_form<NP, DIM, PASS_PRED, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    default: return launch_form<NP, DIM, PASS_CORR, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
   }
 }
 

@@ -132,6 +132,10 @@ struct StepParams {
   int ntr;
   // analytic pressure-temperature relaxation after the pressure one (two phases)
   int pt;
+  // split form of a 2D / 3D pass (ecg_kapila_split.cuh): face-flux arrays per axis (nullptr: the fused
+  // kernels run), and optional events recorded after each axis' face kernel (profiling)
+  double* flux[3];
+  cudaEvent_t* split_ev;
 };
 
 // Host side of the THINC parameters (CellInterfaceO2Cartesian::solveRiemann's beta = 1.6).
@@ -139,6 +143,12 @@ inline void set_thinc(StepParams& P, const ecg_case& c) {
   P.thinc = (c.order == 2 && (c.limiter[2] == ECG_LIM_THINC || c.limiter[3] == ECG_LIM_THINC)) ? 1 : 0;
   P.thinc_cosh = std::cosh(1.6);
   P.thinc_tanh = std::tanh(1.6);
+}
+
+// Faces normal to axis ax of a mesh of n cells per axis, the two domain sides of every line included
+// (the face arrays of the split form).
+__host__ __device__ inline int64_t split_nfaces(const int n[3], int ax) {
+  return (int64_t)(n[0] + (ax == 0)) * (n[1] + (ax == 1)) * (n[2] + (ax == 2));
 }
 
 __device__ __forceinline__ void atomic_min_pos_double(unsigned long long* addr, double v) {

@@ -158,6 +158,20 @@ ecg_status ecg_step(ecg_ctx* ctx, int32_t nsteps, double* dt, double* t, ecg_ste
  * [0] first-order or MUSCL predictor pass, [1] MUSCL corrector pass, [2] time-step update. */
 ecg_status ecg_step_profiled(ecg_ctx* ctx, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats,
                              double* kernel_ms);
+/* The same per kernel, kernel_ms[0..8]: pass 1's X, Y and Z face kernels and its cell kernel, pass 2's
+ * (MUSCL corrector) the same, then the time-step update.  In fused form a pass is one kernel, whose
+ * time goes to its cell-kernel slot ([3] or [7]); entries of kernels that do not run stay 0. */
+ecg_status ecg_step_profiled_kernels(ecg_ctx* ctx, int32_t nsteps, double* dt, double* t, ecg_step_stats* stats,
+                                     double* kernel_ms);
+/* Form of the Kapila step passes on 2D and 3D meshes.  ECG_FORM_SPLIT (the default where it applies):
+ * per axis a face-flux kernel writing every face's flux to a face array of the context, then one cell
+ * kernel accumulating them in the reference's face order; ECG_FORM_FUSED: one kernel per pass that
+ * stages a tile per axis in shared memory.  Both compute every flux with the same arithmetic and
+ * accumulate in the same order, so they give the same bits.  1D cases, passive transports and the Euler
+ * and PTUEq models run fused only (ECG_ERR_UNSUPPORTED for ECG_FORM_SPLIT). */
+enum { ECG_FORM_FUSED = 0, ECG_FORM_SPLIT = 1 };
+ecg_status ecg_set_step_form(ecg_ctx* ctx, int32_t form);
+int32_t ecg_step_form(const ecg_ctx* ctx);
 /* Runs the reference time loop to its stop condition (iterations or total time), in chunks
  * captured as CUDA graphs. */
 ecg_status ecg_run(ecg_ctx* ctx, double* dt, double* t, int32_t* iterations, ecg_step_stats* stats);
