@@ -691,6 +691,10 @@ def main():
             "clocks": clk.summary(),
             "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max,
                        "fallback": st.newton_fallback, "hist": list(st.newton_hist)},
+            "ptmu": ({"solves": st.ptmu_solves, "outer_iters": st.ptmu_outer_iters, "outer_max": st.ptmu_outer_max,
+                      "outer_hist": list(st.ptmu_outer_hist), "tsat_calls": st.ptmu_tsat_calls,
+                      "tsat_iters": st.ptmu_tsat_iters, "tsat_max": st.ptmu_tsat_max}
+                     if case.ptmu is not None else None),
         }
         if seeded is not None:
             line["mlp_seeded"] = seeded

@@ -48,11 +48,14 @@ class StepStats(C.Structure):
     _fields_ = [("cell_updates", C.c_int64), ("relax_calls", C.c_int64), ("newton_evals", C.c_int64),
                 ("newton_fallback", C.c_int64), ("newton_max", C.c_int64), ("seeded", C.c_int64),
                 ("seed_rejected", C.c_int64), ("ptmu_errors", C.c_int64), ("nonfinite_cells", C.c_int64),
-                ("newton_hist", C.c_int64 * 16)]
+                ("newton_hist", C.c_int64 * 16), ("ptmu_solves", C.c_int64), ("ptmu_outer_iters", C.c_int64),
+                ("ptmu_outer_max", C.c_int64), ("ptmu_tsat_calls", C.c_int64), ("ptmu_tsat_iters", C.c_int64),
+                ("ptmu_tsat_max", C.c_int64), ("ptmu_outer_hist", C.c_int64 * 16)]
 
     def as_dict(self) -> Dict[str, object]:
-        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "newton_hist"}
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("newton_hist", "ptmu_outer_hist")}
         d["newton_hist"] = list(self.newton_hist)
+        d["ptmu_outer_hist"] = list(self.ptmu_outer_hist)
         return d
 
 

@@ -332,6 +332,9 @@ ecg_status advance(ecg_ctx* x, int nsteps) {
   return ECG_OK;
 }
 
+}  // namespace
+
+namespace ecg {
 void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
   std::memset(st, 0, sizeof(*st));
   st->cell_updates = updates;
@@ -344,7 +347,17 @@ void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
   st->ptmu_errors = (int64_t)d.ptmu_errors;
   st->nonfinite_cells = (int64_t)d.nonfinite;
   for (int i = 0; i < 16; i++) st->newton_hist[i] = (int64_t)d.hist[i];
+  st->ptmu_solves = (int64_t)d.ptmu_solves;
+  st->ptmu_outer_iters = (int64_t)d.ptmu_outer;
+  st->ptmu_outer_max = (int64_t)d.ptmu_outer_max;
+  st->ptmu_tsat_calls = (int64_t)d.ptmu_tsat_calls;
+  st->ptmu_tsat_iters = (int64_t)d.ptmu_tsat_iters;
+  st->ptmu_tsat_max = (int64_t)d.ptmu_tsat_max;
+  for (int i = 0; i < 16; i++) st->ptmu_outer_hist[i] = (int64_t)d.ptmu_hist[i];
 }
+}  // namespace ecg
+
+namespace {
 
 }  // namespace
 

@@ -593,9 +593,18 @@ __device__ __forceinline__ void pinf_finish(const Model<NP>& M, double a[NP], do
   pstar = pI;
 }
 
+// Iteration counts of one p-T-mu relaxation (diagnostics; they do not change the arithmetic).
+struct PtmuCount {
+  unsigned int solve = 0;      // 1 when the saturation Newton on p* ran
+  unsigned int outer = 0;      // its iterations
+  unsigned int tsat_calls = 0;  // T_sat(p) solves (pure-phase tests included)
+  unsigned int tsat_iters = 0;  // their Newton iterations
+  unsigned int tsat_max = 0;    // the largest of them
+};
+
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
 __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
-                                               bool& err) {
+                                               bool& err, PtmuCount* pc = nullptr) {
   double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
   double gV = V.gamma, piV = (V.type == ECG_EOS_IG) ? 0. : V.pinf, cvV = V.cv, e0V = V.eref, s0V = V.sref;
   double A = (gL * cvL - gV * cvV + s0V - s0L) / (gV * cvV - cvV);
@@ -604,6 +613,9 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
   double D = (gL * cvL - cvL) / (gV * cvV - cvV);
   int iteration = 0;
   double Tsat = 0.1 * B / C, f = 0., df = 1.;
+  // ln(p + pInf) of both phases do not depend on the iterate: evaluated once per solve (the same
+  // values enter the same sum, so f has the bits of the reference's per-iteration evaluation)
+  const double lnV = cr_log(p + piV), lnL = cr_log(p + piL);
   do {
     Tsat -= f / df;
     iteration++;
@@ -611,9 +623,14 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
       err = true;
       break;
     }
-    f = A + B / Tsat + C * cr_log(Tsat) - cr_log(p + piV) + D * cr_log(p + piL);
+    f = A + B / Tsat + C * cr_log(Tsat) - lnV + D * lnL;
     df = C / Tsat - B / (Tsat * Tsat);
   } while (fabs(f) > 1e-10);
+  if (pc) {
+    pc->tsat_calls++;
+    pc->tsat_iters += (unsigned int)iteration;
+    pc->tsat_max = max(pc->tsat_max, (unsigned int)iteration);
+  }
   double dfdp = -1. / (p + piV) + D / (p + piL);
   *dTsat = -dfdp / df;
   return Tsat;
@@ -651,7 +668,8 @@ __device__ __forceinline__ double eos_rhoe_sat(const EosParams& q, double p, dou
 // is recomputed from the new phases).
 template <int NP>
 __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap, double pcrit, double a[NP],
-                                           double r[NP], double p[NP], double rhomix, double emix, bool& err) {
+                                           double r[NP], double p[NP], double rhomix, double emix, bool& err,
+                                           PtmuCount* pc = nullptr) {
   const EosParams& EL = M.eos[liq];
   const EosParams& EV = M.eos[vap];
   double pStar = 0., Tsat, dTsat = 0.;
@@ -662,7 +680,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pv = eos_p(EV, M.eps, rho, emix);
   double Tv = eos_T(EV, M.eps, rho, pv);
   if (pv > 0) {
-    Tsat = compute_tsat(EL, EV, pv, &dTsat, err);
+    Tsat = compute_tsat(EL, EV, pv, &dTsat, err, pc);
     if (Tv >= Tsat) {
       a[vap] = 1.;
       a[liq] = 0.;
@@ -674,7 +692,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pl = eos_p(EL, M.eps, rho, emix);
   double Tl = eos_T(EL, M.eps, rho, pl);
   if (pl > 0.) {
-    Tsat = compute_tsat(EL, EV, pl, &dTsat, err);
+    Tsat = compute_tsat(EL, EV, pl, &dTsat, err, pc);
     if (Tl <= Tsat) {
       a[liq] = 1.;
       a[vap] = 0.;
@@ -696,7 +714,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
     }
 #pragma unroll
     for (int k = 0; k < NP; k++) pStar = eos_fix_p(M.eos[k], pStar);
-    Tsat = compute_tsat(EL, EV, pStar, &dTsat, err);
+    Tsat = compute_tsat(EL, EV, pStar, &dTsat, err, pc);
     rhoLSat = eos_rho_sat(EL, M.eps, pStar, Tsat, dTsat, &drhoLSat);
     rhoVSat = eos_rho_sat(EV, M.eps, pStar, Tsat, dTsat, &drhoVSat);
     aLSat = (rho - rhoVSat) / (rhoLSat - rhoVSat);
@@ -713,6 +731,10 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
     f /= rhoe;
     df /= rhoe;
   } while (fabs(f) > 1e-10);
+  if (pc) {
+    pc->solve = 1;
+    pc->outer = (unsigned int)iteration;
+  }
   a[liq] = aLSat;
   r[liq] = rhoLSat;
   p[liq] = pStar;

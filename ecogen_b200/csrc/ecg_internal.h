@@ -13,6 +13,10 @@ void set_error(const std::string& msg);
 // violation (ecg_create and ecg_step_noalloc accept the same cases).
 ecg_status validate_case(const ecg_case* c);
 
+struct DevStats;
+// Host copy of the device counters of a step call -> the ABI record (cell_updates = updates).
+void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st);
+
 // Number of field pointers in the ABI layout of a case (see include/ecogen_b200.h).
 inline int abi_nfields(const ecg_case& c) {
   if (c.model == ECG_MODEL_EULER) return 6 + c.ntransports;

@@ -9,6 +9,7 @@ namespace ecg {
 
 struct CellCounters {
   unsigned int relax = 0, iters = 0, fallback = 0, seeded = 0, rejected = 0, nonfinite = 0, ptmu = 0;
+  PtmuCount pc;  // p-T-mu iteration counts (kernels with p-T-mu relaxation)
 };
 
 // Reconstructs one side of an internal face (CellInterfaceO2Cartesian::solveRiemann
@@ -451,7 +452,7 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
       emix += Y * eos_e(M.eos[k], M.eps, r0[k], p0[k]);
     }
     bool err = false;
-    if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err)) {
+    if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err, &cc.pc)) {
       rhomix = 0.;
 #pragma unroll
       for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];

@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_
   if (SEED) seed_gate<NP, DIM>(P, M, active, cp, sg);
   if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
+  if (PTMU) block_ptmu_counters(P.stats, cc.pc.solve, cc.pc.outer, cc.pc.tsat_calls, cc.pc.tsat_iters, cc.pc.tsat_max);
 }
 
 template <int NP, int DIM, int AX, int PASS, int TYPES>

@@ -242,17 +242,7 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
     return ECG_ERR_CUDA;
   }
   if (dt_next) *dt_next = r.dt;
-  if (stats) {
-    std::memset(stats, 0, sizeof(*stats));
-    stats->cell_updates = n;
-    stats->relax_calls = (int64_t)ds.relax_calls;
-    stats->newton_evals = (int64_t)ds.newton_evals;
-    stats->newton_fallback = (int64_t)ds.newton_fallback;
-    stats->newton_max = (int64_t)ds.newton_max;
-    stats->ptmu_errors = (int64_t)ds.ptmu_errors;
-    stats->nonfinite_cells = (int64_t)ds.nonfinite;
-    for (int i = 0; i < 16; i++) stats->newton_hist[i] = (int64_t)ds.hist[i];
-  }
+  if (stats) stats_out(ds, n, stats);
   if (ds.ptmu_errors) {
     set_error("p-T-mu relaxation exceeded 50 iterations");
     return ECG_ERR_PHYSICS;

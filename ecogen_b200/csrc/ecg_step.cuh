@@ -195,4 +195,41 @@ __device__ __forceinline__ void block_counters(DevStats* st, unsigned int relax,
   }
 }
 
+// Reduces the p-T-mu iteration counts of a block (kernels with p-T-mu relaxation only) and adds them to
+// the device counters, one global atomic per counter and block.  Every thread of the block must call it.
+__device__ __forceinline__ void block_ptmu_counters(DevStats* st, unsigned int solve, unsigned int outer,
+                                                    unsigned int tsat_calls, unsigned int tsat_iters,
+                                                    unsigned int tsat_max) {
+  __shared__ unsigned int sp[22];
+  const int tid = threadIdx.x;
+  if (tid < 22) sp[tid] = 0u;
+  __syncthreads();
+  const unsigned full = 0xffffffffu;
+  const unsigned int v[4] = {solve, outer, tsat_calls, tsat_iters};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const unsigned int w = __reduce_add_sync(full, v[i]);
+    if ((tid & 31) == 0 && w) atomicAdd(&sp[i], w);
+  }
+  const unsigned int mo = __reduce_max_sync(full, solve ? outer : 0u), mt = __reduce_max_sync(full, tsat_max);
+  if ((tid & 31) == 0) {
+    if (mo) atomicMax(&sp[4], mo);
+    if (mt) atomicMax(&sp[5], mt);
+  }
+  if (solve) atomicAdd(&sp[6 + (outer < 16 ? (outer >= 1 ? outer - 1 : 0) : 15)], 1u);
+  __syncthreads();
+  if (tid < 22 && sp[tid]) {
+    const unsigned long long x = sp[tid];
+    switch (tid) {
+      case 0: atomicAdd(&st->ptmu_solves, x); break;
+      case 1: atomicAdd(&st->ptmu_outer, x); break;
+      case 2: atomicAdd(&st->ptmu_tsat_calls, x); break;
+      case 3: atomicAdd(&st->ptmu_tsat_iters, x); break;
+      case 4: atomicMax(&st->ptmu_outer_max, x); break;
+      case 5: atomicMax(&st->ptmu_tsat_max, x); break;
+      default: atomicAdd(&st->ptmu_hist[tid - 6], x); break;
+    }
+  }
+}
+
 }  // namespace ecg

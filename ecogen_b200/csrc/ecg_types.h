@@ -69,6 +69,10 @@ struct DevStats {
   unsigned long long relax_calls, newton_evals, newton_fallback, seeded, seed_rejected, ptmu_errors, nonfinite;
   unsigned long long newton_max;
   unsigned long long hist[16];
+  // p-T-mu relaxation: saturation solves, their p* iterations (sum, max, histogram), T_sat solves and
+  // their iterations (sum, max)
+  unsigned long long ptmu_solves, ptmu_outer, ptmu_outer_max, ptmu_tsat_calls, ptmu_tsat_iters, ptmu_tsat_max;
+  unsigned long long ptmu_hist[16];
 };
 
 }  // namespace ecg

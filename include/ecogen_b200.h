@@ -97,6 +97,16 @@ typedef struct {
   int64_t ptmu_errors;          /* p-T-mu solves above 50 iterations (reference: error, run stops) */
   int64_t nonfinite_cells;      /* cells whose state became NaN/inf */
   int64_t newton_hist[16];      /* histogram of Newton evaluations: bins 1..15, 16+ in [15] */
+  /* p-T-mu relaxation (RelaxationPTMu::relaxation): solves that ran the saturation Newton on p*, their
+   * Newton iterations (sum, largest, histogram as newton_hist), and the T_sat(p) solves of
+   * Mixture::computeTsat they made (pure-phase tests included) with those solves' iterations */
+  int64_t ptmu_solves;
+  int64_t ptmu_outer_iters;
+  int64_t ptmu_outer_max;
+  int64_t ptmu_tsat_calls;
+  int64_t ptmu_tsat_iters;
+  int64_t ptmu_tsat_max;
+  int64_t ptmu_outer_hist[16];
 } ecg_step_stats;
 
 typedef struct ecg_ctx ecg_ctx;

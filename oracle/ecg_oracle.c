@@ -15,6 +15,15 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* ln of the saturation solve: the host libm's, as the reference (the default build), or a correctly
+ * rounded one (the sensitivity variant libecg_oracle_crlog.so, -DECGO_CR_LOG; see ecg_crlog.h). */
+#ifdef ECGO_CR_LOG
+#include "ecg_crlog.h"
+#define ECGO_LOG ecgo_cr_log
+#else
+#define ECGO_LOG log
+#endif
+
 #define NP_MAX 3
 #define NT_MAX 4   /* passive transports (model.xml numberTransports) */
 
@@ -851,7 +860,7 @@ static double compute_tsat(const ecgo_eos* L, const ecgo_eos* V, double p, doubl
       *err = 1;
       break;
     }
-    f = A + B / Tsat + C * log(Tsat) - log(p + piV) + D * log(p + piL);
+    f = A + B / Tsat + C * ECGO_LOG(Tsat) - ECGO_LOG(p + piV) + D * ECGO_LOG(p + piL);
     df = C / Tsat - B / (Tsat * Tsat);
   } while (fabs(f) > 1e-10);
   double dfdp = -1. / (p + piV) + D / (p + piL);

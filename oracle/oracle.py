@@ -18,6 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libecg_oracle.so")
+# the same restatement with a correctly rounded ln in the saturation solve (ecg_crlog.h): the
+# sensitivity variant, which measures how far a last-ulp change of ln travels through a run
+LIB_PATH_CRLOG = os.path.join(HERE, "_ref", "libecg_oracle_crlog.so")
 
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
@@ -43,6 +46,7 @@ class Stats(C.Structure):
 
 
 _lib = None
+_libs = {}
 
 
 def build() -> str:
@@ -51,32 +55,44 @@ def build() -> str:
     return LIB_PATH
 
 
-def lib():
+def lib(crlog: bool = False):
+    """The oracle library (crlog: the variant with a correctly rounded ln in the saturation solve)."""
     global _lib
+    if crlog:
+        if "crlog" not in _libs:
+            src = os.path.join(HERE, "ecg_oracle.c")
+            if not os.path.exists(LIB_PATH_CRLOG) or os.path.getmtime(LIB_PATH_CRLOG) < os.path.getmtime(src):
+                build()
+            _libs["crlog"] = _declare(C.CDLL(LIB_PATH_CRLOG))
+        return _libs["crlog"]
     if _lib is None:
         src = os.path.join(HERE, "ecg_oracle.c")
         if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
             build()
-        L = C.CDLL(LIB_PATH)
-        dp = C.POINTER(C.c_double)
-        L.ecgo_create.restype = C.c_void_p
-        L.ecgo_create.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
-        L.ecgo_create_ptueq.restype = C.c_void_p
-        L.ecgo_create_ptueq.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
-        L.ecgo_get_transports.argtypes = [C.c_void_p, dp]
-        L.ecgo_destroy.argtypes = [C.c_void_p]
-        L.ecgo_step.argtypes = [C.c_void_p, C.c_int, dp, dp, C.POINTER(Stats)]
-        L.ecgo_get.argtypes = [C.c_void_p] + [dp] * 8
-        L.ecgo_get_phase_pressure.argtypes = [C.c_void_p, dp]
-        L.ecgo_relax_pinf.argtypes = [C.POINTER(Case), dp, dp, dp, dp, C.POINTER(C.c_int)]
-        L.ecgo_pressure_isentropic.restype = C.c_double
-        L.ecgo_pressure_isentropic.argtypes = [C.POINTER(Eos), C.c_double, C.c_double, C.c_double, C.c_int]
-        L.ecgo_density_pfinal.restype = C.c_double
-        L.ecgo_density_pfinal.argtypes = [C.POINTER(Eos), C.c_double, C.c_double, C.c_double, dp, C.c_int]
-        L.ecgo_limiter.restype = C.c_double
-        L.ecgo_limiter.argtypes = [C.c_int, C.c_double, C.c_double]
-        _lib = L
+        _lib = _declare(C.CDLL(LIB_PATH))
     return _lib
+
+
+def _declare(L):
+    """Declares the C signatures of an oracle library."""
+    dp = C.POINTER(C.c_double)
+    L.ecgo_create.restype = C.c_void_p
+    L.ecgo_create.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
+    L.ecgo_create_ptueq.restype = C.c_void_p
+    L.ecgo_create_ptueq.argtypes = [C.POINTER(Case), dp, dp, dp, dp, dp]
+    L.ecgo_get_transports.argtypes = [C.c_void_p, dp]
+    L.ecgo_destroy.argtypes = [C.c_void_p]
+    L.ecgo_step.argtypes = [C.c_void_p, C.c_int, dp, dp, C.POINTER(Stats)]
+    L.ecgo_get.argtypes = [C.c_void_p] + [dp] * 8
+    L.ecgo_get_phase_pressure.argtypes = [C.c_void_p, dp]
+    L.ecgo_relax_pinf.argtypes = [C.POINTER(Case), dp, dp, dp, dp, C.POINTER(C.c_int)]
+    L.ecgo_pressure_isentropic.restype = C.c_double
+    L.ecgo_pressure_isentropic.argtypes = [C.POINTER(Eos), C.c_double, C.c_double, C.c_double, C.c_int]
+    L.ecgo_density_pfinal.restype = C.c_double
+    L.ecgo_density_pfinal.argtypes = [C.POINTER(Eos), C.c_double, C.c_double, C.c_double, dp, C.c_int]
+    L.ecgo_limiter.restype = C.c_double
+    L.ecgo_limiter.argtypes = [C.c_int, C.c_double, C.c_double]
+    return L
 
 
 def _p(a: np.ndarray):
@@ -200,8 +216,9 @@ def initial_fields(case) -> Dict[str, np.ndarray]:
 class Sim:
     """One oracle simulation; mirrors the reference run loop (dt starts at 1e-15, src/Run.cpp:38)."""
 
-    def __init__(self, case, fields: Optional[Dict[str, np.ndarray]] = None):
+    def __init__(self, case, fields: Optional[Dict[str, np.ndarray]] = None, crlog: bool = False):
         self.case = case
+        self._L = lib(crlog)
         self.c = make_case(case)
         f = fields or initial_fields(case)
         self.n = case.ncells
@@ -216,9 +233,9 @@ class Sim:
         if self.c.model == 2:
             T = np.ascontiguousarray(f["T"], dtype=np.float64)
             self._T = T
-            self.h = lib().ecgo_create_ptueq(C.byref(self.c), _p(a), _p(T), _p(p), _p(u), _p(tr) if self.ntr else None)
+            self.h = self._L.ecgo_create_ptueq(C.byref(self.c), _p(a), _p(T), _p(p), _p(u), _p(tr) if self.ntr else None)
         else:
-            self.h = lib().ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u), _p(tr) if self.ntr else None)
+            self.h = self._L.ecgo_create(C.byref(self.c), _p(a), _p(r), _p(p), _p(u), _p(tr) if self.ntr else None)
         if not self.h:
             raise ValueError("ecgo_create refused the case")
         self.dt = C.c_double(1e-15)
@@ -227,7 +244,7 @@ class Sim:
         self.stats = Stats()
 
     def step(self, nsteps: int = 1):
-        lib().ecgo_step(self.h, nsteps, C.byref(self.dt), C.byref(self.t), C.byref(self.stats))
+        self._L.ecgo_step(self.h, nsteps, C.byref(self.dt), C.byref(self.t), C.byref(self.stats))
         self.iteration += nsteps
 
     def run_to_time(self, t_end: float, max_steps: int = 10 ** 9):
@@ -239,19 +256,19 @@ class Sim:
         n, k = self.n, self.np
         out = {"alpha": np.zeros((k, n)), "rho": np.zeros((k, n)), "T": np.zeros((k, n)), "Y": np.zeros((k, n)),
                "rho_mix": np.zeros(n), "p": np.zeros(n), "E": np.zeros(n), "u": np.zeros((3, n))}
-        lib().ecgo_get(self.h, _p(out["alpha"]), _p(out["rho"]), _p(out["T"]), _p(out["Y"]), _p(out["rho_mix"]),
+        self._L.ecgo_get(self.h, _p(out["alpha"]), _p(out["rho"]), _p(out["T"]), _p(out["Y"]), _p(out["rho_mix"]),
                        _p(out["p"]), _p(out["E"]), _p(out["u"]))
         out["tr"] = np.zeros((self.ntr, n))
         if self.ntr:
-            lib().ecgo_get_transports(self.h, _p(out["tr"]))
+            self._L.ecgo_get_transports(self.h, _p(out["tr"]))
         return out
 
     def phase_pressures(self) -> np.ndarray:
         pk = np.zeros((self.np, self.n))
-        lib().ecgo_get_phase_pressure(self.h, _p(pk))
+        self._L.ecgo_get_phase_pressure(self.h, _p(pk))
         return pk
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().ecgo_destroy(self.h)
+            self._L.ecgo_destroy(self.h)
             self.h = None

@@ -65,3 +65,69 @@ def test_limiters_known_answers():
     assert L(3, 1.0, 3.0) == 3.0 * 4.0 / 10.0
     assert L(4, 1.0, 3.0) == 2.0 and L(5, 1.0, 3.0) == 2.0
     assert L(2, 1e-4, 1e-4) == 0.0  # product below the 1e-6 threshold
+
+
+# Longer horizons than the fixtures: the oracle against the reference binary run here (oracle/_ref,
+# built from the reference sources), for the three benchmarked physics families, on meshes both finish
+# in seconds.  The GPU path is checked against the oracle at mid sizes over hundreds of steps
+# (tests/test_gpu_long_horizon.py); this pins the oracle itself over a comparable horizon.
+LONG_PINS = {
+    "bubble2d_vanleer_150": ("c2", 64, 150),
+    "cavity3d_minmod_20": ("c3", 20, 20),
+    "expansion2d_ptmu_60": ("c5", 64, 60),
+}
+
+
+def _pin_case(key):
+    from ecogen_b200 import cases
+    kind, n, it = LONG_PINS[key]
+    if kind == "c2":
+        return cases.shock_bubble_2d(n=n, iterations=it, name="pinBubble")
+    if kind == "c3":
+        return cases.cavity_collapse_3d(n=n, iterations=it, name="pinCavity")
+    return cases.expansion_tube_2d(n=n, iterations=it, name="pinExpansion")
+
+
+def _pin_reference(key):
+    import shutil
+    import tempfile
+
+    from ecogen_b200 import cases
+    from oracle import refrun
+    case = _pin_case(key)
+    work = tempfile.mkdtemp(prefix="ecg_pin_")
+    try:
+        d = case.write(work)
+        cases.write_ecogen_list(work, [d])
+        r = refrun.run(work)
+        assert r.returncode == 0, r.stdout[-2000:]
+        return refrun.reference_prim(refrun.final_fields(work, case.name), case.nphases)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+@pytest.fixture(scope="module")
+def pin_refs():
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    from oracle import refrun
+    if not refrun.available():
+        pytest.skip("reference binary oracle/_ref/ECOGEN not built")
+    ex = cf.ProcessPoolExecutor(max_workers=len(LONG_PINS), mp_context=mp.get_context("spawn"))
+    futs = {k: ex.submit(_pin_reference, k) for k in LONG_PINS}
+    yield futs
+    ex.shutdown(wait=True)
+
+
+@pytest.mark.parametrize("key", list(LONG_PINS))
+def test_oracle_matches_reference_long_horizon(key, pin_refs):
+    case = _pin_case(key)
+    sim = oracle.Sim(case)
+    sim.step(case.iterations)
+    o = sim.fields()
+    ref = pin_refs[key].result(timeout=900)
+    for name in ("alpha", "rho", "p", "u", "E"):
+        if ref.get(name) is None:
+            continue
+        assert np.array_equal(display(o[name], name), ref[name]), f"{key}: {name} differs after {case.iterations} steps"
