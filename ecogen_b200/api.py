@@ -35,13 +35,21 @@ class Eos(C.Structure):
                 ("cv", C.c_double), ("eref", C.c_double), ("sref", C.c_double)]
 
 
+MAX_STRETCH_ZONES = 8
+
+
+class StretchZone(C.Structure):
+    _fields_ = [("start", C.c_double), ("end", C.c_double), ("factor", C.c_double), ("ncells", C.c_int32)]
+
+
 class Case(C.Structure):
     _fields_ = [("model", C.c_int32), ("nphases", C.c_int32), ("alpha_null", C.c_int32), ("order", C.c_int32),
                 ("limiter", C.c_int32 * 4), ("ncells", C.c_int32 * 3), ("length", C.c_double * 3),
                 ("cfl", C.c_double), ("time_iterations", C.c_int32), ("max_iterations", C.c_int32),
                 ("total_time", C.c_double), ("ptmu", C.c_int32), ("ptmu_liquid", C.c_int32),
                 ("ptmu_vapor", C.c_int32), ("eos", Eos * 3), ("bc", C.c_int32 * 6), ("ntransports", C.c_int32),
-                ("pt_relaxation", C.c_int32)]
+                ("pt_relaxation", C.c_int32), ("nstretch", C.c_int32 * 3),
+                ("stretch", (StretchZone * MAX_STRETCH_ZONES) * 3)]
 
 
 class StepStats(C.Structure):
@@ -197,6 +205,13 @@ def case_from_spec(spec) -> Case:
         c.bc[i] = BC_CODE[b.upper()]
     c.ntransports = len(spec.transports or [])
     c.pt_relaxation = 1 if getattr(spec, "pt_relaxation", False) else 0
+    for a, ax in enumerate("xyz"):
+        zones = (getattr(spec, "stretch", None) or {}).get(ax) or []
+        if int(spec.cells[a]) <= 1:
+            zones = []
+        c.nstretch[a] = len(zones)
+        for z, (s0, s1, f, m) in enumerate(zones):
+            c.stretch[a][z] = StretchZone(float(s0), float(s1), float(f), int(m))
     return c
 
 

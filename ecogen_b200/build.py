@@ -63,8 +63,15 @@ def _compile(src: str, extra=None) -> str:
 def build(verbose: bool = False, jobs: int = 8) -> str:
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     lib_srcs = [s for s in srcs if not os.path.basename(s).startswith("ecogen_main")]
+
+    def cost(src):  # the kernel-heavy units first (largest previous object), so the jobs finish together
+        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        return os.path.getsize(obj) if os.path.exists(obj) else (1 << 40 if src.endswith(".cu") else 0)
+
+    order = sorted(lib_srcs, key=cost, reverse=True)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(_compile, lib_srcs))
+        built = dict(zip(order, ex.map(_compile, order)))
+    objs = [built[s] for s in lib_srcs]
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -164,6 +164,8 @@ class Case:
     output_precision: Optional[int] = None  # outputMode precision (ASCII values, infoCalcul.out)
     print_freq: Optional[int] = None        # iterFreq (iteration mode; default: print at the end only)
     restart_file: Optional[int] = None      # restartSimulation restartFileNumber
+    # mesh.xml meshStretching: per axis ("x", "y", "z") a list of zones (startAt, endAt, factor, numberCells)
+    stretch: Optional[Dict[str, List[Tuple[float, float, float, int]]]] = None
     extra: Dict[str, object] = field(default_factory=dict)
 
     def boundary_types(self) -> List[str]:
@@ -222,10 +224,46 @@ class Case:
     def mesh_xml(self) -> str:
         lx, ly, lz = self.lengths
         nx, ny, nz = self.cells
+        st = ""
+        if self.stretch:  # Input::inputMesh src/InputOutput/Input.cpp:460-520
+            st = "    <meshStretching>\n"
+            for ax in ("x", "y", "z"):
+                zones = self.stretch.get(ax)
+                if not zones:
+                    continue
+                st += f"      <{ax.upper()}Stretching>\n"
+                for a, b, f, n in zones:
+                    st += f'        <stretch startAt="{a!r}" endAt="{b!r}" factor="{f!r}" numberCells="{n}"/>\n'
+                st += f"      </{ax.upper()}Stretching>\n"
+            st += "    </meshStretching>\n"
         return ('<?xml version = "1.0" encoding = "UTF-8" standalone = "yes"?>\n<mesh>\n'
                 '  <type structure="cartesian"/>\n  <cartesianMesh>\n'
                 f'    <dimensions x="{lx!r}" y="{ly!r}" z="{lz!r}"/>\n'
-                f'    <numberCells x="{nx}" y="{ny}" z="{nz}"/>\n  </cartesianMesh>\n</mesh>\n')
+                f'    <numberCells x="{nx}" y="{ny}" z="{nz}"/>\n{st}  </cartesianMesh>\n</mesh>\n')
+
+    def axis_cells(self, axis: int) -> Tuple[np.ndarray, np.ndarray]:
+        """Cell sizes and centres along one axis (MeshCartesian::meshStretching
+        src/Meshes/MeshCartesian.cpp:168-210, stretchZone::stretching src/Meshes/stretchZone.cpp:45-66)."""
+        n, l = int(self.cells[axis]), float(self.lengths[axis])
+        zones = (self.stretch or {}).get("xyz"[axis]) if n > 1 else None
+        if not zones:
+            d = l / float(n)
+            return np.full(n, d), (np.arange(n) + 0.5) * d
+        ds, ps = [], []
+        for a, b, f, m in zones:
+            d0 = (b - a) / m
+            if abs(f - 1.0) < 1e-6:
+                for i in range(m):
+                    ds.append(d0)
+                    ps.append(a + (i + 0.5) * d0)
+            else:
+                d0 = (b - a) * (1.0 - f) / (1.0 - math.pow(f, m))
+                ds.append(d0)
+                ps.append(a + 0.5 * d0)
+                for i in range(1, m):
+                    ds.append(d0 * math.pow(f, i))
+                    ps.append(ps[-1] + 0.5 * (ds[-2] + ds[-1]))
+        return np.array(ds), np.array(ps)
 
     def model_xml(self) -> str:
         s = '<?xml version = "1.0" encoding = "UTF-8" standalone = "yes"?>\n<model>\n'

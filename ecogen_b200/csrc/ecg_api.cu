@@ -196,6 +196,20 @@ ecg_status validate_case(const ecg_case* c) {
   }
   int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
   if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
+  for (int a = 0; a < 3; a++) {  // mesh stretching (stretchZone::verifyStretching src/Meshes/stretchZone.cpp:74-93)
+    const int nz = c->nstretch[a];
+    if (nz < 0 || nz > ECG_MAX_STRETCH_ZONES) { set_error("bad number of stretch zones"); return ECG_ERR_INVALID; }
+    if (nz == 0 || c->ncells[a] <= 1) continue;
+    int cells = 0;
+    for (int z = 0; z < nz; z++) {
+      const ecg_stretch_zone& st = c->stretch[a][z];
+      if (st.ncells < 1 || !(st.end > st.start) || !(st.factor > 0.)) { set_error("bad stretch zone"); return ECG_ERR_INVALID; }
+      if (z == 0 ? st.start != 0. : st.start != c->stretch[a][z - 1].end) { set_error("stretch zones are not contiguous from 0"); return ECG_ERR_INVALID; }
+      cells += st.ncells;
+    }
+    if (c->stretch[a][nz - 1].end != c->length[a]) { set_error("stretch zones do not end at the domain length"); return ECG_ERR_INVALID; }
+    if (cells != c->ncells[a]) { set_error("stretch zone cells do not add up to the axis' cells"); return ECG_ERR_INVALID; }
+  }
   int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
   if (n > (int64_t)1 << 31) { set_error("more than 2^31 cells"); return ECG_ERR_TOO_LARGE; }
   return ECG_OK;
@@ -208,13 +222,15 @@ namespace {
 // Distances of the MUSCL reconstruction per axis, with the reference's arithmetic: cell centres
 // (i + 0.5) * d, face position centre + 0.5 * d, lengths as Coord::norm of a difference
 // (src/Meshes/Element.cpp:77-113, src/Maths/Coord.cpp:82).
-void distance_tables(const ecg_case& c, std::vector<double>& h) {
-  h.assign(9 * (size_t)std::max({c.ncells[0], c.ncells[1], c.ncells[2]}), 0.);
+// Then, per axis, the cell sizes (stretched meshes).
+void distance_tables(const ecg_case& c, const std::vector<double>* sz, const std::vector<double>* ctr,
+                     std::vector<double>& h) {
   int nmax = std::max({c.ncells[0], c.ncells[1], c.ncells[2]});
+  h.assign(12 * (size_t)nmax, 0.);
   for (int a = 0; a < 3; a++) {
-    double d = c.length[a] / (double)c.ncells[a];
+    for (int i = 0; i < c.ncells[a]; i++) h[(size_t)(9 + a) * nmax + i] = sz[a][i];
     for (int i = 0; i + 1 < c.ncells[a]; i++) {
-      double pl = (i + 0.5) * d, pr = (i + 1 + 0.5) * d, pf = pl + 0.5 * d;
+      double pl = ctr[a][i], pr = ctr[a][i + 1], pf = pl + 0.5 * sz[a][i];
       double x = pl - pr, y = pf - pl, z = pf - pr;
       h[(size_t)(3 * a + 0) * nmax + i] = std::sqrt(x * x + 0. * 0. + 0. * 0.);
       h[(size_t)(3 * a + 1) * nmax + i] = std::sqrt(y * y + 0. * 0. + 0. * 0.);
@@ -510,8 +526,9 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
     }
     x->split = true;
   }
-  std::vector<double> h;
-  distance_tables(*c, h);
+  std::vector<double> h, sz[3], ctr[3];
+  for (int a = 0; a < 3; a++) axis_cells(*c, a, sz[a], ctr[a]);
+  distance_tables(*c, sz, ctr, h);
   e = cudaMalloc(&x->dist, sizeof(double) * h.size());
   if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(dist)"));
   cudaMemcpy(x->dist, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice);
@@ -521,9 +538,11 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
     x->geo.dcc[a] = x->dist + (size_t)(3 * a + 0) * nmax;
     x->geo.dfl[a] = x->dist + (size_t)(3 * a + 1) * nmax;
     x->geo.dfr[a] = x->dist + (size_t)(3 * a + 2) * nmax;
+    x->geo.dsz[a] = x->dist + (size_t)(9 + a) * nmax;
   }
   x->geo.dim = x->dim;
-  side_geometry(*c, x->geo);
+  x->geo.stretched = case_stretched(*c) ? 1 : 0;
+  side_geometry(*c, sz, ctr, x->geo);
   // MeshCartesian::initializeGeometrieMonoCpu :228-236 and face surfaces :287, :320, :353
   double dX = c->length[0] / (double)c->ncells[0], dY = c->length[1] / (double)c->ncells[1],
          dZ = c->length[2] / (double)c->ncells[2];

@@ -491,6 +491,10 @@ extern "C" ecg_status ecg_batch_create(const ecg_case* cs, int32_t ncases, ecg_b
       set_error("batched mode runs without passive transports");
       return ECG_ERR_UNSUPPORTED;
     }
+    if (case_stretched(x)) {
+      set_error("batched mode runs uniform meshes");
+      return ECG_ERR_UNSUPPORTED;
+    }
     if (x.bc[0] != ECG_BC_NONREFLECTING || x.bc[1] != ECG_BC_NONREFLECTING) {
       set_error("batched mode runs non-reflecting sides only");
       return ECG_ERR_UNSUPPORTED;

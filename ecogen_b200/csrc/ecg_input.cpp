@@ -225,7 +225,36 @@ extern "C" ecg_status ecg_input_read(const char* case_dir, const char* eos_dir, 
   if (c.ncells[0] <= 1) return bail(ECG_ERR_XML, "Number of cells in the x-direction has to be superior to 1");
   if (c.ncells[2] > 1 && c.ncells[1] <= 1)
     return bail(ECG_ERR_XML, "Number of cells in the z-direction can't be superior to 1 if number of cells in the y-direction is equal to 1");
-  if (cm->child("meshStretching")) return bail(ECG_ERR_UNSUPPORTED, "mesh stretching is not supported");
+  if (const Node* ms = cm->child("meshStretching")) {
+    // Input::inputMesh src/InputOutput/Input.cpp:460-520: zones per axis with more than one cell, checked
+    // like stretchZone::verifyStretching (src/Meshes/stretchZone.cpp:74-93); the axis then has the sum of
+    // its zones' cells (MeshCartesian::meshStretching src/Meshes/MeshCartesian.cpp:168-210)
+    const char* tags[3] = {"XStretching", "YStretching", "ZStretching"};
+    for (int a = 0; a < 3; a++) {
+      if (c.ncells[a] <= 1) continue;
+      const Node* ax = ms->child(tags[a]);
+      if (!ax) continue;
+      int nz = 0, cells = 0;
+      for (const Node* st : ax->all("stretch")) {
+        if (nz == ECG_MAX_STRETCH_ZONES) return bail(ECG_ERR_UNSUPPORTED, "more than 8 stretch zones on an axis");
+        ecg_stretch_zone& z = c.stretch[a][nz];
+        if (!st->get_double("startAt", &z.start)) return bail(ECG_ERR_XML, "mesh.xml: <stretch startAt> missing");
+        if (!st->get_double("endAt", &z.end)) return bail(ECG_ERR_XML, "mesh.xml: <stretch endAt> missing");
+        if (!st->get_double("factor", &z.factor)) return bail(ECG_ERR_XML, "mesh.xml: <stretch factor> missing");
+        if (!st->get_int("numberCells", &z.ncells)) return bail(ECG_ERR_XML, "mesh.xml: <stretch numberCells> missing");
+        if (z.ncells < 1) return bail(ECG_ERR_XML, "mesh.xml: <stretch numberCells> below 1");
+        cells += z.ncells;
+        nz++;
+      }
+      if (nz == 0) continue;
+      const bool ok_start = c.stretch[a][0].start == 0., ok_end = c.stretch[a][nz - 1].end == c.length[a];
+      bool contiguous = true;
+      for (int z = 1; z < nz; z++) contiguous = contiguous && c.stretch[a][z].start == c.stretch[a][z - 1].end;
+      if (!ok_start || !ok_end || !contiguous) return bail(ECG_ERR_XML, "mesh.xml: stretching zones (ErrorXMLStretching)");
+      c.nstretch[a] = nz;
+      c.ncells[a] = cells;
+    }
+  }
   if (cm->child("AMR")) return bail(ECG_ERR_UNSUPPORTED, "AMR is not supported");
 
   // ---------------------------------------------------------------- model.xml (Input::inputModel :566)
@@ -632,13 +661,13 @@ extern "C" ecg_status ecg_input_fill(const ecg_input* in, double* const* fields,
   const int nf = ecg::abi_nfields(c);
   for (int f = 0; f < nf; f++)
     if (!fields[f]) return fail(ECG_ERR_INVALID, "ecg_input_fill: null field pointer");
-  const double d[3] = {c.length[0] / (double)c.ncells[0], c.length[1] / (double)c.ncells[1],
-                       c.length[2] / (double)c.ncells[2]};
+  std::vector<double> sz[3], ctr[3];  // cell sizes and centres per axis (stretched or uniform)
+  for (int a = 0; a < 3; a++) ecg::axis_cells(c, a, sz[a], ctr[a]);
   const double eps = c.alpha_null ? 1.e-15 : 0.;
   const int nx = c.ncells[0], ny = c.ncells[1];
   for (int64_t i = 0; i < n; i++) {
     int ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / ((int64_t)nx * ny));
-    const double pos[3] = {(ix + 0.5) * d[0], (iy + 0.5) * d[1], (iz + 0.5) * d[2]};
+    const double pos[3] = {ctr[0][ix], ctr[1][iy], ctr[2][iz]};
     const StateIC* S = nullptr;
     for (const Domain& D : in->domains)
       if (belongs(D, pos)) S = &in->states[D.state];

@@ -224,8 +224,15 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
       double ul[3], ur[3], Fn[3];
       to_local(ax, false, ug, ul);
       to_local(ax, false, vg, ur);
+      int gf[3];  // the face's left cell, then its right cell: their CFL lengths
+      gf[ax] = gl;
+      gf[b1] = org[b1] + l1;
+      gf[b2] = org[b2] + l2;
+      const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+      gf[ax] = gl + 1;
+      const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
       Flux<NP> F;
-      hllc<NP>(M, tl, ul, tr, ur, G.lcfl, G.lcfl, dtmax, Fn, F);
+      hllc<NP>(M, tl, ul, tr, ur, lL, lR, dtmax, Fn, F);
       to_global(ax, false, Fn, F.mom);
 #pragma unroll
       for (int k = 0; k < NP; k++) {
@@ -247,7 +254,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
     if (active) {
       int la = lc[ax];
       int line = lc[b1] + lc[b2] * e1;
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
 #pragma unroll
       for (int side = 0; side < 2; side++) {
         int j = la + side;
@@ -295,7 +302,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
           cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
         }
         to_local(ax, sd == 0, ug, ul);
-        wallp[ax] = wall_pstar<NP>(t, ul, G.lcfl, dtmax);
+        wallp[ax] = wall_pstar<NP>(t, ul, cell_lcfl(G, gc[0], gc[1], gc[2]), dtmax);
       }
     }
     __syncthreads();
@@ -314,17 +321,18 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
       bool neg = (bf & 1) == 0;
       if (neg ? (gc[ax] != 0) : (gc[ax] != G.n[ax] - 1)) continue;
       double sMb = 0.;
+      const double cAb = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
       if (G.bc[bf] == ECG_BC_SYMMETRY)
-        wall_acc<NP, DIM>(ax, neg, wallp[ax], G.coefA[ax], an, pn, aa, am, ae, amom, aE);
+        wall_acc<NP, DIM>(ax, neg, wallp[ax], cAb, an, pn, aa, am, ae, amom, aE);
       else
-        boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, G.lcfl, G.coefA[ax], dtmax, an, pn, aa, am, ae, amom, aE,
-                               &sMb);
+        boundary_face<NP, DIM>(M, P.q, nn, cell, ax, neg, cell_lcfl(G, gc[0], gc[1], gc[2]), cAb, dtmax, an, pn, aa,
+                               am, ae, amom, aE, &sMb);
 #pragma unroll
       for (int t = 0; t < NTM; t++) {  // transports: T sM on a non-reflecting side, nothing on a symmetry side
         if (t >= P.ntr) continue;
         const double ft = (G.bc[bf] == ECG_BC_SYMMETRY) ? 0. : P.q[(int64_t)(FL::NS + t) * nn + cell] * sMb;
-        at[t] -= G.coefA[ax] * ft;
-        at[t] -= -G.coefA[ax] * tn[t] * sMb;
+        at[t] -= cAb * ft;
+        at[t] -= -cAb * tn[t] * sMb;
       }
     }
 

@@ -169,6 +169,9 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
         const int sd = (f == 0) ? 0 : 1;
         const bool neg = sd == 0;
         const int rc = FT::cidx(line, sd == 0 ? fl + 2 : fl + 1);
+        int gc[3] = {g[0], g[1], g[2]};  // the side's cell
+        gc[AX] = sd == 0 ? 0 : nax - 1;
+        const double lc = cell_lcfl(G, gc[0], gc[1], gc[2]);
         Thermo<NP> t;
         double ug[3], ul[3];
         if (G.bc[2 * AX + sd] == ECG_BC_SYMMETRY) {
@@ -179,7 +182,7 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
             cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
           }
           to_local(AX, neg, ug, ul);
-          const double pstar = wall_pstar<NP>(t, ul, G.lcfl, dtmax);
+          const double pstar = wall_pstar<NP>(t, ul, lc, dtmax);
 #pragma unroll
           for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
           F.E = 0.;
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
         } else {
           cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
           to_local(AX, neg, ug, ul);
-          hllc<NP>(M, t, ul, t, ul, G.lcfl, G.lcfl, dtmax, Fn, F);
+          hllc<NP>(M, t, ul, t, ul, lc, lc, dtmax, Fn, F);
         }
         to_global(AX, neg, Fn, F.mom);
       } else {
@@ -225,7 +228,12 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
         double ul[3], ur[3];
         to_local(AX, false, ug, ul);
         to_local(AX, false, vg, ur);
-        hllc<NP>(M, tl, ul, tr, ur, G.lcfl, G.lcfl, dtmax, Fn, F);
+        int gf[3] = {g[0], g[1], g[2]};  // the face's left cell, then its right cell: their CFL lengths
+        gf[AX] = gl;
+        const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+        gf[AX] = gl + 1;
+        const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
+        hllc<NP>(M, tl, ul, tr, ur, lL, lR, dtmax, Fn, F);
         to_global(AX, false, Fn, F.mom);
       }
       const int64_t nfa = split_nfaces(G.n, AX);
@@ -316,7 +324,7 @@ __global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_
 #pragma unroll
     for (int ax = 0; ax < DIM; ax++) {
       const int64_t nfa = split_nfaces(G.n, ax);
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, g[0], g[1], g[2]);
       Flux<NP> F;
       if (g[ax] >= 1) {
         load_face_flux<NP, DIM>(fa[ax], nfa, split_fid(G.n, ax, g[ax], g[0], g[1], g[2]), F);
@@ -337,7 +345,7 @@ __global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_
       Flux<NP> F;
       load_face_flux<NP, DIM>(fa[ax], split_nfaces(G.n, ax), split_fid(G.n, ax, neg ? 0 : G.n[ax], g[0], g[1], g[2]),
                               F);
-      acc_face<NP, DIM>(G.coefA[ax], false, F, an, pn, aa, am, ae, amom, aE);
+      acc_face<NP, DIM>(cell_coefA(G, ax, g[0], g[1], g[2]), false, F, an, pn, aa, am, ae, amom, aE);
     }
     kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
   }

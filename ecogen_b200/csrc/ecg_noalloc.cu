@@ -126,6 +126,10 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
     set_error("ecg_step_noalloc runs without passive transports");
     return ECG_ERR_UNSUPPORTED;
   }
+  if (case_stretched(*c)) {
+    set_error("ecg_step_noalloc runs uniform meshes; use ecg_create / ecg_step for a stretched mesh");
+    return ECG_ERR_UNSUPPORTED;
+  }
   const int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
   if (n > kMaxCells) {
     set_error("ecg_step_noalloc: more than ECG_NOALLOC_MAX_CELLS (65536) cells; use ecg_create / ecg_step");
@@ -158,7 +162,11 @@ extern "C" ecg_status ecg_step_noalloc(const ecg_case* c, const double* state_in
     G.dfr[a] = S->dist + (size_t)(3 * a + 2) * nmax;
   }
   G.dim = dim;
-  side_geometry(*c, G);
+  {
+    std::vector<double> sz[3], ctr[3];  // uniform cells (stretched meshes are refused above)
+    for (int a = 0; a < 3; a++) axis_cells(*c, a, sz[a], ctr[a]);
+    side_geometry(*c, sz, ctr, G);
+  }
   double dX = c->length[0] / (double)c->ncells[0], dY = c->length[1] / (double)c->ncells[1],
          dZ = c->length[2] / (double)c->ncells[2];
   double vol = dX * dY * dZ;

@@ -145,6 +145,30 @@ inline void set_thinc(StepParams& P, const ecg_case& c) {
   P.thinc_tanh = std::tanh(1.6);
 }
 
+// CFL length of cell (i, j, k): the smallest size along the used axes, x 0.6 beyond 1D
+// (MeshCartesian::initializeGeometrieMonoCpu src/Meshes/MeshCartesian.cpp:232-238); the same for every
+// cell of a uniform mesh.
+__device__ __forceinline__ double cell_lcfl(const Geometry& G, int i, int j, int k) {
+  if (!G.stretched) return G.lcfl;
+  double l = 1.e10;
+  if (G.n[0] != 1) l = dmin(l, G.dsz[0][i]);
+  if (G.n[1] != 1) l = dmin(l, G.dsz[1][j]);
+  if (G.n[2] != 1) l = dmin(l, G.dsz[2][k]);
+  if (G.dim > 1) l *= 0.6;
+  return l;
+}
+
+// Face surface over cell volume for the faces of cell (i, j, k) normal to axis ax: the coefA of
+// CellInterface::addFlux / subtractFlux (src/Order1/CellInterface.cpp:269, :287), surface dY dZ (X
+// faces), dX dZ (Y faces) or dX dY (Z faces) over the volume dX dY dZ (:226, :287, :320, :353).
+__device__ __forceinline__ double cell_coefA(const Geometry& G, int ax, int i, int j, int k) {
+  if (!G.stretched) return G.coefA[ax];
+  const double dx = G.dsz[0][i], dy = G.dsz[1][j], dz = G.dsz[2][k];
+  const double vol = dx * dy * dz;
+  const double s = (ax == 0) ? dy * dz : ((ax == 1) ? dx * dz : dx * dy);
+  return s / vol * 1.;
+}
+
 // Faces normal to axis ax of a mesh of n cells per axis, the two domain sides of every line included
 // (the face arrays of the split form).
 __host__ __device__ inline int64_t split_nfaces(const int n[3], int ax) {

@@ -252,7 +252,14 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
       to_local(ax, false, L.u, ul);
       to_local(ax, false, R.u, ur);
       double sM = 0.;
-      hllc_euler(L, ul, R, ur, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE, &sM);
+      int gf[3];  // the face's left cell, then its right cell: their CFL lengths
+      gf[ax] = gl;
+      gf[b1] = org[b1] + l1;
+      gf[b2] = org[b2] + l2;
+      const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+      gf[ax] = gl + 1;
+      const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
+      hllc_euler(L, ul, R, ur, lL, lR, dtmax, Fm, Fn, FE, &sM);
       to_global(ax, false, Fn, Fg);
       sfl[0 * FS + e] = Fm;
 #pragma unroll
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
     if (active) {
       int la = lc[ax];
       int line = lc[b1] + lc[b2] * e1;
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
 #pragma unroll
       for (int side = 0; side < 2; side++) {
         int j = la + side;
@@ -331,7 +338,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
         // ModEuler::solveRiemannWall src/Models/Euler/ModEuler.cpp:368-409
         const double uL = ul[0], cL = S.c, pL = S.p, rhoL = S.rho;
         const double sL = dmin(uL - cL, -uL - cL);
-        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * G.lcfl / fabs(sL));
+        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * cell_lcfl(G, gc[0], gc[1], gc[2]) / fabs(sL));
         wallp[ax] = rhoL * uL * (uL - sL) + pL;
       }
     }
@@ -348,7 +355,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
         const double Fn[3] = {wallp[ax], 0., 0.};
         double Fg[3];
         to_global(ax, neg, Fn, Fg);
-        const double cA = G.coefA[ax];
+        const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
         am -= cA * 0.;
 #pragma unroll
         for (int d = 0; d < DIM; d++) amom[d] -= cA * Fg[d];
@@ -371,9 +378,10 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
       double ul[3], Fn[3], Fm, FE, Fg[3];
       to_local(ax, neg, S.u, ul);
       double sMb = 0.;
-      hllc_euler(S, ul, S, ul, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE, &sMb);
+      const double lc = cell_lcfl(G, gc[0], gc[1], gc[2]);
+      hllc_euler(S, ul, S, ul, lc, lc, dtmax, Fm, Fn, FE, &sMb);
       to_global(ax, neg, Fn, Fg);
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
       am -= cA * Fm;
 #pragma unroll
       for (int d = 0; d < DIM; d++) amom[d] -= cA * Fg[d];

@@ -299,7 +299,14 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
       double ul[3], ur[3], Fn[3], Fg[3], Fm[2], FE;
       to_local(ax, false, S[0].u, ul);
       to_local(ax, false, S[1].u, ur);
-      hllc_pt(S[0], ul, S[1], ur, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE);
+      int gf[3];  // the face's left cell, then its right cell: their CFL lengths
+      gf[ax] = gl;
+      gf[b1] = org[b1] + line % e1;
+      gf[b2] = org[b2] + line / e1;
+      const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+      gf[ax] = gl + 1;
+      const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
+      hllc_pt(S[0], ul, S[1], ur, lL, lR, dtmax, Fm, Fn, FE);
       to_global(ax, false, Fn, Fg);
       sfl[0 * FS + e] = Fm[0];
       sfl[1 * FS + e] = Fm[1];
@@ -312,7 +319,7 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
     if (active) {
       const int la = lc[ax];
       const int line = lc[b1] + lc[b2] * e1;
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
 #pragma unroll
       for (int side = 0; side < 2; side++) {
         const int j = la + side;
@@ -357,12 +364,13 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
       pt_complete(M, s);  // BoundCond::solveRiemann calls fulfillState on its buffer
       double ul[3], Fn[3], Fg[3];
       to_local(ax, neg, s.u, ul);
-      const double cA = G.coefA[ax];
+      const double cA = cell_coefA(G, ax, gc[0], gc[1], gc[2]);
+      const double lc = cell_lcfl(G, gc[0], gc[1], gc[2]);
       if (G.bc[bf] == ECG_BC_SYMMETRY) {
         // ModPTUEq::solveRiemannWall src/Models/PTUEq/ModPTUEq.cpp:233-265 (first order only)
         const double uL = ul[0];
         const double sL = dmin(uL - s.c, -uL - s.c);
-        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, G.lcfl / fabs(sL));
+        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, lc / fabs(sL));
         Fn[0] = s.rho * (uL - sL) * uL + s.p;
         Fn[1] = Fn[2] = 0.;
         to_global(ax, neg, Fn, Fg);
@@ -371,7 +379,7 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
         continue;
       }
       double Fm[2], FE;
-      hllc_pt(s, ul, s, ul, G.lcfl, G.lcfl, dtmax, Fm, Fn, FE);
+      hllc_pt(s, ul, s, ul, lc, lc, dtmax, Fm, Fn, FE);
       to_global(ax, neg, Fn, Fg);
       am[0] -= cA * Fm[0];
       am[1] -= cA * Fm[1];

@@ -2,6 +2,7 @@
 #pragma once
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/ecogen_b200.h"
 
@@ -43,16 +44,21 @@ struct Geometry {
   int bc[6];
   double wslope[6];
   double wdist[6];
+  // Stretched meshes (mesh.xml meshStretching): cell sizes per axis and index; the kernels then take
+  // each cell's own lCFL and surface / volume (cell_lcfl, cell_coefA) instead of lcfl and coefA.
+  int stretched;
+  const double* dsz[3];
 };
 
-// Fills the side fields of a Geometry with the reference's mesh arithmetic (cell centres
-// (i + 0.5) * d, minus faces at 0, plus faces at the last centre + d / 2, src/Meshes/MeshCartesian.cpp:168,
-// :402, :426).
-inline void side_geometry(const ecg_case& c, Geometry& g) {
+// Fills the side fields of a Geometry with the reference's mesh arithmetic (cell centres and sizes of
+// each axis as MeshCartesian::meshStretching computes them, minus faces at 0, plus faces at the last
+// centre + its half size, src/Meshes/MeshCartesian.cpp:168, :402, :426).  sz / ctr: per axis, the cell
+// sizes and centres.
+inline void side_geometry(const ecg_case& c, const std::vector<double>* sz, const std::vector<double>* ctr,
+                          Geometry& g) {
   for (int a = 0; a < 3; a++) {
-    double d = c.length[a] / (double)c.ncells[a];
-    double p0 = (0 + 0.5) * d, pn = (c.ncells[a] - 1 + 0.5) * d;
-    double fm = 0., fp = pn + 0.5 * d;
+    double p0 = ctr[a][0], pn = ctr[a][c.ncells[a] - 1];
+    double fm = 0., fp = pn + 0.5 * sz[a][c.ncells[a] - 1];
     for (int side = 0; side < 2; side++) {
       double cen = side ? pn : p0, face = side ? fp : fm;
       double x = face - cen;

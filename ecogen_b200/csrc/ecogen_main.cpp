@@ -31,6 +31,7 @@
 extern "C" {
 #include "../../include/ecogen_b200.h"
 }
+#include "ecg_internal.h"  // axis_cells: the mesh's cell sizes and centres
 
 namespace {
 
@@ -197,12 +198,13 @@ std::vector<double> grad_rho(const ecg_case& c, const std::vector<double>& rho) 
   const int nx = c.ncells[0], ny = c.ncells[1], nz = c.ncells[2];
   const int64_t n = (int64_t)nx * ny * nz;
   const int nn[3] = {nx, ny, nz};
-  double d[3], bm[3], bp[3];
+  double bm[3], bp[3];
+  std::vector<double> sz[3], ctr[3];  // cell sizes and centres per axis (stretched or uniform)
   for (int a = 0; a < 3; a++) {
-    d[a] = c.length[a] / (double)nn[a];
-    const double p0 = (0 + 0.5) * d[a], pl = (nn[a] - 1 + 0.5) * d[a];
-    bm[a] = std::fabs(p0 - 0.) * 2.;               // Xm face at 0
-    bp[a] = std::fabs(pl - (pl + 0.5 * d[a])) * 2.;  // Xp face at the last centre + d / 2
+    ecg::axis_cells(c, a, sz[a], ctr[a]);
+    const double p0 = ctr[a][0], pl = ctr[a][nn[a] - 1];
+    bm[a] = std::fabs(p0 - 0.) * 2.;                         // Xm face at 0
+    bp[a] = std::fabs(pl - (pl + 0.5 * sz[a][nn[a] - 1])) * 2.;  // Xp face at the last centre + its half size
   }
   std::vector<double> g((size_t)n);
   const int64_t stride[3] = {1, nx, (int64_t)nx * ny};
@@ -216,7 +218,7 @@ std::vector<double> grad_rho(const ecg_case& c, const std::vector<double>& rho) 
         if (o < 0 || o >= nn[a]) continue;
         const int64_t L = side ? i : i - stride[a], R = side ? i + stride[a] : i;
         const int iL = side ? ijk[a] : o, iR = side ? o : ijk[a];
-        const double xL = (iL + 0.5) * d[a], xR = (iR + 0.5) * d[a];
+        const double xL = ctr[a][iL], xR = ctr[a][iR];
         const double dist_a = std::fabs(xL - xR);
         const double dist = std::sqrt((xL - xR) * (xL - xR) + 0. * 0. + 0. * 0.);
         sum[a] += dist_a;
@@ -281,10 +283,11 @@ struct Output {
     o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"RectilinearGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
     o << "  <RectilinearGrid WholeExtent=\"0 " << nx << " 0 " << ny << " 0 " << nz << "\">\n";
     o << "    <Piece Extent=\"0 " << nx << " 0 " << ny << " 0 " << nz << "\">\n      <Coordinates>\n";
-    for (int a = 0; a < 3; a++) {
-      std::vector<double> x((size_t)c.ncells[a] + 1);
-      double d = c.length[a] / (double)c.ncells[a];
-      for (int i = 0; i <= c.ncells[a]; i++) x[i] = i * d;
+    for (int a = 0; a < 3; a++) {  // MeshCartesian::getCoord src/Meshes/MeshCartesian.cpp:1791-1815
+      std::vector<double> sz, ctr, x;
+      ecg::axis_cells(c, a, sz, ctr);
+      for (int i = 0; i < c.ncells[a]; i++) x.push_back(ctr[i] - 0.5 * sz[i]);
+      x.push_back(ctr[c.ncells[a] - 1] + 0.5 * sz[c.ncells[a] - 1]);
       write_array(o, "", x, 1, binary);
     }
     o << "      </Coordinates>\n      <CellData>\n";

@@ -64,6 +64,15 @@ typedef struct {
   double gamma, pinf, b, cv, eref, sref;
 } ecg_eos;
 
+/* One zone of mesh.xml <meshStretching> along an axis (stretchZone, src/Meshes/stretchZone.cpp:45-66):
+ * ncells cells from start to end whose sizes grow geometrically by factor (uniform when |factor - 1| <
+ * 1e-6).  The zones of an axis follow one another from 0 to the axis length. */
+#define ECG_MAX_STRETCH_ZONES 8
+typedef struct {
+  double start, end, factor;
+  int32_t ncells;
+} ecg_stretch_zone;
+
 /* A case as the four ECOGEN XML files describe it (Input::readInputXML src/InputOutput/Input.cpp:54). */
 typedef struct {
   int32_t model;                /* ECG_MODEL_* */
@@ -83,6 +92,9 @@ typedef struct {
   int32_t bc[6];                /* ECG_BC_* of the sides Xm, Xp, Ym, Yp, Zm, Zp (MeshCartesian::assignLimits) */
   int32_t ntransports;          /* passive transports (model.xml numberTransports, src/Transport), 0..2 */
   int32_t pt_relaxation;        /* model.xml <relaxation type="PT">: analytic p-T relaxation (RelaxationPT) */
+  int32_t nstretch[3];          /* mesh.xml meshStretching zones per axis (0: cells of length / ncells);
+                                   the zones' cells add up to ncells[axis] */
+  ecg_stretch_zone stretch[3][ECG_MAX_STRETCH_ZONES];
 } ecg_case;
 
 /* Counters of one ecg_step call (replace the reference's errors / warnings vectors). */

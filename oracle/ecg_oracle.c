@@ -1053,11 +1053,53 @@ double ecgo_limiter(int kind, double s1, double s2) {
 
 /* ----------------------------------------------------------------------------------------- mesh */
 
+/* Cell sizes and centres along one axis: MeshCartesian::meshStretching src/Meshes/MeshCartesian.cpp:168-210
+ * (uniform: l / n and (i + 0.5) d) with stretchZone::stretching src/Meshes/stretchZone.cpp:45-66 for
+ * each zone in turn (geometric progression of ratio `factor`, or uniform when |factor - 1| < 1e-6). */
+static void axis_cells(const ecgo_case* c, int ax, int n, double l, double* d, double* pos) {
+  if (c->nstretch[ax] == 0 || n == 1) {
+    const double dd = l / (double)n;
+    for (int i = 0; i < n; i++) {
+      d[i] = dd;
+      pos[i] = (i + 0.5) * dd;
+    }
+    return;
+  }
+  int m = 0;
+  for (int z = 0; z < c->nstretch[ax]; z++) {
+    const ecgo_stretch* st = &c->stretch[ax][z];
+    double dX0 = (st->end - st->start) / st->ncells;
+    if (fabs(st->factor - 1.) < 1e-6) {
+      for (int i = 0; i < st->ncells; i++, m++) {
+        d[m] = dX0;
+        pos[m] = st->start + (i + 0.5) * dX0;
+      }
+    } else {
+      dX0 = (st->end - st->start) * (1. - st->factor) / (1. - pow(st->factor, st->ncells));
+      d[m] = dX0;
+      pos[m] = st->start + 0.5 * dX0;
+      m++;
+      for (int i = 1; i < st->ncells; i++, m++) {
+        d[m] = dX0 * pow(st->factor, i);
+        pos[m] = pos[m - 1] + 0.5 * (d[m - 1] + d[m]);
+      }
+    }
+  }
+}
+
 static void build_mesh(ecgo_sim* S) {
-  /* MeshCartesian::meshStretching :168 (uniform) and initializeGeometrieMonoCpu :212-558 */
+  /* MeshCartesian::meshStretching :168 and initializeGeometrieMonoCpu :212-558 */
   const ecgo_case* c = &S->c;
   int nx = c->nx, ny = c->ny, nz = c->nz, n = nx * ny * nz;
-  double dX = c->lx / (double)nx, dY = c->ly / (double)ny, dZ = c->lz / (double)nz;
+  double* dX = (double*)malloc(sizeof(double) * (size_t)nx);
+  double* dY = (double*)malloc(sizeof(double) * (size_t)ny);
+  double* dZ = (double*)malloc(sizeof(double) * (size_t)nz);
+  double* pX = (double*)malloc(sizeof(double) * (size_t)nx);
+  double* pY = (double*)malloc(sizeof(double) * (size_t)ny);
+  double* pZ = (double*)malloc(sizeof(double) * (size_t)nz);
+  axis_cells(c, 0, nx, c->lx, dX, pX);
+  axis_cells(c, 1, ny, c->ly, dY, pY);
+  axis_cells(c, 2, nz, c->lz, dZ, pZ);
   S->pos = (double*)calloc((size_t)3 * n, sizeof(double));
   S->vol = (double*)calloc((size_t)n, sizeof(double));
   S->lcfl = (double*)calloc((size_t)n, sizeof(double));
@@ -1065,16 +1107,16 @@ static void build_mesh(ecgo_sim* S) {
   for (int i = 0; i < 6 * n; i++) S->cellface[i] = -1;
   for (int i = 0; i < n; i++) {
     int iz = i / (nx * ny), r = i % (nx * ny), iy = r / nx, ix = r % nx;
-    S->vol[i] = dX * dY * dZ;
+    S->vol[i] = dX[ix] * dY[iy] * dZ[iz];
     double l = 1.e10;
-    if (nx != 1) l = omin(l, dX);
-    if (ny != 1) l = omin(l, dY);
-    if (nz != 1) l = omin(l, dZ);
+    if (nx != 1) l = omin(l, dX[ix]);
+    if (ny != 1) l = omin(l, dY[iy]);
+    if (nz != 1) l = omin(l, dZ[iz]);
     if (S->dim > 1) l *= 0.6;
     S->lcfl[i] = l;
-    S->pos[3 * i + 0] = (ix + 0.5) * dX;
-    S->pos[3 * i + 1] = (iy + 0.5) * dY;
-    S->pos[3 * i + 2] = (iz + 0.5) * dZ;
+    S->pos[3 * i + 0] = pX[ix];
+    S->pos[3 * i + 1] = pY[iy];
+    S->pos[3 * i + 2] = pZ[iz];
   }
   int maxf = 3 * n + 2 * (ny * nz + nx * nz + nx * ny);
   S->faces = (OFace*)calloc((size_t)maxf, sizeof(OFace));
@@ -1088,8 +1130,8 @@ static void build_mesh(ecgo_sim* S) {
         OFace* F = &S->faces[f];
         F->L = IDX(ix, iy, iz); F->R = IDX(ix + 1, iy, iz); F->axis = 0; F->bc = -1;
         SETV(F->n, 1., 0., 0.); SETV(F->t, 0., 1., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dY * dZ;
-        SETV(F->pos, S->pos[3 * F->L] + 0.5 * dX, S->pos[3 * F->L + 1], S->pos[3 * F->L + 2]);
+        F->surface = dY[iy] * dZ[iz];
+        SETV(F->pos, S->pos[3 * F->L] + 0.5 * dX[ix], S->pos[3 * F->L + 1], S->pos[3 * F->L + 2]);
         S->cellface[6 * F->L + 1] = f; S->cellface[6 * F->R + 0] = f;
         f++;
       }
@@ -1099,8 +1141,8 @@ static void build_mesh(ecgo_sim* S) {
         OFace* F = &S->faces[f];
         F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy + 1, iz); F->axis = 1; F->bc = -1;
         SETV(F->n, 0., 1., 0.); SETV(F->t, -1., 0., 0.); SETV(F->b, 0., 0., 1.);
-        F->surface = dX * dZ;
-        SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1] + 0.5 * dY, S->pos[3 * F->L + 2]);
+        F->surface = dX[ix] * dZ[iz];
+        SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1] + 0.5 * dY[iy], S->pos[3 * F->L + 2]);
         S->cellface[6 * F->L + 3] = f; S->cellface[6 * F->R + 2] = f;
         f++;
       }
@@ -1110,8 +1152,8 @@ static void build_mesh(ecgo_sim* S) {
         OFace* F = &S->faces[f];
         F->L = IDX(ix, iy, iz); F->R = IDX(ix, iy, iz + 1); F->axis = 2; F->bc = -1;
         SETV(F->n, 0., 0., 1.); SETV(F->t, 1., 0., 0.); SETV(F->b, 0., 1., 0.);
-        F->surface = dX * dY;
-        SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1], S->pos[3 * F->L + 2] + 0.5 * dZ);
+        F->surface = dX[ix] * dY[iy];
+        SETV(F->pos, S->pos[3 * F->L], S->pos[3 * F->L + 1], S->pos[3 * F->L + 2] + 0.5 * dZ[iz]);
         S->cellface[6 * F->L + 5] = f; S->cellface[6 * F->R + 4] = f;
         f++;
       }
@@ -1134,10 +1176,11 @@ static void build_mesh(ecgo_sim* S) {
           F->L = IDX(ijk[0], ijk[1], ijk[2]); F->R = -1; F->axis = ax;
           F->bc = c->bc[2 * ax + side];
           double sg = side ? 1. : -1.;
-          if (ax == 0) { SETV(F->n, sg, 0., 0.); SETV(F->t, 0., sg, 0.); SETV(F->b, 0., 0., 1.); F->surface = dY * dZ; }
-          if (ax == 1) { SETV(F->n, 0., sg, 0.); SETV(F->t, -sg, 0., 0.); SETV(F->b, 0., 0., 1.); F->surface = dX * dZ; }
-          if (ax == 2) { SETV(F->n, 0., 0., sg); SETV(F->t, sg, 0., 0.); SETV(F->b, 0., 1., 0.); F->surface = dX * dY; }
-          const double dd[3] = {dX, dY, dZ};
+          const double sx = dX[ijk[0]], sy = dY[ijk[1]], sz = dZ[ijk[2]];
+          if (ax == 0) { SETV(F->n, sg, 0., 0.); SETV(F->t, 0., sg, 0.); SETV(F->b, 0., 0., 1.); F->surface = sy * sz; }
+          if (ax == 1) { SETV(F->n, 0., sg, 0.); SETV(F->t, -sg, 0., 0.); SETV(F->b, 0., 0., 1.); F->surface = sx * sz; }
+          if (ax == 2) { SETV(F->n, 0., 0., sg); SETV(F->t, sg, 0., 0.); SETV(F->b, 0., 1., 0.); F->surface = sx * sy; }
+          const double dd[3] = {sx, sy, sz};
           for (int d = 0; d < 3; d++) F->pos[d] = S->pos[3 * F->L + d];
           F->pos[ax] = side ? S->pos[3 * F->L + ax] + 0.5 * dd[ax] : 0.;
           S->cellface[6 * F->L + 2 * ax + side] = f;
@@ -1148,6 +1191,7 @@ static void build_mesh(ecgo_sim* S) {
 #undef IDX
 #undef SETV
   S->nfaces = f;
+  free(dX); free(dY); free(dZ); free(pX); free(pY); free(pZ);
 }
 
 static double vnorm_diff(const double* a, const double* b) { /* Element::distance / Face::distance */

@@ -34,6 +34,13 @@ typedef struct {
   double gamma, pinf, b, cv, eref, sref;
 } ecgo_eos;
 
+/* One zone of mesh.xml meshStretching (stretchZone, src/Meshes/stretchZone.h). */
+#define ECGO_MAX_STRETCH 8
+typedef struct {
+  double start, end, factor;
+  int ncells;
+} ecgo_stretch;
+
 typedef struct {
   int model;       /* ECGO_MODEL_* */
   int nphases;     /* 1 for Euler, 2..3 for Kapila */
@@ -48,6 +55,8 @@ typedef struct {
   int bc[6];       /* ECGO_BC_* per side */
   int ntr;         /* passive transports (0..4) */
   int pt;          /* model.xml <relaxation type="PT">: analytic p-T relaxation after the pressure one */
+  int nstretch[3]; /* stretch zones per axis (0: uniform cells of l / n) */
+  ecgo_stretch stretch[3][ECGO_MAX_STRETCH];
 } ecgo_case;
 
 typedef struct {

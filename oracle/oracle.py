@@ -32,12 +32,20 @@ class Eos(C.Structure):
                 ("cv", C.c_double), ("eref", C.c_double), ("sref", C.c_double)]
 
 
+MAX_STRETCH = 8
+
+
+class Stretch(C.Structure):
+    _fields_ = [("start", C.c_double), ("end", C.c_double), ("factor", C.c_double), ("ncells", C.c_int)]
+
+
 class Case(C.Structure):
     _fields_ = [("model", C.c_int), ("nphases", C.c_int), ("alpha_null", C.c_int), ("order", C.c_int),
                 ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("cfl", C.c_double),
                 ("lim", C.c_int * 4), ("ptmu", C.c_int), ("ptmu_liq", C.c_int), ("ptmu_vap", C.c_int),
-                ("eos", Eos * 3), ("bc", C.c_int * 6), ("ntr", C.c_int), ("pt", C.c_int)]
+                ("eos", Eos * 3), ("bc", C.c_int * 6), ("ntr", C.c_int), ("pt", C.c_int),
+                ("nstretch", C.c_int * 3), ("stretch", (Stretch * MAX_STRETCH) * 3)]
 
 
 class Stats(C.Structure):
@@ -124,16 +132,20 @@ def make_case(case) -> Case:
         c.bc[i] = BC_CODE[b.upper()]
     c.ntr = len(case.transports or [])
     c.pt = 1 if getattr(case, "pt_relaxation", False) else 0
+    for a, ax in enumerate("xyz"):
+        zones = (getattr(case, "stretch", None) or {}).get(ax) or []
+        if int(case.cells[a]) <= 1:
+            zones = []
+        c.nstretch[a] = len(zones)
+        for z, (s0, s1, f, m) in enumerate(zones):
+            c.stretch[a][z] = Stretch(float(s0), float(s1), float(f), int(m))
     return c
 
 
 def cell_centres(case) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
-    """Cell centres (i+0.5)*d per axis, in cell index order (src/Meshes/MeshCartesian.cpp:168)."""
-    nx, ny, nz = case.cells
-    lx, ly, lz = case.lengths
-    xs = (np.arange(nx) + 0.5) * (lx / nx)
-    ys = (np.arange(ny) + 0.5) * (ly / ny)
-    zs = (np.arange(nz) + 0.5) * (lz / nz)
+    """Cell centres per axis -- (i+0.5)*d, or the stretched centres -- in cell index order
+    (src/Meshes/MeshCartesian.cpp:168-210)."""
+    xs, ys, zs = (case.axis_cells(a)[1] for a in range(3))
     Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
     return X.ravel(), Y.ravel(), Z.ravel()
 

@@ -123,6 +123,34 @@ def golden_cases():
     c.interface_limiter, c.interface_vf_limiter = "superbee", "THINC"
     g["ptueq_bubble2d_thinc"] = c
     g["ptueq_bubble3d_o2"] = cases.ptueq_bubble_2d(n=10, nz=6, iterations=4, name="ptueqBubble3D")
+    # stretched meshes (mesh.xml meshStretching, MeshCartesian::meshStretching / stretchZone::stretching):
+    # a uniform zone then a geometric one (and the reverse), per axis
+    g.update(stretched_cases())
+    return g
+
+
+def stretched_cases():
+    g = {}
+    c = cases.shock_tube_1d(ncells=100, iterations=60, order="vanleer", name="tubeStretch")
+    c.stretch = {"x": [(0.0, 0.6, 1.0, 60), (0.6, 1.0, 1.04, 40)]}
+    g["tube1d_stretch_o2"] = c
+    c = cases.shock_tube_1d(ncells=90, iterations=40, name="tubeStretchO1")
+    c.stretch = {"x": [(0.0, 0.3, 0.95, 30), (0.3, 1.0, 1.0, 60)]}
+    g["tube1d_stretch_o1"] = c
+    c = cases.shock_bubble_2d(n=24, iterations=10, name="bubbleStretch")
+    c.cells = (28, 26, 1)
+    c.stretch = {"x": [(0.0, 0.004, 1.0, 12), (0.004, 0.01, 1.05, 16)],
+                 "y": [(0.0, 0.003, 0.93, 8), (0.003, 0.007, 1.0, 10), (0.007, 0.01, 1.08, 8)]}
+    c.boundaries = ["wall", "nonReflecting", "symmetry", "nonReflecting"]
+    g["bubble2d_stretch_o2"] = c
+    c = cases.cavity_collapse_3d(n=10, iterations=4, ninclusions=5, radius_cells=(2.0, 3.0), name="cavityStretch")
+    c.cells = (10, 11, 12)
+    c.stretch = {"y": [(0.0, 0.005, 1.0, 5), (0.005, 0.01, 1.1, 6)], "z": [(0.0, 0.01, 0.95, 12)]}
+    g["cavity3d_stretch_o2"] = c
+    c = cases.euler_blast_2d(n=20, iterations=12, name="eulerStretch")
+    c.cells = (22, 20, 1)
+    c.stretch = {"x": [(0.0, c.lengths[0] / 2, 1.0, 10), (c.lengths[0] / 2, c.lengths[0], 1.06, 12)]}
+    g["euler2d_stretch_o2"] = c
     return g
 
 

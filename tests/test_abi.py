@@ -130,3 +130,47 @@ def test_transports_read_and_filled(tmp_path):
     ref = oracle.initial_fields(case)["tr"]
     assert np.array_equal(np.stack(f[-2:]), ref)
     assert set(np.unique(f[-2])) <= {0.0, 1.0} and set(np.unique(f[-1])) <= {0.25, 2.0}
+
+
+def test_stretched_mesh_read_and_filled(tmp_path):
+    """mesh.xml meshStretching: zones per axis (Input::inputMesh :460-520), the axis' cells their sum,
+    and the initial fill at the stretched cell centres (the oracle's restatement of
+    MeshCartesian::meshStretching, pinned on the reference's own fixtures)."""
+    from tests.golden.make_golden import stretched_cases
+    for key, case in stretched_cases().items():
+        d = case.write(str(tmp_path / key))
+        inp = api.Input(d, os.path.join(str(tmp_path / key), "libEOS"))
+        assert list(inp.case.ncells) == [int(v) for v in case.cells], key
+        for a, ax in enumerate("xyz"):
+            zones = (case.stretch or {}).get(ax) or []
+            assert inp.case.nstretch[a] == len(zones), key
+            for z, (s0, s1, f, m) in enumerate(zones):
+                zr = inp.case.stretch[a][z]
+                assert (zr.start, zr.end, zr.factor, zr.ncells) == (s0, s1, f, m)
+        f = inp.fill()
+        ini = oracle.initial_fields(case)
+        if case.model.upper() == "EULER":
+            assert np.array_equal(f[0], np.ravel(ini["rho"])), key
+        else:
+            assert np.array_equal(np.stack(f[:case.nphases]), ini["alpha"]), key
+            assert np.array_equal(np.stack(f[case.nphases:2 * case.nphases]), ini["rho"]), key
+
+
+def test_stretch_zones_are_checked_without_gpu_work():
+    """Zones that do not start at 0, leave gaps, miss the axis length or the axis' cells are refused
+    (stretchZone::verifyStretching src/Meshes/stretchZone.cpp:74-93) before any device work."""
+    base = api.case_from_spec(cases.shock_tube_1d(ncells=100, iterations=1, order="vanleer"))
+    h = api.C.c_void_p()
+
+    def zones(*zs):
+        c = api.Case.from_buffer_copy(base)
+        c.nstretch[0] = len(zs)
+        for i, z in enumerate(zs):
+            c.stretch[0][i] = api.StretchZone(*z)
+        return api.lib().ecg_create(api.C.byref(c), api.C.byref(h))
+
+    assert zones((0.1, 1.0, 1.0, 100)) == 1               # does not start at 0
+    assert zones((0.0, 0.5, 1.0, 50), (0.6, 1.0, 1.0, 50)) == 1  # gap
+    assert zones((0.0, 0.9, 1.0, 100)) == 1               # does not reach the length
+    assert zones((0.0, 1.0, 1.05, 90)) == 1               # 90 cells on a 100-cell axis
+    assert not h.value

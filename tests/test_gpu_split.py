@@ -39,7 +39,16 @@ def _walls3d():
     return c
 
 
+def _stretched():
+    c = cases.shock_bubble_2d(n=24, iterations=12, name="splitStretch")
+    c.cells = (50, 44, 1)
+    c.stretch = {"x": [(0.0, 0.005, 1.0, 20), (0.005, 0.01, 1.04, 30)], "y": [(0.0, 0.01, 0.97, 44)]}
+    c.boundaries = ["symmetry", "nonReflecting", "wall", "nonReflecting"]
+    return c
+
+
 SPLIT_CASES = {
+    "bubble2d_stretched_walls": _stretched,
     "bubble2d_vanleer_ragged": lambda: cases.shock_bubble_2d(n=70, iterations=20, name="splitBubble"),
     "bubble2d_thinc_generic": _thinc,
     "bubble2d_walls_o2": _walls2d,

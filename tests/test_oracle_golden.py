@@ -16,7 +16,9 @@ KEYS = ["tube1d_o1_full", "tube1d_o2_vanleer", "tube1d_alphanull", "tube1d_nasg_
         "tube1d_transport_o2", "bubble2d_transport", "tube1d_transport_o1", "euler1d_transport_o2", "tube1d_pt_o1",
         "bubble2d_pt", "ptueq_tube_o2", "ptueq_tube_o1", "ptueq_tube_wall_o1",
         "ptueq_bubble2d_o2", "ptueq_bubble2d_o1_sym", "ptueq_bubble2d_thinc", "ptueq_bubble3d_o2",
-        "euler2d_o2_walls", "euler2d_o1", "euler3d_o2"]
+        "euler2d_o2_walls", "euler2d_o1", "euler3d_o2",
+        # stretched meshes
+        "tube1d_stretch_o2", "tube1d_stretch_o1", "bubble2d_stretch_o2", "cavity3d_stretch_o2", "euler2d_stretch_o2"]
 
 
 @pytest.mark.parametrize("key", KEYS)
@@ -43,7 +45,8 @@ def test_oracle_matches_reference(key, golden_cases):
 
 
 @pytest.mark.parametrize("key", ["tube1d_o1_full", "bubble2d_o2", "cavity3d_o2", "expansion2d_ptmu", "euler1d_o1",
-                                 "ptueq_bubble2d_o2", "ptueq_bubble3d_o2"])
+                                 "ptueq_bubble2d_o2", "ptueq_bubble3d_o2", "bubble2d_stretch_o2",
+                                 "cavity3d_stretch_o2"])
 def test_initial_fill_matches_reference(key, golden_cases):
     _, g = load_golden(key)
     case = golden_cases[key]
