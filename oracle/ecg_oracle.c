@@ -23,6 +23,14 @@
 #else
 #define ECGO_LOG log
 #endif
+/* pow of the isentropic star pressure: the host libm's (the default build), or with last-ulp changes in
+ * 1 call in 100 (the sensitivity variant libecg_oracle_powulp.so, -DECGO_POW_ULP; see ecg_powulp.h). */
+#ifdef ECGO_POW_ULP
+#include "ecg_powulp.h"
+#define ECGO_POW ecgo_pow_ulp
+#else
+#define ECGO_POW pow
+#endif
 
 #define NP_MAX 3
 #define NT_MAX 4   /* passive transports (model.xml numberTransports) */
@@ -135,11 +143,11 @@ static double nonzero(double a, double eps) { /* Tools::returnNonZeroValue, src/
 
 static double eos_p_isentropic(const ecgo_eos* q, double eps, double p0, double rho0, double rho1) {
   switch (q->type) {
-    case ECGO_EOS_IG: return p0 * pow(rho1 / omax(rho0, eps), q->gamma);
-    case ECGO_EOS_SG: return (p0 + q->pinf) * pow(rho1 / omax(rho0, eps), q->gamma) - q->pinf;
+    case ECGO_EOS_IG: return p0 * ECGO_POW(rho1 / omax(rho0, eps), q->gamma);
+    case ECGO_EOS_SG: return (p0 + q->pinf) * ECGO_POW(rho1 / omax(rho0, eps), q->gamma) - q->pinf;
     default:
-      return (p0 + q->pinf) * pow(rho1 / omax(rho0, eps), q->gamma) *
-                 pow((1. - rho0 * q->b) / (1. - rho1 * q->b), q->gamma) - q->pinf;
+      return (p0 + q->pinf) * ECGO_POW(rho1 / omax(rho0, eps), q->gamma) *
+                 ECGO_POW((1. - rho0 * q->b) / (1. - rho1 * q->b), q->gamma) - q->pinf;
   }
 }
 

@@ -18,9 +18,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libecg_oracle.so")
-# the same restatement with a correctly rounded ln in the saturation solve (ecg_crlog.h): the
-# sensitivity variant, which measures how far a last-ulp change of ln travels through a run
-LIB_PATH_CRLOG = os.path.join(HERE, "_ref", "libecg_oracle_crlog.so")
+# Sensitivity variants of the same restatement, which measure how far last-ulp changes of the math
+# library travel through a run: "crlog", a correctly rounded ln in the saturation solve (ecg_crlog.h);
+# "powulp", pow of the isentropic star pressure moved by one ulp in 1 call in 100 (ecg_powulp.h).
+VARIANT_PATHS = {"crlog": os.path.join(HERE, "_ref", "libecg_oracle_crlog.so"),
+                 "powulp": os.path.join(HERE, "_ref", "libecg_oracle_powulp.so")}
 
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
@@ -63,16 +65,17 @@ def build() -> str:
     return LIB_PATH
 
 
-def lib(crlog: bool = False):
-    """The oracle library (crlog: the variant with a correctly rounded ln in the saturation solve)."""
+def lib(variant: Optional[str] = None):
+    """The oracle library, or one of its sensitivity variants ("crlog", "powulp")."""
     global _lib
-    if crlog:
-        if "crlog" not in _libs:
+    if variant:
+        if variant not in _libs:
+            path = VARIANT_PATHS[variant]
             src = os.path.join(HERE, "ecg_oracle.c")
-            if not os.path.exists(LIB_PATH_CRLOG) or os.path.getmtime(LIB_PATH_CRLOG) < os.path.getmtime(src):
+            if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
                 build()
-            _libs["crlog"] = _declare(C.CDLL(LIB_PATH_CRLOG))
-        return _libs["crlog"]
+            _libs[variant] = _declare(C.CDLL(path))
+        return _libs[variant]
     if _lib is None:
         src = os.path.join(HERE, "ecg_oracle.c")
         if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
@@ -228,9 +231,9 @@ def initial_fields(case) -> Dict[str, np.ndarray]:
 class Sim:
     """One oracle simulation; mirrors the reference run loop (dt starts at 1e-15, src/Run.cpp:38)."""
 
-    def __init__(self, case, fields: Optional[Dict[str, np.ndarray]] = None, crlog: bool = False):
+    def __init__(self, case, fields: Optional[Dict[str, np.ndarray]] = None, variant: Optional[str] = None):
         self.case = case
-        self._L = lib(crlog)
+        self._L = lib(variant)
         self.c = make_case(case)
         f = fields or initial_fields(case)
         self.n = case.ncells
