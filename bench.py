@@ -70,6 +70,8 @@ def make_case(config: str, size: int | None):
 def seed_model_path(config: str, nphases: int) -> str:
     """The shipped seed model of a workload family (1D tubes have their own)."""
     models = os.path.join(ROOT, "ecogen_b200", "models")
+    if config == "c5":  # the (p*, T) seed of the p-T-mu saturation solve
+        return os.path.join(models, "seed_ptmu.npz")
     if config in ("c1", "c4"):
         p = os.path.join(models, "seed_np2_tube1d.npz")
         if os.path.exists(p):
@@ -600,6 +602,12 @@ def main():
                   "plain_newton_evals_per_relaxation": st_ref.newton_evals / max(1, st_ref.relax_calls),
                   "seeded": st3.seeded, "seed_rejected": st3.seed_rejected, "fallback": st3.newton_fallback,
                   "field_rel_l1_vs_plain": diff, "model": os.path.relpath(model_path, ROOT)}
+        if case.ptmu is not None:  # the p-T-mu saturation solve: iterations with and without the seed
+            seeded.update({"ptmu_seeded": st3.ptmu_seeded, "ptmu_seed_rejected": st3.ptmu_seed_rejected,
+                           "ptmu_outer_iters_per_solve": st3.ptmu_outer_iters / max(1, st3.ptmu_solves),
+                           "plain_ptmu_outer_iters_per_solve": st_ref.ptmu_outer_iters / max(1, st_ref.ptmu_solves),
+                           "tsat_iters_per_solve": st3.ptmu_tsat_iters / max(1, st3.ptmu_solves),
+                           "plain_tsat_iters_per_solve": st_ref.ptmu_tsat_iters / max(1, st_ref.ptmu_solves)})
         ref_ctx.close()
         ctx3.close()
 

@@ -58,7 +58,8 @@ class StepStats(C.Structure):
                 ("seed_rejected", C.c_int64), ("ptmu_errors", C.c_int64), ("nonfinite_cells", C.c_int64),
                 ("newton_hist", C.c_int64 * 16), ("ptmu_solves", C.c_int64), ("ptmu_outer_iters", C.c_int64),
                 ("ptmu_outer_max", C.c_int64), ("ptmu_tsat_calls", C.c_int64), ("ptmu_tsat_iters", C.c_int64),
-                ("ptmu_tsat_max", C.c_int64), ("ptmu_outer_hist", C.c_int64 * 16)]
+                ("ptmu_tsat_max", C.c_int64), ("ptmu_outer_hist", C.c_int64 * 16), ("ptmu_seeded", C.c_int64),
+                ("ptmu_seed_rejected", C.c_int64), ("bounds_violations", C.c_int64)]
 
     def as_dict(self) -> Dict[str, object]:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("newton_hist", "ptmu_outer_hist")}
@@ -75,7 +76,8 @@ class Mlp(C.Structure):
     _fields_ = [("n_in", C.c_int32), ("hidden", C.c_int32), ("w1", C.POINTER(C.c_float)),
                 ("b1", C.POINTER(C.c_float)), ("w2", C.POINTER(C.c_float)), ("b2", C.POINTER(C.c_float)),
                 ("w3", C.POINTER(C.c_float)), ("b3", C.c_float), ("in_shift", C.c_float * MLP_MAX_IN),
-                ("in_scale", C.c_float * MLP_MAX_IN), ("out_shift", C.c_float), ("out_scale", C.c_float)]
+                ("in_scale", C.c_float * MLP_MAX_IN), ("out_shift", C.c_float), ("out_scale", C.c_float),
+                ("n_out", C.c_int32), ("b3_1", C.c_float), ("out_shift_1", C.c_float), ("out_scale_1", C.c_float)]
 
 
 _lib = None
@@ -131,6 +133,8 @@ def lib():
                  "ecg_batch_total_cells"):
         getattr(L, name)  # every symbol the header declares must be exported
     L.ecg_trainer_create.argtypes = [C.c_int32, C.c_int32, C.c_uint64, P(vp)]
+    L.ecg_trainer_create_n.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, P(vp)]
+    L.ecg_trainer_set_norm_out1.argtypes = [vp, C.c_float, C.c_float]
     L.ecg_trainer_destroy.argtypes = [vp]
     L.ecg_trainer_epoch.argtypes = [vp, fp, fp, C.c_int64, C.c_int32, C.c_float, C.c_float, fp]
     L.ecg_trainer_grad.argtypes = [vp, fp, fp, C.c_int32, fp, fp, fp, fp, fp, fp, fp]
@@ -341,11 +345,14 @@ class Context:
         check(lib().ecg_record_pairs(self.h, max_pairs, min_evals), "ecg_record_pairs")
 
     def fetch_pairs(self):
+        """Recorded (features, targets): pressure relaxation 3N features and one target; p-T-mu
+        relaxation 8 features and two targets (ln p*, T_sat(p*)), targets then an (n, 2) array."""
         cnt = C.c_int64(0)
         check(lib().ecg_fetch_pairs(self.h, None, None, C.byref(cnt)), "ecg_fetch_pairs")
-        nin = 3 * self.case.nphases
+        ptmu = bool(self.case.ptmu)
+        nin = 8 if ptmu else 3 * self.case.nphases
         x = np.zeros((cnt.value, nin), dtype=np.float32)
-        y = np.zeros(cnt.value, dtype=np.float32)
+        y = np.zeros((cnt.value, 2) if ptmu else cnt.value, dtype=np.float32)
         if cnt.value:
             check(lib().ecg_fetch_pairs(self.h, x.ctypes.data_as(C.POINTER(C.c_float)),
                                         y.ctypes.data_as(C.POINTER(C.c_float)), C.byref(cnt)), "ecg_fetch_pairs")

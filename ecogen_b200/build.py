@@ -60,7 +60,7 @@ def _compile(src: str, extra=None) -> str:
     return obj
 
 
-def build(verbose: bool = False, jobs: int = 8) -> str:
+def build(verbose: bool = False, jobs: int = 8, lib_only: bool = False) -> str:
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     lib_srcs = [s for s in srcs if not os.path.basename(s).startswith("ecogen_main")]
 
@@ -77,6 +77,8 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if lib_only:
+        return LIB
     # measurement probe (FP64 pipe peak for the bench's FP64 roofline), its own library
     probe_src = os.path.join(HERE, "probe", "ecg_fp64_peak.cu")
     if os.path.exists(probe_src):
@@ -100,6 +102,25 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     return LIB
 
 
+BOUNDS_LIB = os.path.join(HERE, "libecg_bounds.so")
+
+
+def build_bounds(verbose: bool = False, jobs: int = 8) -> str:
+    """The bounds-checked library (libecg_bounds.so): every state, face-array and output index of the
+    step kernels is checked, counted in ecg_step_stats.bounds_violations and the access skipped when
+    outside its buffer.  Built with the generic-EOS kernels only (-DECG_NO_EOS_SPECIALIZATION): the
+    EOS-specialised kernels index exactly as the generic ones, and the build is a fraction of the size."""
+    env = dict(os.environ, ECG_BUILD_DIR=os.path.join(HERE, "_build_bounds"), ECG_LIB_OUT=BOUNDS_LIB,
+               ECG_NVCC_EXTRA="-DECG_BOUNDS_CHECK -DECG_NO_EOS_SPECIALIZATION")
+    r = subprocess.run([sys.executable, "-m", "ecogen_b200.build", "--lib-only"], env=env, cwd=ROOT,
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("bounds-checked build failed:\n" + r.stdout[-3000:] + r.stderr[-3000:])
+    if verbose:
+        print("built", BOUNDS_LIB)
+    return BOUNDS_LIB
+
+
 def ptxas_report(src: str) -> str:
     """Register / shared-memory / spill report of one .cu file (nvcc -Xptxas -v)."""
     cmd = [_nvcc()] + ARCH + NVFLAGS + ["-Xptxas", "-v", "-c", src, "-o", os.devnull]
@@ -110,5 +131,7 @@ def ptxas_report(src: str) -> str:
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "ptxas":
         print(ptxas_report(sys.argv[2]))
+    elif len(sys.argv) > 1 and sys.argv[1] == "bounds":
+        build_bounds(verbose=True)
     else:
-        build(verbose=True)
+        build(verbose=True, lib_only="--lib-only" in sys.argv)

@@ -151,70 +151,6 @@ ecg_status cuda_fail(cudaError_t e, const char* what) {
 
 namespace ecg {
 
-// Checks a case against what the library runs (ecg_create and ecg_step_noalloc accept the same cases).
-ecg_status validate_case(const ecg_case* c) {
-  if (!c) { set_error("null case"); return ECG_ERR_INVALID; }
-  if (c->model != ECG_MODEL_KAPILA && c->model != ECG_MODEL_EULER && c->model != ECG_MODEL_PTUEQ) { set_error("unknown model"); return ECG_ERR_INVALID; }
-  if (c->model == ECG_MODEL_PTUEQ) {
-    // MixPTUEq::computePressure: two phases, IG or SG (src/Models/PTUEq/MixPTUEq.cpp:96-99)
-    if (c->nphases != 2) { set_error("the temperature-pressure equilibrium model has two phases"); return ECG_ERR_UNSUPPORTED; }
-    for (int k = 0; k < 2; k++)
-      if (c->eos[k].type == ECG_EOS_NASG) { set_error("Only IG and SG permitted in thermal equilibrium model"); return ECG_ERR_UNSUPPORTED; }
-    if (c->ntransports) { set_error("solveRiemannTransportIntern not available for the temperature-pressure equilibrium model"); return ECG_ERR_UNSUPPORTED; }
-    if (c->ptmu || c->pt_relaxation) { set_error("relaxations of the temperature-pressure equilibrium model"); return ECG_ERR_UNSUPPORTED; }
-    if (c->alpha_null) { set_error("alphaNull is not an option of the temperature-pressure equilibrium model"); return ECG_ERR_INVALID; }
-    if (c->order == 2)
-      for (int i = 0; i < 6; i++)  // BoundCondWallO2Cartesian::computeSlopes sets phase velocity slopes PhasePTUEq lacks
-        if (c->bc[i] == ECG_BC_SYMMETRY) { set_error("MUSCL symmetry sides of the temperature-pressure equilibrium model (setU not available)"); return ECG_ERR_UNSUPPORTED; }
-  }
-  if (c->model == ECG_MODEL_KAPILA && (c->nphases < 2 || c->nphases > 3)) { set_error("Kapila needs 2 or 3 phases"); return ECG_ERR_UNSUPPORTED; }
-  if (c->model == ECG_MODEL_EULER && c->nphases != 1) { set_error("Euler has one phase"); return ECG_ERR_INVALID; }
-  if (c->order != 1 && c->order != 2) { set_error("order must be 1 or 2"); return ECG_ERR_INVALID; }
-  for (int i = 0; i < 3; i++)
-    if (c->ncells[i] < 1 || !(c->length[i] > 0.)) { set_error("bad mesh"); return ECG_ERR_INVALID; }
-  if (c->ncells[0] <= 1) { set_error("Number of cells in the x-direction has to be superior to 1"); return ECG_ERR_INVALID; }
-  if (c->ncells[2] > 1 && c->ncells[1] <= 1) { set_error("z cells without y cells"); return ECG_ERR_INVALID; }
-  for (int i = 0; i < 4; i++)
-    if (c->limiter[i] < 0 || c->limiter[i] > ECG_LIM_THINC) { set_error("bad limiter"); return ECG_ERR_INVALID; }
-  
-  for (int i = 0; i < 6; i++)
-    if (c->bc[i] != ECG_BC_NONREFLECTING && c->bc[i] != ECG_BC_SYMMETRY) { set_error("bad boundary condition"); return ECG_ERR_INVALID; }
-  if (c->ntransports < 0) { set_error("negative number of transports"); return ECG_ERR_INVALID; }
-  if (c->ntransports > 2) { set_error("more than two passive transports"); return ECG_ERR_UNSUPPORTED; }
-  if (c->pt_relaxation) {
-    if (c->model != ECG_MODEL_KAPILA || c->nphases != 2 || c->ptmu) { set_error("PT relaxation: two Kapila phases, without PTMu"); return ECG_ERR_UNSUPPORTED; }
-    for (int k = 0; k < 2; k++)
-      if (c->eos[k].type == ECG_EOS_NASG) { set_error("PT relaxation needs IG or SG phases"); return ECG_ERR_UNSUPPORTED; }
-  }
-  if (c->ptmu && (c->model != ECG_MODEL_KAPILA || c->nphases != 2)) { set_error("PTMu needs two phases"); return ECG_ERR_INVALID; }
-  if (c->ptmu) {
-    if (c->ptmu_liquid < 0 || c->ptmu_liquid > 1 || c->ptmu_vapor < 0 || c->ptmu_vapor > 1 ||
-        c->ptmu_liquid == c->ptmu_vapor) { set_error("PTMu liquid / vapour phase indices"); return ECG_ERR_INVALID; }
-    // Mixture::computeTsat (src/Models/Mixture.cpp:62-63): IG and SG phases only
-    for (int k = 0; k < 2; k++)
-      if (c->eos[k].type == ECG_EOS_NASG) { set_error("Only IG and SG permitted in thermal equilibrium model: MixPTUEq::computeTsat"); return ECG_ERR_UNSUPPORTED; }
-  }
-  int dim = (c->ncells[0] != 1) + (c->ncells[1] != 1) + (c->ncells[2] != 1);
-  if (c->ptmu && dim == 3) { set_error("PTMu on 3D meshes is not built"); return ECG_ERR_UNSUPPORTED; }
-  for (int a = 0; a < 3; a++) {  // mesh stretching (stretchZone::verifyStretching src/Meshes/stretchZone.cpp:74-93)
-    const int nz = c->nstretch[a];
-    if (nz < 0 || nz > ECG_MAX_STRETCH_ZONES) { set_error("bad number of stretch zones"); return ECG_ERR_INVALID; }
-    if (nz == 0 || c->ncells[a] <= 1) continue;
-    int cells = 0;
-    for (int z = 0; z < nz; z++) {
-      const ecg_stretch_zone& st = c->stretch[a][z];
-      if (st.ncells < 1 || !(st.end > st.start) || !(st.factor > 0.)) { set_error("bad stretch zone"); return ECG_ERR_INVALID; }
-      if (z == 0 ? st.start != 0. : st.start != c->stretch[a][z - 1].end) { set_error("stretch zones are not contiguous from 0"); return ECG_ERR_INVALID; }
-      cells += st.ncells;
-    }
-    if (c->stretch[a][nz - 1].end != c->length[a]) { set_error("stretch zones do not end at the domain length"); return ECG_ERR_INVALID; }
-    if (cells != c->ncells[a]) { set_error("stretch zone cells do not add up to the axis' cells"); return ECG_ERR_INVALID; }
-  }
-  int64_t n = (int64_t)c->ncells[0] * c->ncells[1] * c->ncells[2];
-  if (n > (int64_t)1 << 31) { set_error("more than 2^31 cells"); return ECG_ERR_TOO_LARGE; }
-  return ECG_OK;
-}
-
 }  // namespace ecg
 
 namespace {
@@ -370,6 +306,9 @@ void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
   st->ptmu_tsat_iters = (int64_t)d.ptmu_tsat_iters;
   st->ptmu_tsat_max = (int64_t)d.ptmu_tsat_max;
   for (int i = 0; i < 16; i++) st->ptmu_outer_hist[i] = (int64_t)d.ptmu_hist[i];
+  st->ptmu_seeded = (int64_t)d.ptmu_seeded;
+  st->ptmu_seed_rejected = (int64_t)d.ptmu_seed_rejected;
+  st->bounds_violations = (int64_t)d.bounds_violations;
 }
 }  // namespace ecg
 
@@ -379,8 +318,10 @@ namespace {
 
 namespace ecg {
 
-// B fragments of the seed model's two hidden layers (layout of MlpDev, ecg_mlp_device.cuh).
-__global__ void k_mlp_pack(const float* __restrict__ W, int nin, MlpDev* out) {
+// B fragments of the seed model's two hidden layers (layout of MlpDev, ecg_mlp_device.cuh).  Packed
+// parameters: w1 b1 w2 b2 w3 b3 in_shift in_scale out_shift out_scale, then for a second output
+// w3b b3b out_shift_1 out_scale_1.
+__global__ void k_mlp_pack(const float* __restrict__ W, int nin, int nout, MlpDev* out) {
   const int H = MLP_H;
   const float* w1 = W;
   const float* b1 = w1 + H * nin;
@@ -390,6 +331,7 @@ __global__ void k_mlp_pack(const float* __restrict__ W, int nin, MlpDev* out) {
   const float* b3 = w3 + H;
   const float* ish = b3 + 1;
   const float* isc = ish + nin;
+  const float* w3b = isc + nin + 2;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int i = tid; i < 8 * 32; i += nth) {
     const int nt = i / 32, lane = i % 32, g = lane >> 2, t = lane & 3, n = 8 * nt + g;
@@ -409,6 +351,7 @@ __global__ void k_mlp_pack(const float* __restrict__ W, int nin, MlpDev* out) {
     out->b1[i] = b1[i];
     out->b2[i] = b2[i];
     out->w3[i] = w3[i];
+    out->w3b[i] = nout > 1 ? w3b[i] : 0.f;
   }
   for (int i = tid; i < 16; i += nth) {
     out->ish[i] = i < nin ? ish[i] : 0.f;
@@ -419,21 +362,28 @@ __global__ void k_mlp_pack(const float* __restrict__ W, int nin, MlpDev* out) {
     out->osh = isc[nin];
     out->osc = isc[nin + 1];
     out->pad = 0.f;
+    out->b3b = nout > 1 ? w3b[H] : 0.f;
+    out->osh2 = nout > 1 ? w3b[H + 1] : 0.f;
+    out->osc2 = nout > 1 ? w3b[H + 2] : 0.f;
+    out->pad2 = 0.f;
   }
 }
 
-cudaError_t mlp_install(const float* d_params, int nin, MlpDev* d_out, cudaStream_t stream) {
-  k_mlp_pack<<<4, 256, 0, stream>>>(d_params, nin, d_out);
+cudaError_t mlp_install(const float* d_params, int nin, int nout, MlpDev* d_out, cudaStream_t stream) {
+  k_mlp_pack<<<4, 256, 0, stream>>>(d_params, nin, nout, d_out);
   return cudaGetLastError();
 }
 
-ecg_status mlp_upload(const ecg_mlp* m, int np, MlpDev** dev, cudaStream_t stream) {
-  if (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * np) {
-    set_error("seed model shape must be 3*nphases -> 64 -> 64 -> 1");
+ecg_status mlp_upload(const ecg_mlp* m, int np, bool ptmu, MlpDev** dev, cudaStream_t stream) {
+  const int nout = m->n_out > 1 ? m->n_out : 1;
+  if (ptmu ? (m->hidden != ECG_MLP_HIDDEN || m->n_in != PTMU_NIN || nout != 2)
+           : (m->hidden != ECG_MLP_HIDDEN || m->n_in != 3 * np || nout != 1)) {
+    set_error(ptmu ? "p-T-mu seed model shape must be 8 -> 64 -> 64 -> 2"
+                   : "seed model shape must be 3*nphases -> 64 -> 64 -> 1");
     return ECG_ERR_INVALID;
   }
   const int nin = m->n_in, H = ECG_MLP_HIDDEN;
-  std::vector<float> pk((size_t)mlp_packed_size(nin));
+  std::vector<float> pk((size_t)mlp_packed_size(nin) + (nout > 1 ? H + 3 : 0));
   float* q = pk.data();
   std::memcpy(q, m->w1, sizeof(float) * H * nin); q += H * nin;
   std::memcpy(q, m->b1, sizeof(float) * H); q += H;
@@ -445,11 +395,17 @@ ecg_status mlp_upload(const ecg_mlp* m, int np, MlpDev** dev, cudaStream_t strea
   for (int i = 0; i < nin; i++) *q++ = m->in_scale[i];
   *q++ = m->out_shift;
   *q++ = m->out_scale;
+  if (nout > 1) {
+    std::memcpy(q, m->w3 + H, sizeof(float) * H); q += H;
+    *q++ = m->b3_1;
+    *q++ = m->out_shift_1;
+    *q++ = m->out_scale_1;
+  }
   float* tmp = nullptr;
   cudaError_t e = cudaMalloc(&tmp, sizeof(float) * pk.size());
   if (e == cudaSuccess && !*dev) e = cudaMalloc(dev, sizeof(MlpDev));
   if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, pk.data(), sizeof(float) * pk.size(), cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = mlp_install(tmp, nin, *dev, stream);
+  if (e == cudaSuccess) e = mlp_install(tmp, nin, nout, *dev, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   cudaFree(tmp);
   if (e != cudaSuccess) {
@@ -923,7 +879,7 @@ extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
   }
   if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
   if (x->c.ntransports > 0) { set_error("the seeded kernels run without passive transports"); return ECG_ERR_UNSUPPORTED; }
-  return mlp_upload(m, x->np, &x->mlp, x->stream);
+  return mlp_upload(m, x->np, x->c.ptmu != 0, &x->mlp, x->stream);
 }
 
 extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs, int32_t min_evals) {
@@ -937,9 +893,9 @@ extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs, int32_t mi
   x->rec_count = nullptr;
   x->rec_max = 0;
   if (max_pairs == 0) return ECG_OK;
-  const int nin = 3 * x->np;
+  const int nin = x->c.ptmu ? PTMU_NIN : 3 * x->np, nout = x->c.ptmu ? 2 : 1;
   ECG_CUDA(cudaMalloc(&x->rec_x, sizeof(float) * nin * (size_t)max_pairs));
-  ECG_CUDA(cudaMalloc(&x->rec_y, sizeof(float) * (size_t)max_pairs));
+  ECG_CUDA(cudaMalloc(&x->rec_y, sizeof(float) * nout * (size_t)max_pairs));
   ECG_CUDA(cudaMalloc(&x->rec_count, sizeof(unsigned long long)));
   ECG_CUDA(cudaMemset(x->rec_count, 0, sizeof(unsigned long long)));
   x->rec_max = (unsigned long long)max_pairs;
@@ -954,8 +910,8 @@ extern "C" ecg_status ecg_fetch_pairs(ecg_ctx* x, float* features, float* target
   ECG_CUDA(cudaStreamSynchronize(x->stream));
   if (c > x->rec_max) c = x->rec_max;
   *count = (int64_t)c;
-  const int nin = 3 * x->np;
+  const int nin = x->c.ptmu ? PTMU_NIN : 3 * x->np, nout = x->c.ptmu ? 2 : 1;
   if (features && c) ECG_CUDA(cudaMemcpy(features, x->rec_x, sizeof(float) * nin * c, cudaMemcpyDeviceToHost));
-  if (targets && c) ECG_CUDA(cudaMemcpy(targets, x->rec_y, sizeof(float) * c, cudaMemcpyDeviceToHost));
+  if (targets && c) ECG_CUDA(cudaMemcpy(targets, x->rec_y, sizeof(float) * nout * c, cudaMemcpyDeviceToHost));
   return ECG_OK;
 }

@@ -695,7 +695,7 @@ extern "C" ecg_status ecg_batch_set_seed_model(ecg_batch* b, const ecg_mlp* m) {
     b->mlp = nullptr;
     return ECG_OK;
   }
-  return mlp_upload(m, b->np, &b->mlp, b->stream);
+  return mlp_upload(m, b->np, false, &b->mlp, b->stream);
 }
 
 extern "C" ecg_status ecg_batch_set_shape(ecg_batch* b, int32_t tile, int32_t threads) {

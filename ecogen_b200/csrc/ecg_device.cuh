@@ -600,11 +600,15 @@ struct PtmuCount {
   unsigned int tsat_calls = 0;  // T_sat(p) solves (pure-phase tests included)
   unsigned int tsat_iters = 0;  // their Newton iterations
   unsigned int tsat_max = 0;    // the largest of them
+  unsigned int seeded = 0;      // 1 when the saturation Newton started from a learned (p*, T) seed
+  unsigned int rejected = 0;    // 1 when a learned seed was rejected (plain start)
+  double pstar = 0., tsat = 0.;  // converged p* and T_sat(p*) of the saturation Newton (recording)
 };
 
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
+// T0 > 0: the Newton iteration starts there instead of at 0.1 B / C (a seeded p-T-mu relaxation).
 __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
-                                               bool& err, PtmuCount* pc = nullptr) {
+                                               bool& err, PtmuCount* pc = nullptr, double T0 = -1.) {
   double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
   double gV = V.gamma, piV = (V.type == ECG_EOS_IG) ? 0. : V.pinf, cvV = V.cv, e0V = V.eref, s0V = V.sref;
   double A = (gL * cvL - gV * cvV + s0V - s0L) / (gV * cvV - cvV);
@@ -612,7 +616,7 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
   double C = (gV * cvV - gL * cvL) / (gV * cvV - cvV);
   double D = (gL * cvL - cvL) / (gV * cvV - cvV);
   int iteration = 0;
-  double Tsat = 0.1 * B / C, f = 0., df = 1.;
+  double Tsat = (T0 > 0.) ? T0 : 0.1 * B / C, f = 0., df = 1.;
   // ln(p + pInf) of both phases do not depend on the iterate: evaluated once per solve (the same
   // values enter the same sum, so f has the bits of the reference's per-iteration evaluation)
   const double lnV = cr_log(p + piV), lnL = cr_log(p + piL);
@@ -666,10 +670,14 @@ __device__ __forceinline__ double eos_rhoe_sat(const EosParams& q, double p, dou
 // mixture density and internal energy the cell holds at that point (from buildPrim).  Returns true
 // when the phases were updated (the reference then calls fulfillState, so the mixture density
 // is recomputed from the new phases).
+//
+// Seeded form (p_seed > 0): the Newton iteration on p* starts at p_seed instead of sum_k alpha_k p_k, the
+// T_sat(p) solves start at T_seed (pure-phase tests and the first Newton iteration) and then at the
+// previous iteration's T_sat; every loop still stops at |f| <= 1e-10.
 template <int NP>
 __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap, double pcrit, double a[NP],
                                            double r[NP], double p[NP], double rhomix, double emix, bool& err,
-                                           PtmuCount* pc = nullptr) {
+                                           PtmuCount* pc = nullptr, double p_seed = -1., double T_seed = -1.) {
   const EosParams& EL = M.eos[liq];
   const EosParams& EV = M.eos[vap];
   double pStar = 0., Tsat, dTsat = 0.;
@@ -680,7 +688,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pv = eos_p(EV, M.eps, rho, emix);
   double Tv = eos_T(EV, M.eps, rho, pv);
   if (pv > 0) {
-    Tsat = compute_tsat(EL, EV, pv, &dTsat, err, pc);
+    Tsat = compute_tsat(EL, EV, pv, &dTsat, err, pc, T_seed);
     if (Tv >= Tsat) {
       a[vap] = 1.;
       a[liq] = 0.;
@@ -692,7 +700,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pl = eos_p(EL, M.eps, rho, emix);
   double Tl = eos_T(EL, M.eps, rho, pl);
   if (pl > 0.) {
-    Tsat = compute_tsat(EL, EV, pl, &dTsat, err, pc);
+    Tsat = compute_tsat(EL, EV, pl, &dTsat, err, pc, T_seed);
     if (Tl <= Tsat) {
       a[liq] = 1.;
       a[vap] = 0.;
@@ -705,6 +713,8 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double rhoeLSat, rhoeVSat, drhoeLSat, drhoeVSat;
   int iteration = 0;
   double f = 0., df = 1.;
+  double Tstart = T_seed;  // start of the next T_sat solve (seeded form)
+  if (p_seed > 0.) pStar = p_seed;
   do {
     pStar -= f / df;
     iteration++;
@@ -714,7 +724,8 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
     }
 #pragma unroll
     for (int k = 0; k < NP; k++) pStar = eos_fix_p(M.eos[k], pStar);
-    Tsat = compute_tsat(EL, EV, pStar, &dTsat, err, pc);
+    Tsat = compute_tsat(EL, EV, pStar, &dTsat, err, pc, Tstart);
+    if (p_seed > 0.) Tstart = Tsat;
     rhoLSat = eos_rho_sat(EL, M.eps, pStar, Tsat, dTsat, &drhoLSat);
     rhoVSat = eos_rho_sat(EV, M.eps, pStar, Tsat, dTsat, &drhoVSat);
     aLSat = (rho - rhoVSat) / (rhoLSat - rhoVSat);
@@ -734,6 +745,8 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   if (pc) {
     pc->solve = 1;
     pc->outer = (unsigned int)iteration;
+    pc->pstar = pStar;
+    pc->tsat = Tsat;
   }
   a[liq] = aLSat;
   r[liq] = rhoLSat;

@@ -332,7 +332,46 @@ struct SeedGate {
   double aS[NP], rS[NP];
   double seed;
   bool applies, hard;
+  // p-T-mu relaxation: the network's (p*, T) start and the features it was evaluated on
+  double ptmu_p = -1., ptmu_T = -1.;
+  float ptmu_x[PTMU_NIN];
 };
+
+// Mixture internal energy of the rebuilt state, sum_k Y_k e_k(rho_k, p_k) (MixUEq::computeMixtureVariables
+// :136), which RelaxationPTMu reads before any fulfillState.
+template <int NP>
+__device__ __forceinline__ double rebuilt_emix(const Model<NP>& M, const double a[NP], const double r[NP],
+                                               const double p[NP], double rhomix) {
+  double emix = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    double Y = a[k] * r[k] / dmax(rhomix, M.eps);
+    emix += Y * eos_e(M.eos[k], M.eps, r[k], p[k]);
+  }
+  return emix;
+}
+
+// The learned (p*, T) start of the p-T-mu relaxation of every cell of the warp (all lanes call it;
+// `active` marks a cell): features of the rebuilt state, the network, then the checks that keep a seed
+// (finite, positive, p* below the critical pressure); a rejected seed leaves the plain start.
+template <int NP, int DIM>
+__device__ __forceinline__ void ptmu_seed_gate(const StepParams& P, const Model<NP>& M, bool active,
+                                               const CellPrim<NP, DIM>& cp, SeedGate<NP>& g, CellCounters& cc) {
+  if (active) {
+    const double emix = rebuilt_emix<NP>(M, cp.a, cp.r, cp.pk, cp.rhomix);
+    ptmu_features<NP>(M, P.ptmu_liq, P.ptmu_vap, cp.a, cp.r, cp.pk, cp.rhomix, emix, g.ptmu_x);
+  }
+  double ps = -1., Ts = -1.;
+  mlp_ptmu_seed_warp(P.mlp, active, g.ptmu_x, ps, Ts);
+  g.ptmu_p = g.ptmu_T = -1.;
+  if (!active) return;
+  if (isfinite(ps) && isfinite(Ts) && ps > 0. && ps < P.pcrit && Ts > 0.) {
+    g.ptmu_p = ps;
+    g.ptmu_T = Ts;
+  } else {
+    cc.pc.rejected = 1;
+  }
+}
 
 // First evaluation and the warp-wide seed (all lanes of the warp call it; `active` marks a cell).
 template <int NP, int DIM>
@@ -392,9 +431,12 @@ __device__ __forceinline__ void relax_pt(const Model<NP>& M, double a[NP], doubl
   }
 }
 
+// SEED: with PTMU, the learned (p*, T) start of the p-T-mu relaxation (ptmu_seed_gate), the pressure
+// relaxation plain; without, the learned start of the pressure relaxation (seed_gate).
 template <int NP, int DIM, int PASS, bool PTMU, bool SEED = false, bool XPT = true>
 __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<NP>& M, int64_t nn, int64_t cell,
                                               CellPrim<NP, DIM>& cp, const SeedGate<NP>& g, CellCounters& cc) {
+  constexpr bool kPinfSeed = SEED && !PTMU;
   using FL = Fields<NP, DIM>;
   double* a = cp.a;
   double* r = cp.r;
@@ -409,7 +451,7 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
   for (int k = 0; k < NP; k++) { a0[k] = a[k]; r0[k] = r[k]; p0[k] = pk[k]; }
   double pstar = 0.;
   bool relaxed;
-  if (SEED) {
+  if (kPinfSeed) {
     rs.iters = 0;
     rs.fallback = rs.seeded = rs.rejected = false;
     relaxed = g.applies;
@@ -439,23 +481,30 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
   if (relaxed) {
 #pragma unroll
     for (int k = 0; k < NP; k++) pk[k] = pstar;
-    if (P.rec_x != nullptr && !rs.fallback && rs.iters >= P.rec_min_evals)
+    if (!PTMU && P.rec_x != nullptr && !rs.fallback && rs.iters >= P.rec_min_evals)
       record_pair<NP>(P.rec_x, P.rec_y, P.rec_count, P.rec_max, a0, r0, p0, pstar);
   }
   if (PTMU) {
     // mixture internal energy of the rebuilt state (MixUEq::computeMixtureVariables :136), which
     // RelaxationPTMu reads before any fulfillState
-    double emix = 0.;
-#pragma unroll
-    for (int k = 0; k < NP; k++) {
-      double Y = a0[k] * r0[k] / dmax(rhomix, M.eps);
-      emix += Y * eos_e(M.eos[k], M.eps, r0[k], p0[k]);
-    }
+    const double emix = rebuilt_emix<NP>(M, a0, r0, p0, rhomix);
     bool err = false;
-    if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err, &cc.pc)) {
+    const double ps = SEED ? g.ptmu_p : -1., Ts = SEED ? g.ptmu_T : -1.;
+    if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err, &cc.pc, ps, Ts)) {
       rhomix = 0.;
 #pragma unroll
       for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
+    }
+    if (SEED && cc.pc.solve && ps > 0.) cc.pc.seeded = 1;
+    if (P.rec_x != nullptr && cc.pc.solve && !err && (int)cc.pc.outer >= P.rec_min_evals) {
+      float x[PTMU_NIN];
+      if (SEED) {
+#pragma unroll
+        for (int j = 0; j < PTMU_NIN; j++) x[j] = g.ptmu_x[j];
+      } else {
+        ptmu_features<NP>(M, P.ptmu_liq, P.ptmu_vap, a0, r0, p0, cp.rhomix, emix, x);
+      }
+      record_ptmu_pair(P.rec_x, P.rec_y, P.rec_count, P.rec_max, x, cc.pc.pstar, cc.pc.tsat);
     }
     if (err) cc.ptmu = 1;
   }

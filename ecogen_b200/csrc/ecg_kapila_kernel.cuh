@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
       bool in = g[ax] >= 0 && g[ax] < nax && g[b1] < G.n[b1] && g[b2] < G.n[b2];
       if (in) {
         int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
+        if (!ECG_IN_BOUNDS(P.stats, c, nn)) continue;
 #pragma unroll
         for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
         if (K::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
@@ -261,6 +262,7 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
         int gl = org[ax] + j - 1;
         if (gl < 0 || gl + 1 >= nax) continue;  // boundary face: handled below
         int e = line * (T + 1) + j;
+        if (!ECG_IN_BOUNDS(P.stats, e, FS)) continue;
         Flux<NP> F;
 #pragma unroll
         for (int k = 0; k < NP; k++) {
@@ -346,10 +348,13 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
   }
   // learned seed of the pressure relaxation, gated on the plain start (all lanes of the warp)
   SeedGate<NP> sg;
-  if (SEED) seed_gate<NP, DIM>(P, M, active, cp, sg);
+  if (SEED && !PTMU) seed_gate<NP, DIM>(P, M, active, cp, sg);
+  if (SEED && PTMU) ptmu_seed_gate<NP, DIM>(P, M, active, cp, sg, cc);
   if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
-  if (PTMU) block_ptmu_counters(P.stats, cc.pc.solve, cc.pc.outer, cc.pc.tsat_calls, cc.pc.tsat_iters, cc.pc.tsat_max);
+  if (PTMU)
+    block_ptmu_counters(P.stats, cc.pc.solve, cc.pc.outer, cc.pc.tsat_calls, cc.pc.tsat_iters, cc.pc.tsat_max,
+                        cc.pc.seeded, cc.pc.rejected);
 
   // ---- dtMax: block min, one atomic per block
   __shared__ double red[32];

@@ -45,9 +45,9 @@ template <int NP, int DIM, bool PTMU, bool SEED, int TYPES = EOS_DYNAMIC, int NT
 cudaError_t launch_pass_seed(int pass, const StepParams& P, const Geometry& G, const ecg_eos* eos, double eps,
                              cudaStream_t s, bool prepare) {
   switch (pass) {
-    case PASS_O1: return launch_form<NP, DIM, PASS_O1, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
-    case PASS_PRED: return launch_form<NP, DIM, PASS_PRED, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
-    default: return launch_form<NP, DIM, PASS_CORR, PTMU, SEED && !PTMU, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    case PASS_O1: return launch_form<NP, DIM, PASS_O1, PTMU, SEED, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    case PASS_PRED: return launch_form<NP, DIM, PASS_PRED, PTMU, SEED, TYPES, NTM>(P, G, eos, eps, s, prepare);
+    default: return launch_form<NP, DIM, PASS_CORR, PTMU, SEED, TYPES, NTM>(P, G, eos, eps, s, prepare);
   }
 }
 
@@ -103,7 +103,7 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
     cudaError_t e = launch_pass_seed<NP, DIM, PTMU, false>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, false, kEos>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, false, kEosLim>(pass, P, G, eos, eps, s, true);
-    if (e != cudaSuccess || PTMU) return e;
+    if (e != cudaSuccess) return e;
     e = launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, true);
     if (e == cudaSuccess && kFast) e = launch_pass_seed<NP, DIM, PTMU, true, kEosLim>(pass, P, G, eos, eps, s, true);
@@ -113,7 +113,6 @@ cudaError_t launch_pass(int pass, const StepParams& P, const Geometry& G, const 
   const int L = eos_fast_limiter<NP>();
   const bool fast_lim = P.lim[0] == L && P.lim[1] == L && P.lim[2] == L && P.lim[3] == L;
   if (P.mlp != nullptr) {  // the seeded kernels get the same compile-time configurations as the plain ones
-    if (PTMU) return cudaErrorNotSupported;
     if (fast_eos && fast_lim) return launch_pass_seed<NP, DIM, PTMU, true, kEosLim>(pass, P, G, eos, eps, s, false);
     if (fast_eos) return launch_pass_seed<NP, DIM, PTMU, true, kEos>(pass, P, G, eos, eps, s, false);
     return launch_pass_seed<NP, DIM, PTMU, true>(pass, P, G, eos, eps, s, false);

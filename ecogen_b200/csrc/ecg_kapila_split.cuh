@@ -39,10 +39,15 @@ __device__ __forceinline__ int64_t split_fid(const int n[3], int ax, int f, int 
 // Block of the face kernel of axis AX: TF faces along AX times W lines along the fastest other axis
 // (Y lines for X faces, X lines for Y and Z faces), one thread per face; the block's third coordinate
 // is blockIdx.z.  Shared planes are laid out so that the linear thread order is the storage order.
+// A line of X faces has n_x + 1 faces, so its last chunk holds a single face: chunks of 16 faces keep
+// more lanes busy than chunks of 32 on short lines (257 faces at 256^3: 94 % against 89 %).
+#ifndef ECG_XFACE_TF
+#define ECG_XFACE_TF 16
+#endif
 template <int AX>
 struct FaceTile {
-  static constexpr int TF = (AX == 0) ? 32 : 8;
-  static constexpr int W = (AX == 0) ? 4 : 16;
+  static constexpr int TF = (AX == 0) ? ECG_XFACE_TF : 8;
+  static constexpr int W = (AX == 0) ? 128 / ECG_XFACE_TF : 16;
   static constexpr int NTH = TF * W;
   static constexpr int CP = TF + 3;  // staged cells per line: f0-2 .. f0+TF
   static constexpr int SP = TF + 2;  // slopes per line: faces f0-1 .. f0+TF
@@ -111,6 +116,7 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
     coords(line, f0 - 2 + pos, g);
     if (g[AX] >= 0 && g[AX] < nax && g[ob] < G.n[ob]) {
       const int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
+      if (!ECG_IN_BOUNDS(P.stats, c, nn)) continue;
 #pragma unroll
       for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
       if (KS::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
@@ -157,7 +163,9 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
     const int f = f0 + fl;
     int g[3];
     coords(line, f, g);
-    if (f <= nax && g[ob] < G.n[ob]) {
+    // (bounds-checked builds: the staged cells this face reads, positions fl .. fl + 3 of its line)
+    if (f <= nax && g[ob] < G.n[ob] && ECG_IN_BOUNDS(P.stats, FT::cidx(line, fl), RS) &&
+        ECG_IN_BOUNDS(P.stats, FT::cidx(line, fl + 3), RS)) {
       Flux<NP> F;
       double Fn[3];
       const int gl = f - 1;
@@ -238,18 +246,20 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
       }
       const int64_t nfa = split_nfaces(G.n, AX);
       const int64_t fid = split_fid(G.n, AX, f, g[0], g[1], g[2]);
-      double* out = flux + fid;
+      if (ECG_IN_BOUNDS(P.stats, fid, nfa)) {
+        double* out = flux + fid;
 #pragma unroll
-      for (int k = 0; k < NP; k++) {
-        out[(int64_t)k * nfa] = F.a[k];
-        out[(int64_t)(NP + k) * nfa] = F.m[k];
-        out[(int64_t)(2 * NP + k) * nfa] = F.en[k];
+        for (int k = 0; k < NP; k++) {
+          out[(int64_t)k * nfa] = F.a[k];
+          out[(int64_t)(NP + k) * nfa] = F.m[k];
+          out[(int64_t)(2 * NP + k) * nfa] = F.en[k];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; d++) out[(int64_t)(3 * NP + d) * nfa] = F.mom[d];
+        out[(int64_t)(3 * NP + DIM) * nfa] = F.E;
+        out[(int64_t)(3 * NP + DIM + 1) * nfa] = F.sM;
+        out[(int64_t)(3 * NP + DIM + 2) * nfa] = F.uStar;
       }
-#pragma unroll
-      for (int d = 0; d < DIM; d++) out[(int64_t)(3 * NP + d) * nfa] = F.mom[d];
-      out[(int64_t)(3 * NP + DIM) * nfa] = F.E;
-      out[(int64_t)(3 * NP + DIM + 1) * nfa] = F.sM;
-      out[(int64_t)(3 * NP + DIM + 2) * nfa] = F.uStar;
     }
   }
 
@@ -269,7 +279,9 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
 }
 
 template <int NP, int DIM>
-__device__ __forceinline__ void load_face_flux(const double* __restrict__ fl, int64_t nfa, int64_t fid, Flux<NP>& F) {
+__device__ __forceinline__ void load_face_flux(const double* __restrict__ fl, int64_t nfa, int64_t fid, Flux<NP>& F,
+                                               DevStats* st) {
+  if (!ECG_IN_BOUNDS(st, fid, nfa)) fid = 0;
   const double* p = fl + fid;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
@@ -327,11 +339,11 @@ __global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_
       const double cA = cell_coefA(G, ax, g[0], g[1], g[2]);
       Flux<NP> F;
       if (g[ax] >= 1) {
-        load_face_flux<NP, DIM>(fa[ax], nfa, split_fid(G.n, ax, g[ax], g[0], g[1], g[2]), F);
+        load_face_flux<NP, DIM>(fa[ax], nfa, split_fid(G.n, ax, g[ax], g[0], g[1], g[2]), F, P.stats);
         acc_face<NP, DIM>(cA, true, F, an, pn, aa, am, ae, amom, aE);
       }
       if (g[ax] + 1 <= G.n[ax] - 1) {
-        load_face_flux<NP, DIM>(fa[ax], nfa, split_fid(G.n, ax, g[ax] + 1, g[0], g[1], g[2]), F);
+        load_face_flux<NP, DIM>(fa[ax], nfa, split_fid(G.n, ax, g[ax] + 1, g[0], g[1], g[2]), F, P.stats);
         acc_face<NP, DIM>(cA, false, F, an, pn, aa, am, ae, amom, aE);
       }
     }
@@ -344,16 +356,19 @@ __global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_
       if (neg ? (g[ax] != 0) : (g[ax] != G.n[ax] - 1)) continue;
       Flux<NP> F;
       load_face_flux<NP, DIM>(fa[ax], split_nfaces(G.n, ax), split_fid(G.n, ax, neg ? 0 : G.n[ax], g[0], g[1], g[2]),
-                              F);
+                              F, P.stats);
       acc_face<NP, DIM>(cell_coefA(G, ax, g[0], g[1], g[2]), false, F, an, pn, aa, am, ae, amom, aE);
     }
     kapila_rebuild<NP, DIM, PASS>(P, M, nn, cell, *P.dt, an, rn, pn, aa, am, ae, amom, aE, cp);
   }
   SeedGate<NP> sg;
-  if (SEED) seed_gate<NP, DIM>(P, M, active, cp, sg);
+  if (SEED && !PTMU) seed_gate<NP, DIM>(P, M, active, cp, sg);
+  if (SEED && PTMU) ptmu_seed_gate<NP, DIM>(P, M, active, cp, sg, cc);
   if (active) kapila_finish<NP, DIM, PASS, PTMU, SEED, (TYPES == EOS_DYNAMIC)>(P, M, nn, cell, cp, sg, cc);
   block_counters(P.stats, cc.relax, cc.iters, cc.fallback, cc.seeded, cc.rejected, cc.nonfinite, cc.ptmu, cc.iters, true);
-  if (PTMU) block_ptmu_counters(P.stats, cc.pc.solve, cc.pc.outer, cc.pc.tsat_calls, cc.pc.tsat_iters, cc.pc.tsat_max);
+  if (PTMU)
+    block_ptmu_counters(P.stats, cc.pc.solve, cc.pc.outer, cc.pc.tsat_calls, cc.pc.tsat_iters, cc.pc.tsat_max,
+                        cc.pc.seeded, cc.pc.rejected);
 }
 
 template <int NP, int DIM, int AX, int PASS, int TYPES>

@@ -8,6 +8,7 @@
 //
 // Packed parameter block (floats), H = ECG_MLP_HIDDEN, I = number of inputs:
 //   w1[H*I] b1[H] w2[H*H] b2[H] w3[H] b3 in_shift[I] in_scale[I] out_shift out_scale
+// and for a two-output network (the p-T-mu seed, further down) w3b[H] b3b out_shift_1 out_scale_1.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -72,6 +73,9 @@ struct MlpDev {
   float b1[MLP_H], b2[MLP_H], w3[MLP_H];
   float ish[16], isc[16];
   float b3, osh, osc, pad;
+  // second output of a two-output network (the p-T-mu seed's T_sat head)
+  float w3b[MLP_H];
+  float b3b, osh2, osc2, pad2;
 };
 
 __device__ __forceinline__ unsigned int pack_bf16(float lo, float hi) {
@@ -87,26 +91,16 @@ __device__ __forceinline__ void mma_bf16(float d[4], const unsigned int a[4], un
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Returns the seed for this lane's cell (lanes with `valid`), NaN for the other lanes.
-template <int NP>
-__device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bool valid, const double a[NP],
-                                                const double r[NP], const double p[NP]) {
-  constexpr int NI = 3 * NP;
+// The network's NO raw outputs (before de-normalisation, bias included) for this lane's cell, from its
+// NI normalised inputs (zeros on lanes without a cell).  Every lane of the warp must call it.
+template <int NI, int NO>
+__device__ __forceinline__ void mlp_warp_raw(const MlpDev* __restrict__ W, const float xn[NI], float y[NO]) {
   static_assert(NI <= 16, "inputs padded to one k16 slice");
+  static_assert(NO == 1 || NO == 2, "one or two outputs");
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  float xn[NI];
-  if (valid) {
-    float x[NI];
-    mlp_features<NP>(a, r, p, x);
-#pragma unroll
-    for (int i = 0; i < NI; i++) xn[i] = (x[i] - __ldg(&W->ish[i])) * __ldg(&W->isc[i]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < NI; i++) xn[i] = 0.f;
-  }
-  float out[4];  // row sums: tile 0 rows g, g+8; tile 1 rows g, g+8 (complete on lanes with t == 0)
+  float out[NO][4];  // row sums: tile 0 rows g, g+8; tile 1 rows g, g+8 (complete on lanes with t == 0)
 #pragma unroll
   for (int m = 0; m < 2; m++) {
     // A fragment of rows (16m + g, 16m + g + 8), columns (2t, 2t+1) and (2t+8, 2t+9)
@@ -146,7 +140,9 @@ __device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bo
         A2[kc][3] = hi;
       }
     }
-    float sum_lo = 0.f, sum_hi = 0.f;
+    float sum_lo[NO], sum_hi[NO];
+#pragma unroll
+    for (int o = 0; o < NO; o++) sum_lo[o] = sum_hi[o] = 0.f;
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
       float c[4] = {0.f, 0.f, 0.f, 0.f};
@@ -157,29 +153,59 @@ __device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bo
       }
       const int col = 8 * nt + 2 * t;
       const float2 b2 = __ldg(reinterpret_cast<const float2*>(&W->b2[col]));
-      const float2 w3 = __ldg(reinterpret_cast<const float2*>(&W->w3[col]));
-      sum_lo += w3.x * gelu_f(c[0] + b2.x) + w3.y * gelu_f(c[1] + b2.y);
-      sum_hi += w3.x * gelu_f(c[2] + b2.x) + w3.y * gelu_f(c[3] + b2.y);
+      const float h0 = gelu_f(c[0] + b2.x), h1 = gelu_f(c[1] + b2.y), h2 = gelu_f(c[2] + b2.x),
+                  h3 = gelu_f(c[3] + b2.y);
+#pragma unroll
+      for (int o = 0; o < NO; o++) {
+        const float2 w3 = __ldg(reinterpret_cast<const float2*>(o == 0 ? &W->w3[col] : &W->w3b[col]));
+        sum_lo[o] += w3.x * h0 + w3.y * h1;
+        sum_hi[o] += w3.x * h2 + w3.y * h3;
+      }
     }
 #pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-      sum_lo += __shfl_xor_sync(FULL, sum_lo, o);
-      sum_hi += __shfl_xor_sync(FULL, sum_hi, o);
+    for (int o = 0; o < NO; o++) {
+#pragma unroll
+      for (int q = 1; q < 4; q <<= 1) {
+        sum_lo[o] += __shfl_xor_sync(FULL, sum_lo[o], q);
+        sum_hi[o] += __shfl_xor_sync(FULL, sum_hi[o], q);
+      }
+      out[o][2 * m] = sum_lo[o];
+      out[o][2 * m + 1] = sum_hi[o];
     }
-    out[2 * m] = sum_lo;
-    out[2 * m + 1] = sum_hi;
   }
-  // row `lane` of the 32 x 1 output: tile lane / 16, row lane % 16 held by lane 4 * (lane % 8)
+  // row `lane` of the 32 x NO output: tile lane / 16, row lane % 16 held by lane 4 * (lane % 8)
   const int src = 4 * (lane & 7), sel = lane >> 3;
-  float y = 0.f;
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const float v = __shfl_sync(FULL, out[q], src);
-    if (q == sel) y = v;
+  for (int o = 0; o < NO; o++) {
+    float yo = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float v = __shfl_sync(FULL, out[o][q], src);
+      if (q == sel) yo = v;
+    }
+    y[o] = yo + __ldg(o == 0 ? &W->b3 : &W->b3b);
   }
+}
+
+// Returns the seed for this lane's cell (lanes with `valid`), NaN for the other lanes.
+template <int NP>
+__device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bool valid, const double a[NP],
+                                                const double r[NP], const double p[NP]) {
+  constexpr int NI = 3 * NP;
+  float xn[NI];
+  if (valid) {
+    float x[NI];
+    mlp_features<NP>(a, r, p, x);
+#pragma unroll
+    for (int i = 0; i < NI; i++) xn[i] = (x[i] - __ldg(&W->ish[i])) * __ldg(&W->isc[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NI; i++) xn[i] = 0.f;
+  }
+  float y[1];
+  mlp_warp_raw<NI, 1>(W, xn, y);
   if (!valid) return __longlong_as_double(0x7ff8000000000000LL);
-  y += __ldg(&W->b3);
-  double tt = (double)(y * __ldg(&W->osc) + __ldg(&W->osh));
+  double tt = (double)(y[0] * __ldg(&W->osc) + __ldg(&W->osh));
   double lo = p[0], hi = p[0];
 #pragma unroll
   for (int k = 1; k < NP; k++) {
@@ -190,9 +216,64 @@ __device__ __forceinline__ double mlp_seed_warp(const MlpDev* __restrict__ W, bo
   return lo + tt * (hi - lo);
 }
 
+// ----------------------------------------------------------------------------------------------
+// Learned (p*, T) seed of the p-T-mu relaxation (RelaxationPTMu::relaxation
+// src/Relaxations/RelaxationPTMu.cpp:73-200).  The saturation solve's answer depends on the mixture
+// density and internal energy the cell holds after buildPrim, so the features come from that state:
+//   ln rho, asinh(e / 1e5), alpha_liq, ln rho_liq, ln rho_vap, asinh(sum_k alpha_k p_k / 1e5) (the
+//   plain start), asinh(p_vap(rho, e) / 1e5), asinh(p_liq(rho, e) / 1e5) (the pure-phase pressures)
+// and the targets are ln p* and T_sat(p*) of the converged solve.
+constexpr int PTMU_NIN = 8;
+
+template <int NP>
+__device__ __forceinline__ void ptmu_features(const Model<NP>& M, int liq, int vap, const double a[NP],
+                                              const double r[NP], const double p[NP], double rhomix, double emix,
+                                              float x[PTMU_NIN]) {
+  double ps = 0.;
+#pragma unroll
+  for (int k = 0; k < NP; k++) ps += a[k] * p[k];
+  const double pv = eos_p(M.eos[vap], M.eps, rhomix, emix), pl = eos_p(M.eos[liq], M.eps, rhomix, emix);
+  x[0] = (float)log(rhomix > 1e-300 ? rhomix : 1e-300);
+  x[1] = (float)asinh(emix * 1.e-5);
+  x[2] = (float)a[liq];
+  x[3] = (float)log(r[liq] > 1e-300 ? r[liq] : 1e-300);
+  x[4] = (float)log(r[vap] > 1e-300 ? r[vap] : 1e-300);
+  x[5] = (float)asinh(ps * 1.e-5);
+  x[6] = (float)asinh(pv * 1.e-5);
+  x[7] = (float)asinh(pl * 1.e-5);
+}
+
+// Appends one (features, ln p*, T_sat) record of a converged saturation solve.
+__device__ __forceinline__ void record_ptmu_pair(float* rx, float* ry, unsigned long long* count,
+                                                 unsigned long long maxn, const float x[PTMU_NIN], double pstar,
+                                                 double tsat) {
+  unsigned long long i = atomicAdd(count, 1ull);
+  if (i >= maxn) return;
+#pragma unroll
+  for (int j = 0; j < PTMU_NIN; j++) rx[i * PTMU_NIN + j] = x[j];
+  ry[2 * i] = (float)log(pstar);
+  ry[2 * i + 1] = (float)tsat;
+}
+
+// (p*, T) seed for this lane's cell from its features (lanes with `valid`); every lane of the warp must
+// call it.  p_seed / T_seed are -1 on lanes without a cell.
+__device__ __forceinline__ void mlp_ptmu_seed_warp(const MlpDev* __restrict__ W, bool valid, const float x[PTMU_NIN],
+                                                   double& p_seed, double& T_seed) {
+  float xn[PTMU_NIN];
+#pragma unroll
+  for (int i = 0; i < PTMU_NIN; i++) xn[i] = valid ? (x[i] - __ldg(&W->ish[i])) * __ldg(&W->isc[i]) : 0.f;
+  float y[2];
+  mlp_warp_raw<PTMU_NIN, 2>(W, xn, y);
+  p_seed = T_seed = -1.;
+  if (!valid) return;
+  p_seed = exp((double)(y[0] * __ldg(&W->osc) + __ldg(&W->osh)));
+  T_seed = (double)(y[1] * __ldg(&W->osc2) + __ldg(&W->osh2));
+}
+
 // Builds the device form of a model from the packed FP32 parameters (see the top of this file).
-cudaError_t mlp_install(const float* d_params, int nin, MlpDev* d_out, cudaStream_t stream);
-// Checks, packs and installs an ABI model into *dev (allocated on first use); synchronous.
-ecg_status mlp_upload(const ecg_mlp* m, int np, MlpDev** dev, cudaStream_t stream);
+cudaError_t mlp_install(const float* d_params, int nin, int nout, MlpDev* d_out, cudaStream_t stream);
+// Checks, packs and installs an ABI model into *dev (allocated on first use); synchronous.  The pressure
+// relaxation's model has 3 np inputs and one output, the p-T-mu relaxation's (ptmu) 8 inputs and two.
+ecg_status mlp_upload(const ecg_mlp* m, int np, bool ptmu, MlpDev** dev, cudaStream_t stream);
 
 }  // namespace ecg

@@ -35,9 +35,10 @@ __device__ __forceinline__ float t_gelu(float z, float* d) {
   return 0.5f * z * (1.f + th);
 }
 
-// Forward (and, with grads != nullptr, backward) of rows [r0, r1) of the batch.
-// Gradients are added into g (same layout as the parameters) scaled by 1/n_total; loss_sum receives
-// the sum of squared errors.
+// Forward (and, with grads != nullptr, backward) of rows [r0, r1) of the batch, NOUT outputs per row
+// (y and yhat are n x NOUT).  Gradients are added into g (same layout as the parameters) scaled by
+// 1/n_total; loss_sum receives the sum of squared errors over rows and outputs.
+template <int NOUT>
 __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const float* __restrict__ x,
                                                     const float* __restrict__ y, int n, float* yhat, MlpDev G,
                                                     float* loss_sum, float inv_n) {
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const flo
   float* sh1 = sx + TROWS * nin;       // [TROWS][TH]
   float* sz1 = sh1 + TROWS * TH;       // [TROWS][TH]  (gelu' of layer 1)
   float* sdz2 = sz1 + TROWS * TH;      // [TROWS][TH]
-  float* sy = sdz2 + TROWS * TH;       // [TROWS]
+  float* sy = sdz2 + TROWS * TH;       // [TROWS][NOUT]
   float* gW1 = sy + TROWS;             // [TH][nin] gradient accumulators (row j owned by thread j)
   float* gW2 = gW1 + TH * nin;         // [TH][TH]
   const int j = threadIdx.x;
@@ -61,8 +62,15 @@ __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const flo
     sW2[i] = P.w2[i];
     gW2[i] = 0.f;
   }
-  const float b1j = P.b1[j], b2j = P.b2[j], w3j = P.w3[j], b3 = P.b3[0];
-  float gb1 = 0.f, gb2 = 0.f, gw3 = 0.f, gb3 = 0.f, lsum = 0.f;
+  const float b1j = P.b1[j], b2j = P.b2[j];
+  float w3j[NOUT], b3[NOUT], gw3[NOUT], gb3[NOUT];
+#pragma unroll
+  for (int o = 0; o < NOUT; o++) {
+    w3j[o] = P.w3[o * TH + j];
+    b3[o] = P.b3[o];
+    gw3[o] = gb3[o] = 0.f;
+  }
+  float gb1 = 0.f, gb2 = 0.f, lsum = 0.f;
   __syncthreads();
   const int ntiles = (n + TROWS - 1) / TROWS;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -87,28 +95,39 @@ __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const flo
       h2[r] = t_gelu(z, &d2[r]);
     }
     for (int r = 0; r < nr; r++) {
-      float v = w3j * h2[r];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if ((j & 31) == 0) sdz2[r * TH + j] = v;  // scratch: warp partials at columns 0 and 32
+#pragma unroll
+      for (int o = 0; o < NOUT; o++) {
+        float v = w3j[o] * h2[r];
+        for (int q = 16; q > 0; q >>= 1) v += __shfl_xor_sync(0xffffffffu, v, q);
+        if ((j & 31) == 0) sdz2[r * TH + j + o] = v;  // scratch: warp partials at columns o and 32 + o
+      }
     }
     __syncthreads();
     if (j < nr) {
-      float out = sdz2[j * TH + 0] + sdz2[j * TH + 32] + b3;
-      sy[j] = out;
-      if (yhat) yhat[r0 + j] = out;
+#pragma unroll
+      for (int o = 0; o < NOUT; o++) {
+        float out = sdz2[j * TH + o] + sdz2[j * TH + 32 + o] + b3[o];
+        sy[j * NOUT + o] = out;
+        if (yhat) yhat[(size_t)(r0 + j) * NOUT + o] = out;
+      }
     }
     __syncthreads();
     if (train) {
-      // backward: dL/dy = 2 (yhat - y) / n
+      // backward: dL/dy_o = 2 (yhat_o - y_o) / n
       for (int r = 0; r < nr; r++) {
-        float e = sy[r] - y[r0 + r];
-        float dy = 2.f * e * inv_n;
-        if (j == 0) {
-          gb3 += dy;
-          lsum += e * e;
+        float dsum = 0.f;
+#pragma unroll
+        for (int o = 0; o < NOUT; o++) {
+          float e = sy[r * NOUT + o] - y[(size_t)(r0 + r) * NOUT + o];
+          float dy = 2.f * e * inv_n;
+          if (j == 0) {
+            gb3[o] += dy;
+            lsum += e * e;
+          }
+          gw3[o] += dy * h2[r];
+          dsum += dy * w3j[o];
         }
-        gw3 += dy * h2[r];
-        float dz2 = dy * w3j * d2[r];
+        float dz2 = dsum * d2[r];
         sdz2[r * TH + j] = dz2;
         gb2 += dz2;
         for (int i = 0; i < TH; i++) gW2[j * TH + i] += dz2 * sh1[r * TH + i];
@@ -130,9 +149,11 @@ __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const flo
     for (int i = 0; i < TH; i++) atomicAdd(&G.w2[j * TH + i], gW2[j * TH + i]);
     atomicAdd(&G.b1[j], gb1);
     atomicAdd(&G.b2[j], gb2);
-    atomicAdd(&G.w3[j], gw3);
+#pragma unroll
+    for (int o = 0; o < NOUT; o++) atomicAdd(&G.w3[o * TH + j], gw3[o]);
     if (j == 0) {
-      atomicAdd(&G.b3[0], gb3);
+#pragma unroll
+      for (int o = 0; o < NOUT; o++) atomicAdd(&G.b3[o], gb3[o]);
       atomicAdd(loss_sum, lsum);
     }
   }
@@ -158,8 +179,9 @@ using namespace ecg;
 
 struct ecg_trainer {
   int nin = 0;
+  int nout = 1;
   int nparam = 0;
-  float* p = nullptr;   // flat: w1 b1 w2 b2 w3 b3
+  float* p = nullptr;   // flat: w1 b1 w2 b2 w3[nout][H] b3[nout]
   float* g = nullptr;
   float* m = nullptr;
   float* v = nullptr;
@@ -170,25 +192,27 @@ struct ecg_trainer {
   size_t cap = 0;
   long step = 0;
   std::vector<float> host;  // export copy
-  float in_shift[ECG_MLP_MAX_IN] = {}, in_scale[ECG_MLP_MAX_IN] = {}, out_shift = 0.f, out_scale = 1.f;
+  float in_shift[ECG_MLP_MAX_IN] = {}, in_scale[ECG_MLP_MAX_IN] = {};
+  float out_shift[2] = {0.f, 0.f}, out_scale[2] = {1.f, 1.f};
   cudaStream_t stream = nullptr;
 };
 
 namespace {
 
-MlpDev views(float* base, int nin) {
+MlpDev views(float* base, int nin, int nout) {
   MlpDev d;
   d.w1 = base;
   d.b1 = d.w1 + TH * nin;
   d.w2 = d.b1 + TH;
   d.b2 = d.w2 + TH * TH;
   d.w3 = d.b2 + TH;
-  d.b3 = d.w3 + TH;
+  d.b3 = d.w3 + TH * nout;
   return d;
 }
 
 size_t smem_bytes(int nin) {
-  return sizeof(float) * (size_t)(TH * nin + TH * TH + TROWS * nin + 3 * TROWS * TH + TROWS + TH * nin + TH * TH);
+  return sizeof(float) *
+         (size_t)(TH * nin + TH * TH + TROWS * nin + 3 * TROWS * TH + 2 * TROWS + TH * nin + TH * TH);
 }
 
 ecg_status tfail(cudaError_t e, const char* w) {
@@ -207,24 +231,28 @@ ecg_status ensure(ecg_trainer* tr, size_t n) {
   cudaFree(tr->dy);
   cudaFree(tr->dyhat);
   TCUDA(cudaMalloc(&tr->dx, sizeof(float) * n * tr->nin));
-  TCUDA(cudaMalloc(&tr->dy, sizeof(float) * n));
-  TCUDA(cudaMalloc(&tr->dyhat, sizeof(float) * n));
+  TCUDA(cudaMalloc(&tr->dy, sizeof(float) * n * tr->nout));
+  TCUDA(cudaMalloc(&tr->dyhat, sizeof(float) * n * tr->nout));
   tr->cap = n;
   return ECG_OK;
 }
 
 ecg_status run_batch(ecg_trainer* tr, const float* dxp, const float* dyp, int n, bool train, float* yhat_dev,
                      float* loss_out) {
-  MlpDev P = views(tr->p, tr->nin);
-  MlpDev G = train ? views(tr->g, tr->nin) : MlpDev{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  MlpDev P = views(tr->p, tr->nin, tr->nout);
+  MlpDev G = train ? views(tr->g, tr->nin, tr->nout) : MlpDev{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   if (train) {
     TCUDA(cudaMemsetAsync(tr->g, 0, sizeof(float) * tr->nparam, tr->stream));
     TCUDA(cudaMemsetAsync(tr->loss, 0, sizeof(float), tr->stream));
   }
   int ntiles = (n + TROWS - 1) / TROWS;
   int grid = std::min(ntiles, 148 * 4);
-  k_mlp_fwd_bwd<<<grid, TH, smem_bytes(tr->nin), tr->stream>>>(P, tr->nin, dxp, dyp, n, yhat_dev, G, tr->loss,
-                                                              1.f / (float)n);
+  if (tr->nout == 2)
+    k_mlp_fwd_bwd<2><<<grid, TH, smem_bytes(tr->nin), tr->stream>>>(P, tr->nin, dxp, dyp, n, yhat_dev, G, tr->loss,
+                                                                   1.f / (float)n);
+  else
+    k_mlp_fwd_bwd<1><<<grid, TH, smem_bytes(tr->nin), tr->stream>>>(P, tr->nin, dxp, dyp, n, yhat_dev, G, tr->loss,
+                                                                   1.f / (float)n);
   TCUDA(cudaGetLastError());
   if (loss_out) {
     float l = 0.f;
@@ -238,14 +266,20 @@ ecg_status run_batch(ecg_trainer* tr, const float* dxp, const float* dyp, int n,
 }  // namespace
 
 extern "C" ecg_status ecg_trainer_create(int32_t nin, int32_t hidden, uint64_t seed, ecg_trainer** out) {
-  if (!out || nin < 1 || nin > ECG_MLP_MAX_IN || hidden != ECG_MLP_HIDDEN) {
-    set_error("trainer shape must be nin (<=16) -> 64 -> 64 -> 1");
+  return ecg_trainer_create_n(nin, 1, hidden, seed, out);
+}
+
+extern "C" ecg_status ecg_trainer_create_n(int32_t nin, int32_t nout, int32_t hidden, uint64_t seed,
+                                           ecg_trainer** out) {
+  if (!out || nin < 1 || nin > ECG_MLP_MAX_IN || hidden != ECG_MLP_HIDDEN || nout < 1 || nout > 2) {
+    set_error("trainer shape must be nin (<=16) -> 64 -> 64 -> nout (1 or 2)");
     return ECG_ERR_INVALID;
   }
   *out = nullptr;
   auto tr = new ecg_trainer();
   tr->nin = nin;
-  tr->nparam = TH * nin + TH + TH * TH + TH + TH + 1;
+  tr->nout = nout;
+  tr->nparam = TH * nin + TH + TH * TH + TH + nout * TH + nout;
   for (int i = 0; i < ECG_MLP_MAX_IN; i++) tr->in_scale[i] = 1.f;
   std::vector<float> h(tr->nparam, 0.f);
   std::mt19937_64 g(seed);
@@ -255,7 +289,7 @@ extern "C" ecg_status ecg_trainer_create(int32_t nin, int32_t hidden, uint64_t s
   };
   fill(h.data(), nin, TH * nin);
   fill(h.data() + TH * nin + TH, TH, TH * TH);
-  fill(h.data() + TH * nin + TH + TH * TH + TH, TH, TH);
+  fill(h.data() + TH * nin + TH + TH * TH + TH, TH, nout * TH);
   cudaError_t e = cudaStreamCreateWithFlags(&tr->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&tr->p, sizeof(float) * tr->nparam);
   if (e == cudaSuccess) e = cudaMalloc(&tr->g, sizeof(float) * tr->nparam);
@@ -266,7 +300,9 @@ extern "C" ecg_status ecg_trainer_create(int32_t nin, int32_t hidden, uint64_t s
   if (e == cudaSuccess) e = cudaMemset(tr->m, 0, sizeof(float) * tr->nparam);
   if (e == cudaSuccess) e = cudaMemset(tr->v, 0, sizeof(float) * tr->nparam);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(nin));
+    e = cudaFuncSetAttribute(k_mlp_fwd_bwd<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(nin));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mlp_fwd_bwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(nin));
   if (e != cudaSuccess) {
     ecg_trainer_destroy(tr);
     return tfail(e, "ecg_trainer_create");
@@ -299,13 +335,13 @@ extern "C" ecg_status ecg_trainer_epoch(ecg_trainer* tr, const float* x, const f
   ecg_status s = ensure(tr, (size_t)n);
   if (s != ECG_OK) return s;
   TCUDA(cudaMemcpyAsync(tr->dx, x, sizeof(float) * n * tr->nin, cudaMemcpyHostToDevice, tr->stream));
-  TCUDA(cudaMemcpyAsync(tr->dy, y, sizeof(float) * n, cudaMemcpyHostToDevice, tr->stream));
+  TCUDA(cudaMemcpyAsync(tr->dy, y, sizeof(float) * n * tr->nout, cudaMemcpyHostToDevice, tr->stream));
   double total = 0.;
   int64_t nb = 0;
   for (int64_t r = 0; r < n; r += batch) {
     int cnt = (int)std::min<int64_t>(batch, n - r);
     float l = 0.f;
-    s = run_batch(tr, tr->dx + r * tr->nin, tr->dy + r, cnt, true, nullptr, &l);
+    s = run_batch(tr, tr->dx + r * tr->nin, tr->dy + r * tr->nout, cnt, true, nullptr, &l);
     if (s != ECG_OK) return s;
     tr->step++;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -330,7 +366,7 @@ extern "C" ecg_status ecg_trainer_grad(ecg_trainer* tr, const float* x, const fl
   ecg_status s = ensure(tr, (size_t)n);
   if (s != ECG_OK) return s;
   TCUDA(cudaMemcpyAsync(tr->dx, x, sizeof(float) * n * tr->nin, cudaMemcpyHostToDevice, tr->stream));
-  TCUDA(cudaMemcpyAsync(tr->dy, y, sizeof(float) * n, cudaMemcpyHostToDevice, tr->stream));
+  TCUDA(cudaMemcpyAsync(tr->dy, y, sizeof(float) * n * tr->nout, cudaMemcpyHostToDevice, tr->stream));
   float l = 0.f;
   s = run_batch(tr, tr->dx, tr->dy, n, true, nullptr, &l);
   if (s != ECG_OK) return s;
@@ -346,9 +382,9 @@ extern "C" ecg_status ecg_trainer_grad(ecg_trainer* tr, const float* x, const fl
   q += TH * TH;
   if (gb2) std::memcpy(gb2, q, sizeof(float) * TH);
   q += TH;
-  if (gw3) std::memcpy(gw3, q, sizeof(float) * TH);
-  q += TH;
-  if (gb3) *gb3 = *q;
+  if (gw3) std::memcpy(gw3, q, sizeof(float) * TH * tr->nout);
+  q += TH * tr->nout;
+  if (gb3) std::memcpy(gb3, q, sizeof(float) * tr->nout);
   if (loss) *loss = l;
   return ECG_OK;
 }
@@ -363,7 +399,7 @@ extern "C" ecg_status ecg_trainer_forward(ecg_trainer* tr, const float* x, int32
   TCUDA(cudaMemcpyAsync(tr->dx, x, sizeof(float) * n * tr->nin, cudaMemcpyHostToDevice, tr->stream));
   s = run_batch(tr, tr->dx, tr->dy, n, false, tr->dyhat, nullptr);
   if (s != ECG_OK) return s;
-  TCUDA(cudaMemcpyAsync(yhat, tr->dyhat, sizeof(float) * n, cudaMemcpyDeviceToHost, tr->stream));
+  TCUDA(cudaMemcpyAsync(yhat, tr->dyhat, sizeof(float) * n * tr->nout, cudaMemcpyDeviceToHost, tr->stream));
   TCUDA(cudaStreamSynchronize(tr->stream));
   return ECG_OK;
 }
@@ -378,8 +414,19 @@ extern "C" ecg_status ecg_trainer_set_norm(ecg_trainer* tr, const float* in_shif
     tr->in_shift[i] = in_shift[i];
     tr->in_scale[i] = in_scale[i];
   }
-  tr->out_shift = out_shift;
-  tr->out_scale = out_scale;
+  tr->out_shift[0] = out_shift;
+  tr->out_scale[0] = out_scale;
+  return ECG_OK;
+}
+
+// De-normalisation of the second output of a two-output network (exported as out_shift_1 / _scale_1).
+extern "C" ecg_status ecg_trainer_set_norm_out1(ecg_trainer* tr, float out_shift, float out_scale) {
+  if (!tr || tr->nout < 2) {
+    set_error("the trainer has one output");
+    return ECG_ERR_INVALID;
+  }
+  tr->out_shift[1] = out_shift;
+  tr->out_scale[1] = out_scale;
   return ECG_OK;
 }
 
@@ -404,19 +451,23 @@ extern "C" ecg_status ecg_trainer_export(ecg_trainer* tr, ecg_mlp* out) {
   out->b2 = q;
   q += TH;
   out->w3 = q;
-  q += TH;
-  out->b3 = *q;
+  q += TH * tr->nout;
+  out->b3 = q[0];
+  out->n_out = tr->nout;
+  if (tr->nout == 2) out->b3_1 = q[1];
   for (int i = 0; i < nin; i++) {
     out->in_shift[i] = tr->in_shift[i];
     out->in_scale[i] = tr->in_scale[i];
   }
-  out->out_shift = tr->out_shift;
-  out->out_scale = tr->out_scale;
+  out->out_shift = tr->out_shift[0];
+  out->out_scale = tr->out_scale[0];
+  out->out_shift_1 = tr->out_shift[1];
+  out->out_scale_1 = tr->out_scale[1];
   return ECG_OK;
 }
 
 extern "C" ecg_status ecg_trainer_import(ecg_trainer* tr, const ecg_mlp* in) {
-  if (!tr || !in || in->n_in != tr->nin || in->hidden != TH) {
+  if (!tr || !in || in->n_in != tr->nin || in->hidden != TH || (in->n_out > 1 ? in->n_out : 1) != tr->nout) {
     set_error("bad argument");
     return ECG_ERR_INVALID;
   }
@@ -431,15 +482,18 @@ extern "C" ecg_status ecg_trainer_import(ecg_trainer* tr, const ecg_mlp* in) {
   q += TH * TH;
   std::memcpy(q, in->b2, sizeof(float) * TH);
   q += TH;
-  std::memcpy(q, in->w3, sizeof(float) * TH);
-  q += TH;
-  *q = in->b3;
+  std::memcpy(q, in->w3, sizeof(float) * TH * tr->nout);
+  q += TH * tr->nout;
+  q[0] = in->b3;
+  if (tr->nout == 2) q[1] = in->b3_1;
   TCUDA(cudaMemcpy(tr->p, h.data(), sizeof(float) * tr->nparam, cudaMemcpyHostToDevice));
   for (int i = 0; i < nin; i++) {
     tr->in_shift[i] = in->in_shift[i];
     tr->in_scale[i] = in->in_scale[i];
   }
-  tr->out_shift = in->out_shift;
-  tr->out_scale = in->out_scale;
+  tr->out_shift[0] = in->out_shift;
+  tr->out_scale[0] = in->out_scale;
+  tr->out_shift[1] = in->out_shift_1;
+  tr->out_scale[1] = in->out_scale_1;
   return ECG_OK;
 }

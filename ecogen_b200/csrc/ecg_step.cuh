@@ -169,6 +169,21 @@ __device__ __forceinline__ double cell_coefA(const Geometry& G, int ax, int i, i
   return s / vol * 1.;
 }
 
+// Bounds-checked builds (-DECG_BOUNDS_CHECK, libecg_bounds.so): every state, face-array and output
+// access of the step kernels checks its linear index against its buffer; an index outside is counted
+// in DevStats::bounds_violations and the access is skipped -- never a trap.  Regular builds compile the
+// checks away.
+#ifdef ECG_BOUNDS_CHECK
+__device__ __forceinline__ bool ecg_in_bounds(DevStats* st, int64_t i, int64_t n) {
+  if (i >= 0 && i < n) return true;
+  atomicAdd(&st->bounds_violations, 1ull);
+  return false;
+}
+#define ECG_IN_BOUNDS(st, i, n) ecg_in_bounds((st), (int64_t)(i), (int64_t)(n))
+#else
+#define ECG_IN_BOUNDS(st, i, n) true
+#endif
+
 // Faces normal to axis ax of a mesh of n cells per axis, the two domain sides of every line included
 // (the face arrays of the split form).
 __host__ __device__ inline int64_t split_nfaces(const int n[3], int ax) {
@@ -223,10 +238,11 @@ __device__ __forceinline__ void block_counters(DevStats* st, unsigned int relax,
 // the device counters, one global atomic per counter and block.  Every thread of the block must call it.
 __device__ __forceinline__ void block_ptmu_counters(DevStats* st, unsigned int solve, unsigned int outer,
                                                     unsigned int tsat_calls, unsigned int tsat_iters,
-                                                    unsigned int tsat_max) {
-  __shared__ unsigned int sp[22];
+                                                    unsigned int tsat_max, unsigned int seeded,
+                                                    unsigned int rejected) {
+  __shared__ unsigned int sp[24];
   const int tid = threadIdx.x;
-  if (tid < 22) sp[tid] = 0u;
+  if (tid < 24) sp[tid] = 0u;
   __syncthreads();
   const unsigned full = 0xffffffffu;
   const unsigned int v[4] = {solve, outer, tsat_calls, tsat_iters};
@@ -235,6 +251,9 @@ __device__ __forceinline__ void block_ptmu_counters(DevStats* st, unsigned int s
     const unsigned int w = __reduce_add_sync(full, v[i]);
     if ((tid & 31) == 0 && w) atomicAdd(&sp[i], w);
   }
+  const unsigned int ws = __reduce_add_sync(full, seeded), wr = __reduce_add_sync(full, rejected);
+  if ((tid & 31) == 0 && ws) atomicAdd(&sp[22], ws);
+  if ((tid & 31) == 0 && wr) atomicAdd(&sp[23], wr);
   const unsigned int mo = __reduce_max_sync(full, solve ? outer : 0u), mt = __reduce_max_sync(full, tsat_max);
   if ((tid & 31) == 0) {
     if (mo) atomicMax(&sp[4], mo);
@@ -242,9 +261,11 @@ __device__ __forceinline__ void block_ptmu_counters(DevStats* st, unsigned int s
   }
   if (solve) atomicAdd(&sp[6 + (outer < 16 ? (outer >= 1 ? outer - 1 : 0) : 15)], 1u);
   __syncthreads();
-  if (tid < 22 && sp[tid]) {
+  if (tid < 24 && sp[tid]) {
     const unsigned long long x = sp[tid];
     switch (tid) {
+      case 22: atomicAdd(&st->ptmu_seeded, x); break;
+      case 23: atomicAdd(&st->ptmu_seed_rejected, x); break;
       case 0: atomicAdd(&st->ptmu_solves, x); break;
       case 1: atomicAdd(&st->ptmu_outer, x); break;
       case 2: atomicAdd(&st->ptmu_tsat_calls, x); break;

@@ -79,6 +79,8 @@ struct DevStats {
   // their iterations (sum, max)
   unsigned long long ptmu_solves, ptmu_outer, ptmu_outer_max, ptmu_tsat_calls, ptmu_tsat_iters, ptmu_tsat_max;
   unsigned long long ptmu_hist[16];
+  unsigned long long ptmu_seeded, ptmu_seed_rejected;
+  unsigned long long bounds_violations;  // bounds-checked builds: accesses outside their buffer (skipped)
 };
 
 }  // namespace ecg

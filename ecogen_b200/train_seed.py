@@ -1,6 +1,6 @@
 """Trains the relaxation-seed MLPs shipped in ecogen_b200/models/ (on the GPU, with the library's kernels).
 
-    python -m ecogen_b200.train_seed [--family cavity3d|bubble2d|tube1d] [--pairs 2000000] [--epochs 20]
+    python -m ecogen_b200.train_seed [--family cavity3d|bubble2d|tube1d|ptmu] [--pairs 2000000] [--epochs 20]
 
 cavity3d (three phases, models/seed_np3.npz): pairs recorded by the plain solver on 3D
 cavity-collapse cases whose inclusion seeds (1000..) are disjoint from the benchmark case's seed
@@ -8,7 +8,9 @@ cavity-collapse cases whose inclusion seeds (1000..) are disjoint from the bench
 positions and bubble radii than the benchmark case.  tube1d (two phases,
 models/seed_np2_tube1d.npz): first-order 1D water/air shock tubes with other left pressures and
 interface positions than the benchmark tube (1e9 Pa at 0.7).  Prints the training loss per epoch
-and the recording statistics.
+and the recording statistics.  ptmu (models/seed_ptmu.npz, 8 -> 64 -> 64 -> 2): (p*, T_sat) of the
+saturation solves of the p-T-mu relaxation, recorded on 2D expansion tubes with other strip velocities
+and vapour fractions than the benchmark case.
 """
 from __future__ import annotations
 
@@ -26,7 +28,7 @@ MODELS = os.path.join(HERE, "models")
 
 
 FAMILIES = {"cavity3d": (3, "seed_np3.npz", 64), "bubble2d": (2, "seed_np2.npz", 512),
-            "tube1d": (2, "seed_np2_tube1d.npz", 1000)}
+            "tube1d": (2, "seed_np2_tube1d.npz", 1000), "ptmu": (2, "seed_ptmu.npz", 256)}
 
 
 def training_cases(family: str, n: int):
@@ -34,6 +36,11 @@ def training_cases(family: str, n: int):
         specs = [(3e8, 0.6), (6e8, 0.75), (2e9, 0.65), (1e8, 0.5), (8e8, 0.8), (5e9, 0.7)]
         return [cases.shock_tube_1d(ncells=n, iterations=10 ** 6, p_left=pl, x_interface=xi, name=f"tube{s}")
                 for s, (pl, xi) in enumerate(specs)]
+    if family == "ptmu":  # expansion tubes with other strip velocities and vapour fractions than the
+        # benchmark's (500 m/s, alpha_vap 1e-2)
+        specs = [(300.0, 5e-3), (700.0, 2e-2), (400.0, 1.5e-2), (600.0, 7e-3)]
+        return [cases.expansion_tube_2d(n=n, iterations=10 ** 6, velocity=v, alpha_vap=a, name=f"expansion{s}")
+                for s, (v, a) in enumerate(specs)]
     if family == "cavity3d":
         return [cases.cavity_collapse_3d(n=n, iterations=10 ** 6, seed=1000 + s, ninclusions=max(8, (n // 16) ** 3),
                                          radius_cells=(3.0, 10.0)) for s in range(6)]
@@ -58,7 +65,10 @@ def main():
     steps, warm = args.steps, args.warm
     if args.family == "tube1d":  # small cases: record along the whole run
         steps, warm = max(steps, 400), 0
-    x, y = seed.record(training_cases(args.family, n), steps=steps, max_pairs=args.pairs, warm=warm)
+    # the p-T-mu seed learns from every saturation solve, the pressure seed from the hard relaxations
+    min_evals = 1 if args.family == "ptmu" else 2
+    x, y = seed.record(training_cases(args.family, n), steps=steps, max_pairs=args.pairs, warm=warm,
+                       min_evals=min_evals)
     t1 = time.time()
     model, losses = seed.train(x, y, epochs=args.epochs, batch=8192, lr=2e-3, log=print)
     t2 = time.time()

@@ -119,6 +119,10 @@ typedef struct {
   int64_t ptmu_tsat_iters;
   int64_t ptmu_tsat_max;
   int64_t ptmu_outer_hist[16];
+  int64_t ptmu_seeded;          /* saturation solves started from the learned (p*, T) seed */
+  int64_t ptmu_seed_rejected;   /* learned (p*, T) seeds rejected (plain start) */
+  int64_t bounds_violations;    /* bounds-checked builds (-DECG_BOUNDS_CHECK) only: device accesses outside
+                                   their buffer, counted and skipped; always 0 in the regular build */
 } ecg_step_stats;
 
 typedef struct ecg_ctx ecg_ctx;
@@ -247,25 +251,40 @@ typedef struct {
   const float* b1;              /* [hidden] */
   const float* w2;              /* [hidden][hidden] */
   const float* b2;              /* [hidden] */
-  const float* w3;              /* [hidden] */
+  const float* w3;              /* [n_out][hidden] */
   float b3;
   float in_shift[ECG_MLP_MAX_IN], in_scale[ECG_MLP_MAX_IN]; /* feature normalisation */
   float out_shift, out_scale;   /* target de-normalisation */
+  /* A second output (n_out = 2; 0 reads as 1): its bias and de-normalisation.  The two-output network
+   * (8 -> 64 -> 64 -> 2) seeds the p-T-mu saturation solve with (p*, T_sat(p*)). */
+  int32_t n_out;
+  float b3_1, out_shift_1, out_scale_1;
 } ecg_mlp;
-/* Installs (copies) the weights; NULL restores the plain start sum_k alpha_k p_k.  With a model the
- * step makes the plain iteration's first Newton evaluation for every cell and starts the cells it
- * leaves unconverged again from the network's seed (kept only when finite and inside the bracket of
- * the phase pressures); Newton still stops at |f| <= 1e-10. */
+/* Installs (copies) the weights; NULL restores the plain starts.
+ * Pressure relaxation (n_in = 3 N, n_out = 1): the step makes the plain iteration's first Newton
+ * evaluation for every cell and starts the cells it leaves unconverged again from the network's seed
+ * (kept only when finite and inside the bracket of the phase pressures); Newton still stops at
+ * |f| <= 1e-10.
+ * p-T-mu relaxation (a case with ptmu; n_in = 8, n_out = 2): the saturation Newton on p* starts from
+ * the network's p* and the T_sat(p) Newton of its first iteration from the network's T (later ones
+ * from the previous iteration's T_sat); a seed that is not finite and positive, or a p* at or above
+ * the critical pressure, is rejected (plain start, counted).  Both Newton loops still stop at
+ * |f| <= 1e-10, so the plain iteration remains the judge; the pressure relaxation runs plain. */
 ecg_status ecg_set_seed_model(ecg_ctx* ctx, const ecg_mlp* mlp);
-/* Records up to max_pairs (features, converged pressure) pairs from the relaxations of the next
- * ecg_step calls that took at least min_evals Newton evaluations (1 = all) into an internal device
- * buffer; ecg_fetch_pairs copies them out. */
+/* Records up to max_pairs (features, targets) pairs from the relaxations of the next ecg_step calls
+ * into an internal device buffer; ecg_fetch_pairs copies them out.  Pressure relaxation: 3 N features,
+ * one target (the relaxed pressure's place in the bracket of the phase pressures), relaxations that
+ * took at least min_evals Newton evaluations (1 = all).  p-T-mu relaxation: 8 features, two targets
+ * (ln p*, T_sat(p*)) of every saturation solve (min_evals: at least that many p* iterations). */
 ecg_status ecg_record_pairs(ecg_ctx* ctx, int64_t max_pairs, int32_t min_evals);
 ecg_status ecg_fetch_pairs(ecg_ctx* ctx, float* features, float* targets, int64_t* count);
 
 /* ------------------------------------------------------------------ MLP training on the GPU */
 typedef struct ecg_trainer ecg_trainer;
 ecg_status ecg_trainer_create(int32_t n_in, int32_t hidden, uint64_t seed, ecg_trainer** out);
+/* The same with n_out outputs (1 or 2): targets y are then n x n_out, the loss sums the outputs' mean
+ * squared errors, and ecg_trainer_grad's gw3 / gb3 hold n_out x hidden and n_out values. */
+ecg_status ecg_trainer_create_n(int32_t n_in, int32_t n_out, int32_t hidden, uint64_t seed, ecg_trainer** out);
 void ecg_trainer_destroy(ecg_trainer* tr);
 /* One AdamW epoch over (x, y) (host arrays, n rows), minibatches of `batch`; returns mean loss. */
 ecg_status ecg_trainer_epoch(ecg_trainer* tr, const float* x, const float* y, int64_t n, int32_t batch, float lr,
@@ -280,6 +299,8 @@ ecg_status ecg_trainer_export(ecg_trainer* tr, ecg_mlp* out);
 ecg_status ecg_trainer_import(ecg_trainer* tr, const ecg_mlp* in);
 ecg_status ecg_trainer_set_norm(ecg_trainer* tr, const float* in_shift, const float* in_scale, float out_shift,
                                 float out_scale);
+/* De-normalisation of the second output of a two-output trainer (out_shift_1 / out_scale_1). */
+ecg_status ecg_trainer_set_norm_out1(ecg_trainer* tr, float out_shift, float out_scale);
 
 /* ------------------------------------------------------------------ batched independent cases */
 /* Many independent 1D cases of uneven cell counts advanced together by one persistent kernel per
