@@ -496,6 +496,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="default", choices=["default", "split", "fused"],
                     help="form of the 2D / 3D Kapila passes (ecg_set_step_form); default: the library's")
+    ap.add_argument("--staging", default="default", choices=["default", "tma", "plain"],
+                    help="face-kernel tile staging of the split form (default: TMA where the mesh allows)")
     args = ap.parse_args()
     rank, world, local = env_rank()
     case = make_case(args.config, args.size)
@@ -552,6 +554,8 @@ def main():
         c = api.Context(inp.case)
         if args.form != "default":
             c.set_step_form(api.FORM_SPLIT if args.form == "split" else api.FORM_FUSED)
+        if args.staging != "default":
+            c.set_face_staging(api.STAGING_TMA if args.staging == "tma" else api.STAGING_PLAIN)
         return c
 
     ctx = new_context()
@@ -605,11 +609,35 @@ def main():
                   "seeded": st3.seeded, "seed_rejected": st3.seed_rejected, "fallback": st3.newton_fallback,
                   "field_rel_l1_vs_plain": diff, "model": os.path.relpath(model_path, ROOT)}
         if case.ptmu is not None:  # the p-T-mu saturation solve: iterations with and without the seed
-            seeded.update({"ptmu_seeded": st3.ptmu_seeded, "ptmu_seed_rejected": st3.ptmu_seed_rejected,
+            seeded.update({"ptmu_seed_mode": "T", "ptmu_seeded": st3.ptmu_seeded,
+                           "ptmu_seed_rejected": st3.ptmu_seed_rejected,
                            "ptmu_outer_iters_per_solve": st3.ptmu_outer_iters / max(1, st3.ptmu_solves),
                            "plain_ptmu_outer_iters_per_solve": st_ref.ptmu_outer_iters / max(1, st_ref.ptmu_solves),
                            "tsat_iters_per_solve": st3.ptmu_tsat_iters / max(1, st3.ptmu_solves),
                            "plain_tsat_iters_per_solve": st_ref.ptmu_tsat_iters / max(1, st_ref.ptmu_solves)})
+            # the alternative: the network's p* starts the saturation Newton as well
+            ctx4 = new_context()
+            ctx4.upload(fields0)
+            model.install(ctx4)
+            ctx4.set_ptmu_seed(api.PTMU_SEED_P_T)
+            ctx4.step(args.warmup)
+            stream4 = torch.cuda.ExternalStream(api.lib().ecg_stream(ctx4.h))
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream4)
+            st4 = ctx4.step(args.steps)
+            q1.record(stream4)
+            q1.synchronize()
+            ms4 = q0.elapsed_time(q1)
+            d4 = ctx4.download_dict()
+            seeded["p_and_T"] = {
+                "value": case.ncells * args.steps / (ms4 * 1e-3), "speedup_vs_plain": ms_max / ms4,
+                "ptmu_outer_iters_per_solve": st4.ptmu_outer_iters / max(1, st4.ptmu_solves),
+                "tsat_iters_per_solve": st4.ptmu_tsat_iters / max(1, st4.ptmu_solves),
+                "ptmu_seed_rejected": st4.ptmu_seed_rejected,
+                "field_rel_l1_vs_plain": max(float(np.abs(a[k] - d4[k]).sum() / max(np.abs(a[k]).sum(), 1e-300))
+                                             for k in ("alpha", "rho", "p", "E"))}
+            ctx4.close()
         ref_ctx.close()
         ctx3.close()
         if case.ptmu is None:
@@ -641,6 +669,9 @@ def main():
     step_ms = sum(kms) / nprof
     kernel_ms = {name: v / nprof for name, v in zip(KERNEL_SLOTS, kms) if v > 0.0}
     form = "split" if ctx.step_form == api.FORM_SPLIT else "fused"
+    config["form"] = form
+    if form == "split":
+        config["face_staging"] = "tma" if ctx.face_staging == api.STAGING_TMA else "plain"
 
     # ---- end to end through the C ABI with host buffers: upload from pinned host memory, one
     #      ecg_step call per step (host -> device dt/t, device -> host dt/t/counters), download

@@ -19,6 +19,8 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported case", 3: "CUDA error"
           5: "physics check failed", 6: "out of memory", 7: "size above the stated maximum", 8: "device wait timed out"}
 MODEL_KAPILA, MODEL_EULER, MODEL_PTUEQ = 0, 1, 2
 FORM_FUSED, FORM_SPLIT = 0, 1
+STAGING_PLAIN, STAGING_TMA = 0, 1
+PTMU_SEED_T, PTMU_SEED_P_T = 0, 1
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
@@ -59,7 +61,8 @@ class StepStats(C.Structure):
                 ("newton_hist", C.c_int64 * 16), ("ptmu_solves", C.c_int64), ("ptmu_outer_iters", C.c_int64),
                 ("ptmu_outer_max", C.c_int64), ("ptmu_tsat_calls", C.c_int64), ("ptmu_tsat_iters", C.c_int64),
                 ("ptmu_tsat_max", C.c_int64), ("ptmu_outer_hist", C.c_int64 * 16), ("ptmu_seeded", C.c_int64),
-                ("ptmu_seed_rejected", C.c_int64), ("bounds_violations", C.c_int64)]
+                ("ptmu_seed_rejected", C.c_int64), ("bounds_violations", C.c_int64),
+                ("staging_timeouts", C.c_int64)]
 
     def as_dict(self) -> Dict[str, object]:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("newton_hist", "ptmu_outer_hist")}
@@ -117,6 +120,10 @@ def lib():
     L.ecg_set_step_form.argtypes = [vp, C.c_int32]
     L.ecg_step_form.restype = C.c_int32
     L.ecg_step_form.argtypes = [vp]
+    L.ecg_set_face_staging.argtypes = [vp, C.c_int32]
+    L.ecg_face_staging.restype = C.c_int32
+    L.ecg_face_staging.argtypes = [vp]
+    L.ecg_set_ptmu_seed.argtypes = [vp, C.c_int32]
     L.ecg_step_noalloc.argtypes = [P(Case), vp, vp, C.c_double, dp, P(StepStats), vp]
     L.ecg_ncells.restype = C.c_int64
     L.ecg_ncells.argtypes = [vp]
@@ -326,6 +333,19 @@ class Context:
     @property
     def step_form(self) -> int:
         return int(lib().ecg_step_form(self.h))
+
+    def set_face_staging(self, staging: int):
+        """STAGING_TMA (default where the mesh allows) or STAGING_PLAIN (ecg_set_face_staging)."""
+        check(lib().ecg_set_face_staging(self.h, staging), "ecg_set_face_staging")
+
+    @property
+    def face_staging(self) -> int:
+        """The staging the next split-form step uses (ecg_face_staging)."""
+        return int(lib().ecg_face_staging(self.h))
+
+    def set_ptmu_seed(self, mode: int):
+        """PTMU_SEED_T (default) or PTMU_SEED_P_T: what a p-T-mu seed model starts (ecg_set_ptmu_seed)."""
+        check(lib().ecg_set_ptmu_seed(self.h, mode), "ecg_set_ptmu_seed")
 
     def run(self) -> StepStats:
         st = StepStats()

@@ -19,6 +19,7 @@
 #include "ecg_internal.h"
 #include "ecg_mlp_device.cuh"
 #include "ecg_step.cuh"
+#include "ecg_tma.cuh"
 
 namespace ecg {
 
@@ -115,6 +116,8 @@ struct ecg_ctx {
   double* tmp = nullptr;      // download scratch (mixture pressure)
   double* flux[3] = {nullptr, nullptr, nullptr};  // face arrays of the split form (Kapila 2D / 3D)
   bool split = false;         // step passes in split form (face kernels + cell kernel)
+  FaceMaps fmaps{};           // tensor maps of the face kernels' TMA staging (fmaps.ok = 0: none)
+  int staging = ECG_STAGING_TMA;
   DevScalars* scal = nullptr;
   DevStats* stats = nullptr;
   // pinned host staging of the scalars and counters an ecg_step call exchanges (asynchronous copies,
@@ -123,6 +126,7 @@ struct ecg_ctx {
   DevStats* h_stats = nullptr;
   int cur = 0;
   int newton_cap = 100;
+  int ptmu_seed_p = 0;  // ECG_PTMU_SEED_P_T: the network's p* starts the saturation Newton too
   MlpDev* mlp = nullptr;
   float* rec_x = nullptr;
   float* rec_y = nullptr;
@@ -150,6 +154,74 @@ ecg_status cuda_fail(cudaError_t e, const char* what) {
 }  // namespace
 
 namespace ecg {
+
+}  // namespace ecg
+
+namespace ecg {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// The two maps (all primitive fields; field 0 alone) of buffer b for the face kernels of axis AX.
+template <int AX>
+static bool encode_axis(EncodeTiledFn enc, FaceMaps& m, int b, int dim, const cuuint64_t* gdim, const cuuint64_t* gstr,
+                        int nq) {
+  using FT = FaceTile<AX>;
+  const cuuint32_t rank = (cuuint32_t)(dim + 1);
+  cuuint32_t box[4], es[4] = {1, 1, 1, 1};
+  for (int d = 0; d < dim; d++) box[d] = (cuuint32_t)FT::box(d);
+  void* base = const_cast<double*>(m.buf[b]);
+  for (int which = 0; which < 2; which++) {
+    box[dim] = which == 0 ? (cuuint32_t)nq : 1u;
+    CUtensorMap* out = which == 0 ? &m.q[b][AX] : &m.a0[b][AX];
+    if (enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
+
+bool build_face_maps(FaceMaps& m, const double* const bufs[3], int dim, const int n[3], int nq) {
+  std::memset(&m, 0, sizeof(m));
+  // 2D meshes are x-y meshes; a row of x cells must be a multiple of 16 bytes (tensor strides)
+  if (dim < 2 || dim > 3 || (dim == 2 && n[2] != 1) || (n[0] & 1)) return false;
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  cuuint64_t gdim[4], gstr[3];
+  gdim[0] = (cuuint64_t)n[0];
+  gdim[1] = (cuuint64_t)n[1];
+  if (dim == 3) gdim[2] = (cuuint64_t)n[2];
+  gdim[dim] = (cuuint64_t)nq;
+  gstr[0] = (cuuint64_t)n[0] * sizeof(double);
+  if (dim == 3) gstr[1] = (cuuint64_t)n[0] * n[1] * sizeof(double);
+  gstr[dim - 1] = (cuuint64_t)n[0] * n[1] * n[2] * sizeof(double);
+  for (int b = 0; b < 3; b++) {
+    m.buf[b] = bufs[b];
+    if (!bufs[b]) continue;
+    if (!encode_axis<0>(enc, m, b, dim, gdim, gstr, nq) || !encode_axis<1>(enc, m, b, dim, gdim, gstr, nq) ||
+        (dim == 3 && !encode_axis<2>(enc, m, b, dim, gdim, gstr, nq))) {
+      std::memset(&m, 0, sizeof(m));
+      return false;
+    }
+  }
+  m.ok = 1;
+  return true;
+}
 
 }  // namespace ecg
 
@@ -197,7 +269,9 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.ptmu_liq = x->c.ptmu_liquid;
   P.ptmu_vap = x->c.ptmu_vapor;
   P.pcrit = x->pcrit;
+  P.ptmu_seed_p = x->ptmu_seed_p;
   for (int a = 0; a < 3; a++) P.flux[a] = x->split ? x->flux[a] : nullptr;
+  P.fmaps = (x->split && x->staging == ECG_STAGING_TMA && x->fmaps.ok) ? &x->fmaps : nullptr;
   double* sn = x->state[parity];
   double* s1 = x->state[1 - parity];
   const bool euler = x->c.model == ECG_MODEL_EULER;
@@ -309,6 +383,7 @@ void stats_out(const DevStats& d, int64_t updates, ecg_step_stats* st) {
   st->ptmu_seeded = (int64_t)d.ptmu_seeded;
   st->ptmu_seed_rejected = (int64_t)d.ptmu_seed_rejected;
   st->bounds_violations = (int64_t)d.bounds_violations;
+  st->staging_timeouts = (int64_t)d.staging_timeouts;
 }
 }  // namespace ecg
 
@@ -481,6 +556,12 @@ extern "C" ecg_status ecg_create(const ecg_case* c, ecg_ctx** out) {
       if (e != cudaSuccess) return fail_free(cuda_fail(e, "cudaMalloc(face fluxes)"));
     }
     x->split = true;
+#ifndef ECG_BOUNDS_CHECK
+    // TMA staging of the face kernels' tiles where the layout allows it (the bounds-checked build
+    // checks the kernels' own loads, so it stages them that way)
+    const double* bufs[3] = {x->state[0], x->state[1], x->half};
+    build_face_maps(x->fmaps, bufs, x->dim, c->ncells, x->nq);
+#endif
   }
   std::vector<double> h, sz[3], ctr[3];
   for (int a = 0; a < 3; a++) axis_cells(*c, a, sz[a], ctr[a]);
@@ -588,6 +669,17 @@ extern "C" ecg_status ecg_set_step_form(ecg_ctx* x, int32_t form) {
 }
 
 extern "C" int32_t ecg_step_form(const ecg_ctx* x) { return (x && x->split) ? ECG_FORM_SPLIT : ECG_FORM_FUSED; }
+
+extern "C" ecg_status ecg_set_face_staging(ecg_ctx* x, int32_t staging) {
+  if (!x || (staging != ECG_STAGING_PLAIN && staging != ECG_STAGING_TMA)) { set_error("bad staging"); return ECG_ERR_INVALID; }
+  x->staging = staging;
+  x->graph_dirty = true;
+  return ECG_OK;
+}
+
+extern "C" int32_t ecg_face_staging(const ecg_ctx* x) {
+  return (x && x->split && x->staging == ECG_STAGING_TMA && x->fmaps.ok) ? ECG_STAGING_TMA : ECG_STAGING_PLAIN;
+}
 
 extern "C" ecg_status ecg_set_newton_cap(ecg_ctx* x, int32_t cap) {
   if (!x || cap < 1 || cap > 100000) { set_error("bad Newton cap"); return ECG_ERR_INVALID; }
@@ -840,6 +932,10 @@ static ecg_status step_common(ecg_ctx* x, int mode, int32_t nsteps, double* dt, 
   *t = r.t;
   if (iterations) *iterations = (int32_t)r.it;
   if (stats) stats_out(ds, done_steps * x->n, stats);
+  if (ds.staging_timeouts) {
+    set_error("a face kernel's TMA staging copy did not complete");
+    return ECG_ERR_CUDA;
+  }
   if (ds.ptmu_errors) {
     set_error("p-T-mu relaxation exceeded 50 iterations");
     return ECG_ERR_PHYSICS;
@@ -880,6 +976,13 @@ extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
   if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
   if (x->c.ntransports > 0) { set_error("the seeded kernels run without passive transports"); return ECG_ERR_UNSUPPORTED; }
   return mlp_upload(m, x->np, x->c.ptmu != 0, &x->mlp, x->stream);
+}
+
+extern "C" ecg_status ecg_set_ptmu_seed(ecg_ctx* x, int32_t mode) {
+  if (!x || (mode != ECG_PTMU_SEED_T && mode != ECG_PTMU_SEED_P_T)) { set_error("bad p-T-mu seed mode"); return ECG_ERR_INVALID; }
+  x->ptmu_seed_p = mode == ECG_PTMU_SEED_P_T ? 1 : 0;
+  x->graph_dirty = true;
+  return ECG_OK;
 }
 
 extern "C" ecg_status ecg_record_pairs(ecg_ctx* x, int64_t max_pairs, int32_t min_evals) {

@@ -607,6 +607,9 @@ struct PtmuCount {
 
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
 // T0 > 0: the Newton iteration starts there instead of at 0.1 B / C (a seeded p-T-mu relaxation).
+// f(T) = A + B / T + C ln T - ... falls for T < B / C and is convex there, so Newton started anywhere
+// below B / C reaches the root the cold start 0.1 B / C reaches; a start at or beyond 0.5 B / C is not
+// taken (cold start).
 __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
                                                bool& err, PtmuCount* pc = nullptr, double T0 = -1.) {
   double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
@@ -616,7 +619,7 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
   double C = (gV * cvV - gL * cvL) / (gV * cvV - cvV);
   double D = (gL * cvL - cvL) / (gV * cvV - cvV);
   int iteration = 0;
-  double Tsat = (T0 > 0.) ? T0 : 0.1 * B / C, f = 0., df = 1.;
+  double Tsat = (T0 > 0. && T0 < 0.5 * B / C) ? T0 : 0.1 * B / C, f = 0., df = 1.;
   // ln(p + pInf) of both phases do not depend on the iterate: evaluated once per solve (the same
   // values enter the same sum, so f has the bits of the reference's per-iteration evaluation)
   const double lnV = cr_log(p + piV), lnL = cr_log(p + piL);
@@ -671,9 +674,11 @@ __device__ __forceinline__ double eos_rhoe_sat(const EosParams& q, double p, dou
 // when the phases were updated (the reference then calls fulfillState, so the mixture density
 // is recomputed from the new phases).
 //
-// Seeded form (p_seed > 0): the Newton iteration on p* starts at p_seed instead of sum_k alpha_k p_k, the
-// T_sat(p) solves start at T_seed (pure-phase tests and the first Newton iteration) and then at the
-// previous iteration's T_sat; every loop still stops at |f| <= 1e-10.
+// Seeded forms: T_seed > 0: the T_sat(p) solves of the saturation Newton start at T_seed (the first)
+// and then at the previous iteration's T_sat, instead of the cold start 0.1 B / C of every solve (the
+// pure-phase tests keep the cold start, so they decide as the reference does); p_seed > 0: the Newton
+// iteration on p* starts at p_seed instead of sum_k alpha_k p_k.  Every loop still stops at
+// |f| <= 1e-10.
 template <int NP>
 __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap, double pcrit, double a[NP],
                                            double r[NP], double p[NP], double rhomix, double emix, bool& err,
@@ -688,7 +693,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pv = eos_p(EV, M.eps, rho, emix);
   double Tv = eos_T(EV, M.eps, rho, pv);
   if (pv > 0) {
-    Tsat = compute_tsat(EL, EV, pv, &dTsat, err, pc, T_seed);
+    Tsat = compute_tsat(EL, EV, pv, &dTsat, err, pc);
     if (Tv >= Tsat) {
       a[vap] = 1.;
       a[liq] = 0.;
@@ -700,7 +705,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double pl = eos_p(EL, M.eps, rho, emix);
   double Tl = eos_T(EL, M.eps, rho, pl);
   if (pl > 0.) {
-    Tsat = compute_tsat(EL, EV, pl, &dTsat, err, pc, T_seed);
+    Tsat = compute_tsat(EL, EV, pl, &dTsat, err, pc);
     if (Tl <= Tsat) {
       a[liq] = 1.;
       a[vap] = 0.;
@@ -725,7 +730,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
 #pragma unroll
     for (int k = 0; k < NP; k++) pStar = eos_fix_p(M.eos[k], pStar);
     Tsat = compute_tsat(EL, EV, pStar, &dTsat, err, pc, Tstart);
-    if (p_seed > 0.) Tstart = Tsat;
+    if (T_seed > 0.) Tstart = Tsat;
     rhoLSat = eos_rho_sat(EL, M.eps, pStar, Tsat, dTsat, &drhoLSat);
     rhoVSat = eos_rho_sat(EV, M.eps, pStar, Tsat, dTsat, &drhoVSat);
     aLSat = (rho - rhoVSat) / (rhoLSat - rhoVSat);

@@ -365,8 +365,12 @@ __device__ __forceinline__ void ptmu_seed_gate(const StepParams& P, const Model<
   mlp_ptmu_seed_warp(P.mlp, active, g.ptmu_x, ps, Ts);
   g.ptmu_p = g.ptmu_T = -1.;
   if (!active) return;
-  if (isfinite(ps) && isfinite(Ts) && ps > 0. && ps < P.pcrit && Ts > 0.) {
-    g.ptmu_p = ps;
+  // the T start is used when finite and positive; the p* start (ECG_PTMU_SEED_P_T only) when finite,
+  // positive and below the critical pressure as well
+  const bool okT = isfinite(Ts) && Ts > 0.;
+  const bool okP = !P.ptmu_seed_p || (isfinite(ps) && ps > 0. && ps < P.pcrit);
+  if (okT && okP) {
+    g.ptmu_p = P.ptmu_seed_p ? ps : -1.;
     g.ptmu_T = Ts;
   } else {
     cc.pc.rejected = 1;
@@ -495,7 +499,7 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
 #pragma unroll
       for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
     }
-    if (SEED && cc.pc.solve && ps > 0.) cc.pc.seeded = 1;
+    if (SEED && cc.pc.solve && Ts > 0.) cc.pc.seeded = 1;
     if (P.rec_x != nullptr && cc.pc.solve && !err && (int)cc.pc.outer >= P.rec_min_evals) {
       float x[PTMU_NIN];
       if (SEED) {

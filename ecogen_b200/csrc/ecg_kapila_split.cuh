@@ -27,6 +27,7 @@
 // so that consecutive threads of either kernel touch consecutive faces.
 #pragma once
 #include "ecg_kapila_kernel.cuh"
+#include "ecg_tma.cuh"
 
 namespace ecg {
 
@@ -36,43 +37,36 @@ __device__ __forceinline__ int64_t split_fid(const int n[3], int ax, int f, int 
   return (int64_t)i + (int64_t)n[0] * ((int64_t)j + (int64_t)n[1] * f);
 }
 
-// Block of the face kernel of axis AX: TF faces along AX times W lines along the fastest other axis
-// (Y lines for X faces, X lines for Y and Z faces), one thread per face; the block's third coordinate
-// is blockIdx.z.  Shared planes are laid out so that the linear thread order is the storage order.
-// A line of X faces has n_x + 1 faces, so its last chunk holds a single face: chunks of 16 faces keep
-// more lanes busy than chunks of 32 on short lines (257 faces at 256^3: 94 % against 89 %).
-#ifndef ECG_XFACE_TF
-#define ECG_XFACE_TF 16
-#endif
-template <int AX>
-struct FaceTile {
-  static constexpr int TF = (AX == 0) ? ECG_XFACE_TF : 8;
-  static constexpr int W = (AX == 0) ? 128 / ECG_XFACE_TF : 16;
-  static constexpr int NTH = TF * W;
-  static constexpr int CP = TF + 3;  // staged cells per line: f0-2 .. f0+TF
-  static constexpr int SP = TF + 2;  // slopes per line: faces f0-1 .. f0+TF
-  static constexpr int RS = W * CP;  // one staged plane
-  static constexpr int SS = W * SP;  // one slope plane
-  __host__ __device__ static constexpr int cidx(int line, int pos) { return AX == 0 ? line * CP + pos : pos * W + line; }
-  __host__ __device__ static constexpr int sidx(int line, int s) { return AX == 0 ? line * SP + s : s * W + line; }
-};
-
 template <int NP, int DIM, int AX, int PASS>
 struct FaceKernelShape {
   using FL = Fields<NP, DIM>;
   using FT = FaceTile<AX>;
   static constexpr bool O2 = (PASS != PASS_O1);
   static constexpr int NA0 = (PASS == PASS_CORR) ? 1 : 0;  // separate time-n alpha_0 plane
+  static constexpr size_t staged_bytes() { return sizeof(double) * (size_t)FT::RS * (FL::NQ + NA0); }
+  // staged planes, slope planes, the staging mbarrier, and room to align the base to 128 bytes
   static constexpr size_t smem_bytes() {
-    return sizeof(double) * ((size_t)FT::RS * (FL::NQ + NA0) + (O2 ? (size_t)FT::SS * FL::NSL : 0));
+    return staged_bytes() + (O2 ? sizeof(double) * (size_t)FT::SS * FL::NSL : 0) + sizeof(uint64_t) + 128;
   }
 };
 
-#ifndef ECG_FACE_MINB
-#define ECG_FACE_MINB 6
+// Resident blocks per SM asked of the face and cell kernels (registers 65536 / (128 x MINB)).  Measured
+// on one B200 (cell-updates/s): 2D shock-bubble 2048^2: face kernels at 6 blocks 1459 M, at 8 1533 M,
+// cell kernel at 8 1470 M; 3D three-phase cavity 256^3: face kernels at 6 blocks 656 M, at 8 642 M, cell
+// kernel at 8 604 M.
+#ifndef ECG_FACE_MINB_2D
+#define ECG_FACE_MINB_2D 8
+#endif
+#ifndef ECG_FACE_MINB_3D
+#define ECG_FACE_MINB_3D 6
 #endif
 #ifndef ECG_CELL_MINB
 #define ECG_CELL_MINB 6
+#endif
+// The face kernels reconstruct the two sides of a face through one copy of the code (a loop kept
+// rolled), which halves that part of the kernel's instruction footprint.
+#ifndef ECG_FACE_ROLLED
+#define ECG_FACE_ROLLED 1
 #endif
 #ifndef ECG_CELL_PTMU_MINB
 #define ECG_CELL_PTMU_MINB 4
@@ -80,15 +74,19 @@ struct FaceKernelShape {
 constexpr int CELL_THREADS = 128;
 
 template <int NP, int DIM, int AX, int PASS, int TYPES>
-__global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
-    k_kapila_faces(StepParams P, Geometry G, Model<NP> M0, double* __restrict__ flux) {
+__global__ void __launch_bounds__(FaceTile<AX>::NTH, DIM == 2 ? ECG_FACE_MINB_2D : ECG_FACE_MINB_3D)
+    k_kapila_faces(StepParams P, Geometry G, Model<NP> M0, double* __restrict__ flux,
+                   const __grid_constant__ CUtensorMap mq, const __grid_constant__ CUtensorMap ma0, int tma) {
   const Model<NP> M = specialize_eos<NP, TYPES>(M0);
   using FT = FaceTile<AX>;
   using KS = FaceKernelShape<NP, DIM, AX, PASS>;
   using FL = Fields<NP, DIM>;
   constexpr bool O2 = KS::O2;
   constexpr int RS = FT::RS, SS = FT::SS, CP = FT::CP;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // 128-byte aligned base for the tensor copies (offset taken in the shared window, so the compiler
+  // keeps every access a shared-memory access)
+  double* smem = reinterpret_cast<double*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
   double* sq = smem;                                // [NQ][RS]
   double* sa0 = sq + (size_t)FL::NQ * RS;           // [NA0][RS]
   double* ssl = sa0 + (size_t)KS::NA0 * RS;         // [NSL][SS]
@@ -109,17 +107,42 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
     g[AX == 2 ? 1 : 2] = third;
   };
 
-  // ---- stage the cells f0-2 .. f0+TF of every line
-  for (int e = tid; e < RS; e += FT::NTH) {
-    const int line = AX == 0 ? e / CP : e % FT::W, pos = AX == 0 ? e % CP : e / FT::W;
-    int g[3];
-    coords(line, f0 - 2 + pos, g);
-    if (g[AX] >= 0 && g[AX] < nax && g[ob] < G.n[ob]) {
-      const int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
-      if (!ECG_IN_BOUNDS(P.stats, c, nn)) continue;
+  // ---- stage the cells f0-2 .. f0-3+CP of every line
+  if (tma) {
+    // one tensor copy of the box (x, y[, z], field) for all primitive fields, one for the time-n
+    // alpha_0 plane; cells outside the mesh arrive as zeros
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + KS::staged_bytes() / sizeof(double) +
+                                                (O2 ? (size_t)FT::SS * FL::NSL : 0));
+    if (tid == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+      mbar_expect_tx(bar, (uint32_t)KS::staged_bytes());
+      int o[3];  // box origin along x, y, z
+      o[AX] = f0 - 2;
+      o[ob] = l0;
+      o[AX == 2 ? 1 : 2] = third;
+      if (DIM == 3) {
+        tma_load_4d(sq, &mq, bar, o[0], o[1], o[2], 0);
+        if (KS::NA0) tma_load_4d(sa0, &ma0, bar, o[0], o[1], o[2], FL::A);
+      } else {
+        tma_load_3d(sq, &mq, bar, o[0], o[1], 0);
+        if (KS::NA0) tma_load_3d(sa0, &ma0, bar, o[0], o[1], FL::A);
+      }
+    }
+    // bounded wait; a copy that never lands is reported to the host (the step then fails)
+    if (!mbar_wait_bounded(bar, 0, 1 << 22) && (tid & 31) == 0) atomicAdd(&P.stats->staging_timeouts, 1ull);
+  } else {
+    for (int e = tid; e < RS; e += FT::NTH) {
+      const int line = AX == 0 ? e / CP : e % FT::W, pos = AX == 0 ? e % CP : e / FT::W;
+      int g[3];
+      coords(line, f0 - 2 + pos, g);
+      if (g[AX] >= 0 && g[AX] < nax && g[ob] < G.n[ob]) {
+        const int64_t c = (int64_t)g[0] + (int64_t)g[1] * G.n[0] + (int64_t)g[2] * G.n[0] * G.n[1];
+        if (!ECG_IN_BOUNDS(P.stats, c, nn)) continue;
 #pragma unroll
-      for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
-      if (KS::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
+        for (int f = 0; f < FL::NQ; f++) sq[f * RS + e] = P.q[(int64_t)f * nn + c];
+        if (KS::NA0) sa0[e] = P.sn[(int64_t)FL::A * nn + c];
+      }
     }
   }
   __syncthreads();
@@ -169,81 +192,101 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, ECG_FACE_MINB)
       Flux<NP> F;
       double Fn[3];
       const int gl = f - 1;
-      if (f == 0 || f == nax) {
+      // the states either side of the face in its frame, then one HLLC solve (or a symmetry side's
+      // reflecting flux): one copy of the solver's code in the kernel
+      const bool side = (f == 0 || f == nax);
+      const int sd = (f == 0) ? 0 : 1;
+      const bool neg = side && sd == 0;
+      const bool wall = side && G.bc[2 * AX + sd] == ECG_BC_SYMMETRY;
+      Thermo<NP> tl, tr;
+      double ul[3], ur[3], lL, lR;
+      if (side) {
         // a side: non-reflecting HLLC(cell, cell) in the side's frame (BoundCondNonReflecting::
         // solveRiemannBoundary src/BoundConds/BoundCondNonReflecting.cpp:62), or a symmetry side's
         // reflecting flux (ModUEq::solveRiemannWall src/Models/UEq/ModUEq.cpp:452) of the buffer cell,
         // MUSCL-extrapolated towards the side (BoundCondWallO2Cartesian::solveRiemann :111-141)
-        const int sd = (f == 0) ? 0 : 1;
-        const bool neg = sd == 0;
         const int rc = FT::cidx(line, sd == 0 ? fl + 2 : fl + 1);
         int gc[3] = {g[0], g[1], g[2]};  // the side's cell
         gc[AX] = sd == 0 ? 0 : nax - 1;
-        const double lc = cell_lcfl(G, gc[0], gc[1], gc[2]);
-        Thermo<NP> t;
-        double ug[3], ul[3];
-        if (G.bc[2 * AX + sd] == ECG_BC_SYMMETRY) {
-          if (O2) {
-            const int fw = FT::sidx(line, fl + 1), fo = FT::sidx(line, sd == 0 ? fl + 2 : fl);
-            wall_side<NP, DIM>(M, P.lim, sq, RS, rc, ssl, SS, fw, fo, a0[rc], G.wdist[2 * AX + sd], t, ug);
-          } else {
-            cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
-          }
-          to_local(AX, neg, ug, ul);
-          const double pstar = wall_pstar<NP>(t, ul, lc, dtmax);
-#pragma unroll
-          for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
-          F.E = 0.;
-          F.sM = 0.;
-          F.uStar = 0.;
-          Fn[0] = pstar;
-          Fn[1] = 0.;
-          Fn[2] = 0.;
+        lL = lR = cell_lcfl(G, gc[0], gc[1], gc[2]);
+        double ug[3];
+        if (O2 && wall) {
+          const int fw = FT::sidx(line, fl + 1), fo = FT::sidx(line, sd == 0 ? fl + 2 : fl);
+          wall_side<NP, DIM>(M, P.lim, sq, RS, rc, ssl, SS, fw, fo, a0[rc], G.wdist[2 * AX + sd], tl, ug);
         } else {
-          cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
-          to_local(AX, neg, ug, ul);
-          hllc<NP>(M, t, ul, t, ul, lc, lc, dtmax, Fn, F);
+          cell_thermo<NP, DIM>(M, sq, RS, rc, tl, ug);
         }
-        to_global(AX, neg, Fn, F.mom);
+        to_local(AX, neg, ug, ul);
+        tr = tl;
+#pragma unroll
+        for (int d = 0; d < 3; d++) ur[d] = ul[d];
       } else {
         // internal face between cells gl and gl + 1 (positions fl + 1 and fl + 2)
         const int rl = FT::cidx(line, fl + 1), rr = FT::cidx(line, fl + 2);
-        Thermo<NP> tl, tr;
-        double ug[3], vg[3];
-        if (!O2) {
-          cell_thermo<NP, DIM>(M, sq, RS, rl, tl, ug);
-          cell_thermo<NP, DIM>(M, sq, RS, rr, tr, vg);
-        } else {
-          const int f1 = FT::sidx(line, fl + 1);  // this face
-          const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
-          // beyond a symmetry side the opposite slope is the side's and alphaCellAfterOppositeSide is the
-          // cell's own time-n alpha (CellO2Cartesian::computeLocalSlopes :68-71); a non-reflecting side
-          // has neither
-          const bool wL = !hasL && G.bc[2 * AX] == ECG_BC_SYMMETRY;
-          const bool wR = !hasR && G.bc[2 * AX + 1] == ECG_BC_SYMMETRY;
-          const int f2l = (hasL || wL) ? FT::sidx(line, fl) : -1;      // face (gl-1, gl)
-          const int f2r = (hasR || wR) ? FT::sidx(line, fl + 2) : -1;  // face (gl+1, gl+2)
-          const double aL = sq[FL::A * RS + rl], aR = sq[FL::A * RS + rr];
-          const double aLL = hasL ? a0[FT::cidx(line, fl)] : (wL ? a0[rl] : 0.);
-          const double aRR = hasR ? a0[FT::cidx(line, fl + 3)] : (wR ? a0[rr] : 0.);
-          constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
-          constexpr int kLim = code_limiter(TYPES);
-          reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[AX][gl], 1.,
-                                                  tl, ug);
-          reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[AX][gl], -1.,
-                                                  tr, vg);
+        const int f1 = FT::sidx(line, fl + 1);  // this face
+        const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
+        // beyond a symmetry side the opposite slope is the side's and alphaCellAfterOppositeSide is the
+        // cell's own time-n alpha (CellO2Cartesian::computeLocalSlopes :68-71); a non-reflecting side
+        // has neither
+        const bool wL = !hasL && G.bc[2 * AX] == ECG_BC_SYMMETRY;
+        const bool wR = !hasR && G.bc[2 * AX + 1] == ECG_BC_SYMMETRY;
+        const int f2l = (hasL || wL) ? FT::sidx(line, fl) : -1;      // face (gl-1, gl)
+        const int f2r = (hasR || wR) ? FT::sidx(line, fl + 2) : -1;  // face (gl+1, gl+2)
+        double aL = 0., aR = 0., aLL = 0., aRR = 0.;
+        if (O2) {
+          aL = sq[FL::A * RS + rl];
+          aR = sq[FL::A * RS + rr];
+          aLL = hasL ? a0[FT::cidx(line, fl)] : (wL ? a0[rl] : 0.);
+          aRR = hasR ? a0[FT::cidx(line, fl + 3)] : (wR ? a0[rr] : 0.);
         }
-        double ul[3], ur[3];
-        to_local(AX, false, ug, ul);
-        to_local(AX, false, vg, ur);
+        constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
+        constexpr int kLim = code_limiter(TYPES);
+        // left side, then right side, through one copy of the reconstruction code
+#if ECG_FACE_ROLLED
+#pragma unroll 1
+#endif
+        for (int s = 0; s < 2; s++) {
+          const bool R = s != 0;
+          Thermo<NP> t;
+          double w[3], wl[3];
+          if (!O2) {
+            cell_thermo<NP, DIM>(M, sq, RS, R ? rr : rl, t, w);
+          } else {
+            reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, R ? rr : rl, ssl, SS, f1, R ? f2r : f2l,
+                                                    R ? aR : aL, R ? aL : aR, R ? aRR : aLL,
+                                                    R ? G.dfr[AX][gl] : G.dfl[AX][gl], R ? -1. : 1., t, w);
+          }
+          to_local(AX, false, w, wl);
+          if (R) {
+            tr = t;
+#pragma unroll
+            for (int d = 0; d < 3; d++) ur[d] = wl[d];
+          } else {
+            tl = t;
+#pragma unroll
+            for (int d = 0; d < 3; d++) ul[d] = wl[d];
+          }
+        }
         int gf[3] = {g[0], g[1], g[2]};  // the face's left cell, then its right cell: their CFL lengths
         gf[AX] = gl;
-        const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+        lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
         gf[AX] = gl + 1;
-        const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
-        hllc<NP>(M, tl, ul, tr, ur, lL, lR, dtmax, Fn, F);
-        to_global(AX, false, Fn, F.mom);
+        lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
       }
+      if (wall) {
+        const double pstar = wall_pstar<NP>(tl, ul, lL, dtmax);
+#pragma unroll
+        for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
+        F.E = 0.;
+        F.sM = 0.;
+        F.uStar = 0.;
+        Fn[0] = pstar;
+        Fn[1] = 0.;
+        Fn[2] = 0.;
+      } else {
+        hllc<NP>(M, tl, ul, tr, ur, lL, lR, dtmax, Fn, F);
+      }
+      to_global(AX, neg, Fn, F.mom);
       const int64_t nfa = split_nfaces(G.n, AX);
       const int64_t fid = split_fid(G.n, AX, f, g[0], g[1], g[2]);
       if (ECG_IN_BOUNDS(P.stats, fid, nfa)) {
@@ -377,12 +420,27 @@ cudaError_t launch_faces(const StepParams& P, const Geometry& G, const Model<NP>
   auto kern = k_kapila_faces<NP, DIM, AX, PASS, TYPES>;
   const size_t sm = FaceKernelShape<NP, DIM, AX, PASS>::smem_bytes();
   if (prepare) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  // tensor maps of the buffers this pass reads (TMA staging), when the context built them
+  CUtensorMap mq{}, ma0{};
+  int tma = 0;
+  if (P.fmaps && P.fmaps->ok) {
+    const CUtensorMap *q = nullptr, *a = nullptr;
+    for (int b = 0; b < 3; b++) {
+      if (P.fmaps->buf[b] && P.fmaps->buf[b] == P.q) q = &P.fmaps->q[b][AX];
+      if (P.fmaps->buf[b] && P.fmaps->buf[b] == P.sn) a = &P.fmaps->a0[b][AX];
+    }
+    if (q && (PASS != PASS_CORR || a)) {
+      mq = *q;
+      if (a) ma0 = *a;
+      tma = 1;
+    }
+  }
   const int nax = G.n[AX], ob = AX == 0 ? 1 : 0, third = AX == 2 ? G.n[1] : G.n[2];
   dim3 grid, blk(FT::NTH);
   const unsigned gf = (unsigned)((nax + 1 + FT::TF - 1) / FT::TF), gl = (unsigned)((G.n[ob] + FT::W - 1) / FT::W);
   if (AX == 0) grid = dim3(gf, gl, (unsigned)third);
   else grid = dim3(gl, gf, (unsigned)third);
-  kern<<<grid, blk, sm, s>>>(P, G, M, P.flux[AX]);
+  kern<<<grid, blk, sm, s>>>(P, G, M, P.flux[AX], mq, ma0, tma);
   return cudaGetLastError();
 }
 

@@ -25,14 +25,22 @@ __device__ __forceinline__ void mlp_features(const double a[NP], const double r[
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     x[3 * k + 0] = (float)a[k];
-    x[3 * k + 1] = (float)log(r[k] > 1e-300 ? r[k] : 1e-300);
-    x[3 * k + 2] = (float)asinh(p[k] * 1.e-5);
+    x[3 * k + 1] = logf(fmaxf((float)r[k], 1e-30f));  // single precision: the features enter as BF16
+    x[3 * k + 2] = asinhf((float)(p[k] * 1.e-5));
   }
 }
 
+// GELU (tanh form) of the inference path with the SFU's tanh (tanh.approx.f32, relative error about
+// 2^-11): its result is rounded to BF16 for the next layer, 2^-8 relative, so the approximation is below
+// the network's own precision.  Training evaluates the same formula with tanhf.
+__device__ __forceinline__ float tanh_sfu(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu_f(float x) {
   const float c = 0.7978845608028654f;  // sqrt(2/pi)
-  return 0.5f * x * (1.f + tanhf(c * (x + 0.044715f * x * x * x)));
+  return 0.5f * x * (1.f + tanh_sfu(c * (x + 0.044715f * x * x * x)));
 }
 
 // Appends one (features, target) pair of a converged relaxation to the recording buffer.
@@ -233,14 +241,15 @@ __device__ __forceinline__ void ptmu_features(const Model<NP>& M, int liq, int v
 #pragma unroll
   for (int k = 0; k < NP; k++) ps += a[k] * p[k];
   const double pv = eos_p(M.eos[vap], M.eps, rhomix, emix), pl = eos_p(M.eos[liq], M.eps, rhomix, emix);
-  x[0] = (float)log(rhomix > 1e-300 ? rhomix : 1e-300);
-  x[1] = (float)asinh(emix * 1.e-5);
+  // single precision: the features enter the network as BF16
+  x[0] = logf(fmaxf((float)rhomix, 1e-30f));
+  x[1] = asinhf((float)(emix * 1.e-5));
   x[2] = (float)a[liq];
-  x[3] = (float)log(r[liq] > 1e-300 ? r[liq] : 1e-300);
-  x[4] = (float)log(r[vap] > 1e-300 ? r[vap] : 1e-300);
-  x[5] = (float)asinh(ps * 1.e-5);
-  x[6] = (float)asinh(pv * 1.e-5);
-  x[7] = (float)asinh(pl * 1.e-5);
+  x[3] = logf(fmaxf((float)r[liq], 1e-30f));
+  x[4] = logf(fmaxf((float)r[vap], 1e-30f));
+  x[5] = asinhf((float)(ps * 1.e-5));
+  x[6] = asinhf((float)(pv * 1.e-5));
+  x[7] = asinhf((float)(pl * 1.e-5));
 }
 
 // Appends one (features, ln p*, T_sat) record of a converged saturation solve.

@@ -49,8 +49,8 @@ __global__ void __launch_bounds__(TH) k_mlp_fwd_bwd(MlpDev P, int nin, const flo
   float* sh1 = sx + TROWS * nin;       // [TROWS][TH]
   float* sz1 = sh1 + TROWS * TH;       // [TROWS][TH]  (gelu' of layer 1)
   float* sdz2 = sz1 + TROWS * TH;      // [TROWS][TH]
-  float* sy = sdz2 + TROWS * TH;       // [TROWS][NOUT]
-  float* gW1 = sy + TROWS;             // [TH][nin] gradient accumulators (row j owned by thread j)
+  float* sy = sdz2 + TROWS * TH;       // [TROWS][NOUT], room for two outputs
+  float* gW1 = sy + 2 * TROWS;         // [TH][nin] gradient accumulators (row j owned by thread j)
   float* gW2 = gW1 + TH * nin;         // [TH][TH]
   const int j = threadIdx.x;
   const bool train = (G.w1 != nullptr);

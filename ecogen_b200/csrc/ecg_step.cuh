@@ -124,6 +124,7 @@ struct StepParams {
   // p-T-mu relaxation
   int ptmu, ptmu_liq, ptmu_vap;
   double pcrit;
+  int ptmu_seed_p;  // seeded p-T-mu: 1 = the network's p* starts the saturation Newton too (else T only)
   // THINC reconstruction of alpha (a volume-fraction limiter is THINC): cosh and tanh of the
   // sharpness beta = 1.6, evaluated once on the host like the reference does
   int thinc;
@@ -136,6 +137,8 @@ struct StepParams {
   // kernels run), and optional events recorded after each axis' face kernel (profiling)
   double* flux[3];
   cudaEvent_t* split_ev;
+  // host side: tensor maps of the face kernels' TMA staging (nullptr: the kernels load their tiles)
+  const struct FaceMaps* fmaps;
 };
 
 // Host side of the THINC parameters (CellInterfaceO2Cartesian::solveRiemann's beta = 1.6).

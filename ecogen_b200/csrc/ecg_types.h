@@ -81,6 +81,7 @@ struct DevStats {
   unsigned long long ptmu_hist[16];
   unsigned long long ptmu_seeded, ptmu_seed_rejected;
   unsigned long long bounds_violations;  // bounds-checked builds: accesses outside their buffer (skipped)
+  unsigned long long staging_timeouts;   // face-kernel warps whose TMA staging wait ran out
 };
 
 }  // namespace ecg

@@ -123,6 +123,8 @@ typedef struct {
   int64_t ptmu_seed_rejected;   /* learned (p*, T) seeds rejected (plain start) */
   int64_t bounds_violations;    /* bounds-checked builds (-DECG_BOUNDS_CHECK) only: device accesses outside
                                    their buffer, counted and skipped; always 0 in the regular build */
+  int64_t staging_timeouts;     /* face-kernel warps whose wait for a TMA staging copy ran out (the step
+                                   then returns ECG_ERR_CUDA); 0 in a healthy run */
 } ecg_step_stats;
 
 typedef struct ecg_ctx ecg_ctx;
@@ -198,6 +200,14 @@ ecg_status ecg_step_profiled_kernels(ecg_ctx* ctx, int32_t nsteps, double* dt, d
 enum { ECG_FORM_FUSED = 0, ECG_FORM_SPLIT = 1 };
 ecg_status ecg_set_step_form(ecg_ctx* ctx, int32_t form);
 int32_t ecg_step_form(const ecg_ctx* ctx);
+/* How the split form's face kernels stage their cell tiles in shared memory.  ECG_STAGING_TMA (the
+ * default): one tensor copy (cp.async.bulk.tensor through a tensor map of the state) per block, where
+ * the layout allows one (an even number of cells along x); elsewhere, and with ECG_STAGING_PLAIN, the
+ * threads load the tiles themselves.  Both give the same bits. */
+enum { ECG_STAGING_PLAIN = 0, ECG_STAGING_TMA = 1 };
+ecg_status ecg_set_face_staging(ecg_ctx* ctx, int32_t staging);
+/* The staging the next split-form step uses: ECG_STAGING_TMA only where the maps exist. */
+int32_t ecg_face_staging(const ecg_ctx* ctx);
 /* Runs the reference time loop to its stop condition (iterations or total time), in chunks
  * captured as CUDA graphs. */
 ecg_status ecg_run(ecg_ctx* ctx, double* dt, double* t, int32_t* iterations, ecg_step_stats* stats);
@@ -265,12 +275,18 @@ typedef struct {
  * evaluation for every cell and starts the cells it leaves unconverged again from the network's seed
  * (kept only when finite and inside the bracket of the phase pressures); Newton still stops at
  * |f| <= 1e-10.
- * p-T-mu relaxation (a case with ptmu; n_in = 8, n_out = 2): the saturation Newton on p* starts from
- * the network's p* and the T_sat(p) Newton of its first iteration from the network's T (later ones
- * from the previous iteration's T_sat); a seed that is not finite and positive, or a p* at or above
- * the critical pressure, is rejected (plain start, counted).  Both Newton loops still stop at
- * |f| <= 1e-10, so the plain iteration remains the judge; the pressure relaxation runs plain. */
+ * p-T-mu relaxation (a case with ptmu; n_in = 8, n_out = 2): what the network starts is set by
+ * ecg_set_ptmu_seed; a seed that is not finite and positive (a p* at or above the critical pressure)
+ * is rejected (plain start, counted).  Both Newton loops still stop at |f| <= 1e-10, so the plain
+ * iteration remains the judge; the pressure relaxation runs plain. */
 ecg_status ecg_set_seed_model(ecg_ctx* ctx, const ecg_mlp* mlp);
+/* What the learned seed of a p-T-mu case starts.  ECG_PTMU_SEED_T (the default): the T_sat(p) Newton
+ * solves (Mixture::computeTsat, cold start 0.1 B / C at src/Models/Mixture.cpp:85) -- the first from
+ * the network's T_sat(p*), each later one from the previous solve's result -- while the saturation
+ * Newton on p* starts at sum_k alpha_k p_k as in the reference (RelaxationPTMu.cpp:129).
+ * ECG_PTMU_SEED_P_T: the saturation Newton starts from the network's p* as well. */
+enum { ECG_PTMU_SEED_T = 0, ECG_PTMU_SEED_P_T = 1 };
+ecg_status ecg_set_ptmu_seed(ecg_ctx* ctx, int32_t mode);
 /* Records up to max_pairs (features, targets) pairs from the relaxations of the next ecg_step calls
  * into an internal device buffer; ecg_fetch_pairs copies them out.  Pressure relaxation: 3 N features,
  * one target (the relaxed pressure's place in the bracket of the phase pressures), relaxations that

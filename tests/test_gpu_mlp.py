@@ -54,7 +54,7 @@ def test_training_reduces_loss():
     assert losses[-1] < 0.1 * losses[0]
 
 
-def _run(case, tmp, model=None):
+def _run(case, tmp, model=None, ptmu_mode=None):
     import os
     os.makedirs(str(tmp), exist_ok=True)
     d = case.write(str(tmp))
@@ -63,6 +63,8 @@ def _run(case, tmp, model=None):
     ctx.upload(inp.fill())
     if model is not None:
         model.install(ctx)
+    if ptmu_mode is not None:
+        ctx.set_ptmu_seed(ptmu_mode)
     st = ctx.step(case.iterations)
     out = ctx.download_dict()
     ctx.close()
@@ -102,9 +104,14 @@ def test_seeded_relaxation_same_residual_fewer_iterations(tmp_path):
 
 @pytest.mark.gpu
 def test_ptmu_seed_fewer_saturation_iterations_same_residual(tmp_path):
-    """The (p*, T) seed of the p-T-mu saturation solve: trained on expansion tubes unlike the test case,
-    it must cut the T_sat(p) Newton iterations (the cold start 0.1 B / C is far from T_sat) and keep the
-    fields within the spread the solve's own 1e-10 residual allows."""
+    """The (p*, T) network of the p-T-mu saturation solve, trained on expansion tubes unlike the test case.
+
+    Its T starts the T_sat(p) Newton solves (the reference starts every one cold at 0.1 B / C, far from
+    T_sat), so they must take far fewer iterations, while the saturation Newton on p* keeps the plain
+    start (sum_k alpha_k p_k, already within one or two iterations) and its iteration count.  An untrained
+    network asked the same must do worse than the trained one, and starting p* from the network as well
+    (ECG_PTMU_SEED_P_T) is the measured alternative: it converges to the same residual with more p*
+    iterations.  Fields stay within the spread the solves' own 1e-10 residuals allow."""
     train_cases = [cases.expansion_tube_2d(n=48, iterations=10, velocity=v, alpha_vap=a, name=f"trainPTMu{i}")
                    for i, (v, a) in enumerate([(300.0, 5e-3), (700.0, 2e-2), (400.0, 1.5e-2)])]
     x, y = seed.record(train_cases, steps=10, max_pairs=200000, min_evals=1)
@@ -116,9 +123,27 @@ def test_ptmu_seed_fewer_saturation_iterations_same_residual(tmp_path):
     plain, st0 = _run(test_case, tmp_path / "plain")
     seeded, st1 = _run(test_case, tmp_path / "seeded", model)
     assert st0.ptmu_seeded == 0 and st1.ptmu_seeded > 0.9 * st1.ptmu_solves
-    assert st1.ptmu_errors == 0
-    assert st1.ptmu_tsat_iters < 0.6 * st0.ptmu_tsat_iters, (st1.ptmu_tsat_iters, st0.ptmu_tsat_iters)
-    assert st1.ptmu_outer_iters <= st0.ptmu_outer_iters
+    assert st1.ptmu_errors == 0 and st1.ptmu_solves == st0.ptmu_solves
+    assert st1.ptmu_tsat_iters < 0.5 * st0.ptmu_tsat_iters, (st1.ptmu_tsat_iters, st0.ptmu_tsat_iters)
+    assert abs(st1.ptmu_outer_iters - st0.ptmu_outer_iters) <= 0.02 * st0.ptmu_outer_iters
     for name in ("alpha", "rho", "E"):
         assert rel_l1(seeded[name], plain[name]) < 1e-8, name
     assert rel_l1(seeded["p"], plain["p"]) < 1e-6
+    # what training buys: random weights with the same normalisation give worse T starts
+    tr = seed.Trainer(8, seed=7, n_out=2)
+    untrained = tr.model()
+    um = untrained.mlp
+    for i in range(8):
+        um.in_shift[i], um.in_scale[i] = model.mlp.in_shift[i], model.mlp.in_scale[i]
+    um.out_shift, um.out_scale = model.mlp.out_shift, model.mlp.out_scale
+    um.out_shift_1, um.out_scale_1 = model.mlp.out_shift_1, model.mlp.out_scale_1
+    _, st2 = _run(test_case, tmp_path / "untrained", untrained)
+    tr.close()
+    assert st2.ptmu_errors == 0
+    assert st1.ptmu_tsat_iters < st2.ptmu_tsat_iters, (st1.ptmu_tsat_iters, st2.ptmu_tsat_iters)
+    # p* from the network too: same residual, not fewer p* iterations than the plain start
+    both, st3 = _run(test_case, tmp_path / "both", model, ptmu_mode=api.PTMU_SEED_P_T)
+    assert st3.ptmu_errors == 0 and st3.ptmu_seeded > 0.9 * st3.ptmu_solves
+    assert st3.ptmu_outer_iters >= st0.ptmu_outer_iters
+    for name in ("alpha", "rho", "E"):
+        assert rel_l1(both[name], plain[name]) < 1e-8, name

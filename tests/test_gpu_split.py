@@ -5,7 +5,9 @@ cell in the reference's face order, so after N steps every field, dt, t and ever
 must be identical -- not merely close.  The cases cover the kernel variants the split form runs:
 EOS types and limiter compiled in (the benchmark's), generic EOS with THINC, symmetry / wall sides
 in MUSCL and first order, three phases in 3D, p-T-mu relaxation, the learned seed, and meshes whose
-sizes are not multiples of the face-kernel blocks.
+sizes are not multiples of the face-kernel blocks.  The face kernels stage their tiles by TMA tensor
+copies where the mesh allows (an even number of x cells) and by their own loads elsewhere; both stagings
+must give the same bits too.
 """
 import os
 
@@ -60,12 +62,16 @@ SPLIT_CASES = {
 }
 
 
-def _run(case, tmp, form, steps, model=None):
+def _run(case, tmp, form, steps, model=None, staging=None):
     d = case.write(str(tmp))
     inp = api.Input(d, os.path.join(str(tmp), "libEOS"))
     ctx = api.Context(inp.case)
     assert ctx.step_form == api.FORM_SPLIT  # the default for 2D / 3D Kapila cases
+    # TMA staging is the default wherever the x rows allow a tensor copy (even number of x cells)
+    assert ctx.face_staging == (api.STAGING_TMA if case.cells[0] % 2 == 0 else api.STAGING_PLAIN)
     ctx.set_step_form(form)
+    if staging is not None:
+        ctx.set_face_staging(staging)
     ctx.upload(inp.fill())
     if model is not None:
         model.install(ctx)
@@ -124,4 +130,65 @@ def test_split_form_is_refused_where_it_does_not_apply(tmp_path):
     assert ctx.step_form == api.FORM_FUSED
     with pytest.raises(api.EcgError):
         ctx.set_step_form(api.FORM_SPLIT)
+    ctx.close()
+
+
+TMA_CASES = {
+    "bubble2d_vanleer": lambda: cases.shock_bubble_2d(n=70, iterations=12, name="tmaBubble"),
+    "bubble2d_walls_o1": lambda: _walls_o1_even(),
+    "bubble2d_stretched_walls": _stretched,
+    "cavity3d_3phase_minmod": lambda: cases.cavity_collapse_3d(n=26, iterations=6, ninclusions=12,
+                                                               radius_cells=(2.0, 5.0), name="tmaCavity"),
+    "cavity3d_walls": _walls3d,
+    "expansion2d_ptmu": lambda: cases.expansion_tube_2d(n=48, iterations=8, name="tmaPTMu"),
+}
+
+
+def _walls_o1_even():
+    c = cases.shock_bubble_2d(n=34, iterations=10, limiter=None, name="tmaWallsO1")
+    c.boundaries = ["symmetry", "wall", "nonReflecting", "symmetry"]
+    return c
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", list(TMA_CASES))
+def test_tma_staging_equals_plain_staging(key, tmp_path):
+    """Tensor-copy staging of the face kernels' tiles against the kernels' own loads: the same bits, on
+    meshes whose sizes are not multiples of the blocks (partial boxes at the ends of the lines, zero-filled
+    cells outside the mesh), with walls, first order and MUSCL, 2D and 3D."""
+    case = TMA_CASES[key]()
+    assert case.cells[0] % 2 == 0
+    steps = case.iterations
+    (tmp_path / "t").mkdir()
+    (tmp_path / "p").mkdir()
+    tma = _run(case, tmp_path / "t", api.FORM_SPLIT, steps, staging=api.STAGING_TMA)
+    plain = _run(case, tmp_path / "p", api.FORM_SPLIT, steps, staging=api.STAGING_PLAIN)
+    _same(tma, plain)
+    assert tma[1]["staging_timeouts"] == 0
+
+
+@pytest.mark.gpu
+def test_staging_setting_and_odd_rows(tmp_path):
+    """An odd number of x cells leaves no 16-byte row stride for a tensor map: the context reports plain
+    staging and runs it; the fused form has no face kernels to stage for."""
+    case = cases.shock_bubble_2d(n=37, iterations=2, name="tmaOdd")
+    d = case.write(str(tmp_path))
+    inp = api.Input(d, os.path.join(str(tmp_path), "libEOS"))
+    ctx = api.Context(inp.case)
+    assert ctx.face_staging == api.STAGING_PLAIN
+    ctx.set_face_staging(api.STAGING_TMA)  # accepted, but no maps exist for this mesh
+    assert ctx.face_staging == api.STAGING_PLAIN
+    ctx.close()
+    even = cases.shock_bubble_2d(n=38, iterations=2, name="tmaEven")
+    d = even.write(str(tmp_path / "e"))
+    inp = api.Input(d, os.path.join(str(tmp_path / "e"), "libEOS"))
+    ctx = api.Context(inp.case)
+    assert ctx.face_staging == api.STAGING_TMA
+    ctx.set_face_staging(api.STAGING_PLAIN)
+    assert ctx.face_staging == api.STAGING_PLAIN
+    ctx.set_face_staging(api.STAGING_TMA)
+    ctx.set_step_form(api.FORM_FUSED)
+    assert ctx.face_staging == api.STAGING_PLAIN
+    with pytest.raises(api.EcgError):
+        ctx.set_face_staging(7)
     ctx.close()
