@@ -607,6 +607,7 @@ def main():
                   "newton_evals_per_relaxation": st3.newton_evals / max(1, st3.relax_calls),
                   "plain_newton_evals_per_relaxation": st_ref.newton_evals / max(1, st_ref.relax_calls),
                   "seeded": st3.seeded, "seed_rejected": st3.seed_rejected, "fallback": st3.newton_fallback,
+                  "nonfinite_cells": st3.nonfinite_cells,
                   "field_rel_l1_vs_plain": diff, "model": os.path.relpath(model_path, ROOT)}
         if case.ptmu is not None:  # the p-T-mu saturation solve: iterations with and without the seed
             seeded.update({"ptmu_seed_mode": "T", "ptmu_seeded": st3.ptmu_seeded,

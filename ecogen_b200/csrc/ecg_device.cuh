@@ -607,9 +607,11 @@ struct PtmuCount {
 
 // Mixture::computeTsat src/Models/Mixture.cpp:59-100 (liquid and vapour IG/SG).
 // T0 > 0: the Newton iteration starts there instead of at 0.1 B / C (a seeded p-T-mu relaxation).
-// f(T) = A + B / T + C ln T - ... falls for T < B / C and is convex there, so Newton started anywhere
-// below B / C reaches the root the cold start 0.1 B / C reaches; a start at or beyond 0.5 B / C is not
-// taken (cold start).
+// With B / C > 0, f(T) = A + B / T + C ln T - ... is monotone and of one curvature on (0, B / C), the
+// branch the cold start 0.1 B / C converges on: a start left of the root approaches it monotonically, a
+// start right of it jumps left of it in one step, possibly past T = 0.  So a start is taken only inside
+// (0, 0.5 B / C), and an iterate that leaves (0, B / C) sends the iteration back to the cold start
+// (at most once); either way it converges to the root the reference's iteration finds.
 __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosParams& V, double p, double* dTsat,
                                                bool& err, PtmuCount* pc = nullptr, double T0 = -1.) {
   double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
@@ -619,12 +621,17 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
   double C = (gV * cvV - gL * cvL) / (gV * cvV - cvV);
   double D = (gL * cvL - cvL) / (gV * cvV - cvV);
   int iteration = 0;
-  double Tsat = (T0 > 0. && T0 < 0.5 * B / C) ? T0 : 0.1 * B / C, f = 0., df = 1.;
+  bool seeded = T0 > 0. && T0 < 0.5 * B / C;
+  double Tsat = seeded ? T0 : 0.1 * B / C, f = 0., df = 1.;
   // ln(p + pInf) of both phases do not depend on the iterate: evaluated once per solve (the same
   // values enter the same sum, so f has the bits of the reference's per-iteration evaluation)
   const double lnV = cr_log(p + piV), lnL = cr_log(p + piL);
   do {
     Tsat -= f / df;
+    if (seeded && !(Tsat > 0. && Tsat < B / C)) {  // a seeded iterate left the root's branch
+      seeded = false;
+      Tsat = 0.1 * B / C;
+    }
     iteration++;
     if (iteration > 50) {
       err = true;

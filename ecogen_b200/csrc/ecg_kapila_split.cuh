@@ -63,15 +63,19 @@ struct FaceKernelShape {
 #ifndef ECG_CELL_MINB
 #define ECG_CELL_MINB 6
 #endif
-// The face kernels reconstruct the two sides of a face through one copy of the code (a loop kept
-// rolled), which halves that part of the kernel's instruction footprint.
-#ifndef ECG_FACE_ROLLED
-#define ECG_FACE_ROLLED 1
+// The p-T-mu cell kernels run one warp per block: their cells take very different numbers of Newton
+// iterations, and in 4-warp blocks the warps that finish first waited at the block's counter reduction
+// for the slowest one (barrier stalls were 5.6 of 12.4 cycles between issues on the 1024^2 expansion),
+// holding their slots; a one-warp block frees its slot for the next block as soon as it is done.
+// 16 such blocks per SM keep the 128-register budget of 4 blocks of 4 warps.
+#ifndef ECG_CELL_PTMU_THREADS
+#define ECG_CELL_PTMU_THREADS 32
 #endif
 #ifndef ECG_CELL_PTMU_MINB
-#define ECG_CELL_PTMU_MINB 4
+#define ECG_CELL_PTMU_MINB (512 / ECG_CELL_PTMU_THREADS)
 #endif
 constexpr int CELL_THREADS = 128;
+__host__ __device__ constexpr int cell_threads(bool ptmu) { return ptmu ? ECG_CELL_PTMU_THREADS : CELL_THREADS; }
 
 template <int NP, int DIM, int AX, int PASS, int TYPES>
 __global__ void __launch_bounds__(FaceTile<AX>::NTH, DIM == 2 ? ECG_FACE_MINB_2D : ECG_FACE_MINB_3D)
@@ -83,10 +87,8 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, DIM == 2 ? ECG_FACE_MINB_2D
   using FL = Fields<NP, DIM>;
   constexpr bool O2 = KS::O2;
   constexpr int RS = FT::RS, SS = FT::SS, CP = FT::CP;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  // 128-byte aligned base for the tensor copies (offset taken in the shared window, so the compiler
-  // keeps every access a shared-memory access)
-  double* smem = reinterpret_cast<double*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+  extern __shared__ unsigned char smem_raw[];
+  double* smem = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
   double* sq = smem;                                // [NQ][RS]
   double* sa0 = sq + (size_t)FL::NQ * RS;           // [NA0][RS]
   double* ssl = sa0 + (size_t)KS::NA0 * RS;         // [NSL][SS]
@@ -192,101 +194,81 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, DIM == 2 ? ECG_FACE_MINB_2D
       Flux<NP> F;
       double Fn[3];
       const int gl = f - 1;
-      // the states either side of the face in its frame, then one HLLC solve (or a symmetry side's
-      // reflecting flux): one copy of the solver's code in the kernel
-      const bool side = (f == 0 || f == nax);
-      const int sd = (f == 0) ? 0 : 1;
-      const bool neg = side && sd == 0;
-      const bool wall = side && G.bc[2 * AX + sd] == ECG_BC_SYMMETRY;
-      Thermo<NP> tl, tr;
-      double ul[3], ur[3], lL, lR;
-      if (side) {
+      if (f == 0 || f == nax) {
         // a side: non-reflecting HLLC(cell, cell) in the side's frame (BoundCondNonReflecting::
         // solveRiemannBoundary src/BoundConds/BoundCondNonReflecting.cpp:62), or a symmetry side's
         // reflecting flux (ModUEq::solveRiemannWall src/Models/UEq/ModUEq.cpp:452) of the buffer cell,
         // MUSCL-extrapolated towards the side (BoundCondWallO2Cartesian::solveRiemann :111-141)
+        const int sd = (f == 0) ? 0 : 1;
+        const bool neg = sd == 0;
         const int rc = FT::cidx(line, sd == 0 ? fl + 2 : fl + 1);
         int gc[3] = {g[0], g[1], g[2]};  // the side's cell
         gc[AX] = sd == 0 ? 0 : nax - 1;
-        lL = lR = cell_lcfl(G, gc[0], gc[1], gc[2]);
-        double ug[3];
-        if (O2 && wall) {
-          const int fw = FT::sidx(line, fl + 1), fo = FT::sidx(line, sd == 0 ? fl + 2 : fl);
-          wall_side<NP, DIM>(M, P.lim, sq, RS, rc, ssl, SS, fw, fo, a0[rc], G.wdist[2 * AX + sd], tl, ug);
-        } else {
-          cell_thermo<NP, DIM>(M, sq, RS, rc, tl, ug);
-        }
-        to_local(AX, neg, ug, ul);
-        tr = tl;
+        const double lc = cell_lcfl(G, gc[0], gc[1], gc[2]);
+        Thermo<NP> t;
+        double ug[3], ul[3];
+        if (G.bc[2 * AX + sd] == ECG_BC_SYMMETRY) {
+          if (O2) {
+            const int fw = FT::sidx(line, fl + 1), fo = FT::sidx(line, sd == 0 ? fl + 2 : fl);
+            wall_side<NP, DIM>(M, P.lim, sq, RS, rc, ssl, SS, fw, fo, a0[rc], G.wdist[2 * AX + sd], t, ug);
+          } else {
+            cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
+          }
+          to_local(AX, neg, ug, ul);
+          const double pstar = wall_pstar<NP>(t, ul, lc, dtmax);
 #pragma unroll
-        for (int d = 0; d < 3; d++) ur[d] = ul[d];
+          for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
+          F.E = 0.;
+          F.sM = 0.;
+          F.uStar = 0.;
+          Fn[0] = pstar;
+          Fn[1] = 0.;
+          Fn[2] = 0.;
+        } else {
+          cell_thermo<NP, DIM>(M, sq, RS, rc, t, ug);
+          to_local(AX, neg, ug, ul);
+          hllc<NP>(M, t, ul, t, ul, lc, lc, dtmax, Fn, F);
+        }
+        to_global(AX, neg, Fn, F.mom);
       } else {
         // internal face between cells gl and gl + 1 (positions fl + 1 and fl + 2)
         const int rl = FT::cidx(line, fl + 1), rr = FT::cidx(line, fl + 2);
-        const int f1 = FT::sidx(line, fl + 1);  // this face
-        const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
-        // beyond a symmetry side the opposite slope is the side's and alphaCellAfterOppositeSide is the
-        // cell's own time-n alpha (CellO2Cartesian::computeLocalSlopes :68-71); a non-reflecting side
-        // has neither
-        const bool wL = !hasL && G.bc[2 * AX] == ECG_BC_SYMMETRY;
-        const bool wR = !hasR && G.bc[2 * AX + 1] == ECG_BC_SYMMETRY;
-        const int f2l = (hasL || wL) ? FT::sidx(line, fl) : -1;      // face (gl-1, gl)
-        const int f2r = (hasR || wR) ? FT::sidx(line, fl + 2) : -1;  // face (gl+1, gl+2)
-        double aL = 0., aR = 0., aLL = 0., aRR = 0.;
-        if (O2) {
-          aL = sq[FL::A * RS + rl];
-          aR = sq[FL::A * RS + rr];
-          aLL = hasL ? a0[FT::cidx(line, fl)] : (wL ? a0[rl] : 0.);
-          aRR = hasR ? a0[FT::cidx(line, fl + 3)] : (wR ? a0[rr] : 0.);
+        Thermo<NP> tl, tr;
+        double ug[3], vg[3];
+        if (!O2) {
+          cell_thermo<NP, DIM>(M, sq, RS, rl, tl, ug);
+          cell_thermo<NP, DIM>(M, sq, RS, rr, tr, vg);
+        } else {
+          const int f1 = FT::sidx(line, fl + 1);  // this face
+          const bool hasL = (gl - 1 >= 0), hasR = (gl + 2 < nax);
+          // beyond a symmetry side the opposite slope is the side's and alphaCellAfterOppositeSide is the
+          // cell's own time-n alpha (CellO2Cartesian::computeLocalSlopes :68-71); a non-reflecting side
+          // has neither
+          const bool wL = !hasL && G.bc[2 * AX] == ECG_BC_SYMMETRY;
+          const bool wR = !hasR && G.bc[2 * AX + 1] == ECG_BC_SYMMETRY;
+          const int f2l = (hasL || wL) ? FT::sidx(line, fl) : -1;      // face (gl-1, gl)
+          const int f2r = (hasR || wR) ? FT::sidx(line, fl + 2) : -1;  // face (gl+1, gl+2)
+          const double aL = sq[FL::A * RS + rl], aR = sq[FL::A * RS + rr];
+          const double aLL = hasL ? a0[FT::cidx(line, fl)] : (wL ? a0[rl] : 0.);
+          const double aRR = hasR ? a0[FT::cidx(line, fl + 3)] : (wR ? a0[rr] : 0.);
+          constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
+          constexpr int kLim = code_limiter(TYPES);
+          reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, f2l, aL, aR, aLL, G.dfl[AX][gl], 1.,
+                                                  tl, ug);
+          reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, f2r, aR, aL, aRR, G.dfr[AX][gl], -1.,
+                                                  tr, vg);
         }
-        constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
-        constexpr int kLim = code_limiter(TYPES);
-        // left side, then right side, through one copy of the reconstruction code
-#if ECG_FACE_ROLLED
-#pragma unroll 1
-#endif
-        for (int s = 0; s < 2; s++) {
-          const bool R = s != 0;
-          Thermo<NP> t;
-          double w[3], wl[3];
-          if (!O2) {
-            cell_thermo<NP, DIM>(M, sq, RS, R ? rr : rl, t, w);
-          } else {
-            reconstruct_side<NP, DIM, kThinc, kLim>(M, P, sq, RS, R ? rr : rl, ssl, SS, f1, R ? f2r : f2l,
-                                                    R ? aR : aL, R ? aL : aR, R ? aRR : aLL,
-                                                    R ? G.dfr[AX][gl] : G.dfl[AX][gl], R ? -1. : 1., t, w);
-          }
-          to_local(AX, false, w, wl);
-          if (R) {
-            tr = t;
-#pragma unroll
-            for (int d = 0; d < 3; d++) ur[d] = wl[d];
-          } else {
-            tl = t;
-#pragma unroll
-            for (int d = 0; d < 3; d++) ul[d] = wl[d];
-          }
-        }
+        double ul[3], ur[3];
+        to_local(AX, false, ug, ul);
+        to_local(AX, false, vg, ur);
         int gf[3] = {g[0], g[1], g[2]};  // the face's left cell, then its right cell: their CFL lengths
         gf[AX] = gl;
-        lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
+        const double lL = cell_lcfl(G, gf[0], gf[1], gf[2]);
         gf[AX] = gl + 1;
-        lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
-      }
-      if (wall) {
-        const double pstar = wall_pstar<NP>(tl, ul, lL, dtmax);
-#pragma unroll
-        for (int k = 0; k < NP; k++) F.a[k] = F.m[k] = F.en[k] = 0.;
-        F.E = 0.;
-        F.sM = 0.;
-        F.uStar = 0.;
-        Fn[0] = pstar;
-        Fn[1] = 0.;
-        Fn[2] = 0.;
-      } else {
+        const double lR = cell_lcfl(G, gf[0], gf[1], gf[2]);
         hllc<NP>(M, tl, ul, tr, ur, lL, lR, dtmax, Fn, F);
+        to_global(AX, false, Fn, F.mom);
       }
-      to_global(AX, neg, Fn, F.mom);
       const int64_t nfa = split_nfaces(G.n, AX);
       const int64_t fid = split_fid(G.n, AX, f, g[0], g[1], g[2]);
       if (ECG_IN_BOUNDS(P.stats, fid, nfa)) {
@@ -340,14 +322,14 @@ __device__ __forceinline__ void load_face_flux(const double* __restrict__ fl, in
 }
 
 template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES>
-__global__ void __launch_bounds__(CELL_THREADS, PTMU ? ECG_CELL_PTMU_MINB : ECG_CELL_MINB)
+__global__ void __launch_bounds__(cell_threads(PTMU), PTMU ? ECG_CELL_PTMU_MINB : ECG_CELL_MINB)
     k_kapila_cells(StepParams P, Geometry G, Model<NP> M0, const double* __restrict__ fx,
                    const double* __restrict__ fy, const double* __restrict__ fz) {
   const Model<NP> M = specialize_eos<NP, TYPES>(M0);
   using FL = Fields<NP, DIM>;
   if (*P.done) return;
   const int64_t nn = P.n;
-  const int64_t cell = (int64_t)blockIdx.x * CELL_THREADS + threadIdx.x;
+  const int64_t cell = (int64_t)blockIdx.x * cell_threads(PTMU) + threadIdx.x;
   const bool active = cell < nn;
   int g[3] = {0, 0, 0};
   if (active) {
@@ -459,8 +441,9 @@ cudaError_t launch_split(const StepParams& P, const Geometry& G, const ecg_eos* 
   if (DIM > 2 && e == cudaSuccess) e = launch_faces<NP, DIM, (DIM > 2 ? 2 : 0), PASS, TYPES>(P, G, M, s, prepare);
   if (DIM > 2 && e == cudaSuccess && P.split_ev && !prepare) e = cudaEventRecord(P.split_ev[2], s);
   if (e != cudaSuccess || prepare) return e;
-  const unsigned blocks = (unsigned)((P.n + CELL_THREADS - 1) / CELL_THREADS);
-  k_kapila_cells<NP, DIM, PASS, PTMU, SEED, TYPES><<<blocks, CELL_THREADS, 0, s>>>(P, G, M, P.flux[0], P.flux[1],
+  constexpr int CT = cell_threads(PTMU);
+  const unsigned blocks = (unsigned)((P.n + CT - 1) / CT);
+  k_kapila_cells<NP, DIM, PASS, PTMU, SEED, TYPES><<<blocks, CT, 0, s>>>(P, G, M, P.flux[0], P.flux[1],
                                                                                  DIM > 2 ? P.flux[2] : nullptr);
   return cudaGetLastError();
 }

@@ -123,7 +123,10 @@ def test_ptmu_seed_fewer_saturation_iterations_same_residual(tmp_path):
     plain, st0 = _run(test_case, tmp_path / "plain")
     seeded, st1 = _run(test_case, tmp_path / "seeded", model)
     assert st0.ptmu_seeded == 0 and st1.ptmu_seeded > 0.9 * st1.ptmu_solves
-    assert st1.ptmu_errors == 0 and st1.ptmu_solves == st0.ptmu_solves
+    assert st1.ptmu_errors == 0 and st1.nonfinite_cells == 0 and st1.newton_fallback == st0.newton_fallback
+    # the pure-phase tests decide as the plain iteration does; states that differ at the solves' residual
+    # level may flip a borderline cell
+    assert abs(st1.ptmu_solves - st0.ptmu_solves) <= 0.01 * st0.ptmu_solves
     assert st1.ptmu_tsat_iters < 0.5 * st0.ptmu_tsat_iters, (st1.ptmu_tsat_iters, st0.ptmu_tsat_iters)
     assert abs(st1.ptmu_outer_iters - st0.ptmu_outer_iters) <= 0.02 * st0.ptmu_outer_iters
     for name in ("alpha", "rho", "E"):
