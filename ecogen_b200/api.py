@@ -21,6 +21,7 @@ MODEL_KAPILA, MODEL_EULER, MODEL_PTUEQ = 0, 1, 2
 FORM_FUSED, FORM_SPLIT = 0, 1
 STAGING_PLAIN, STAGING_TMA = 0, 1
 PTMU_SEED_T, PTMU_SEED_P_T = 0, 1
+CAP_FALLBACK, CAP_ACCEPT = 0, 1
 EOS_CODE = {"IG": 0, "SG": 1, "NASG": 2}
 BC_CODE = {"NONREFLECTING": 0, "SYMMETRY": 1, "WALL": 1}
 LIM_CODE = {None: 0, "NONE": 0, "MINMOD": 1, "VANLEER": 2, "VANALBADA": 3, "SUPERBEE": 4, "MC": 5, "THINC": 6}
@@ -130,6 +131,7 @@ def lib():
     L.ecg_stream.restype = vp
     L.ecg_stream.argtypes = [vp]
     L.ecg_set_newton_cap.argtypes = [vp, C.c_int32]
+    L.ecg_set_newton_cap_mode.argtypes = [vp, C.c_int32]
     L.ecg_set_seed_model.argtypes = [vp, P(Mlp)]
     L.ecg_record_pairs.argtypes = [vp, C.c_int64, C.c_int32]
     L.ecg_fetch_pairs.argtypes = [vp, fp, fp, P(C.c_int64)]
@@ -357,6 +359,10 @@ class Context:
 
     def set_newton_cap(self, cap: int):
         check(lib().ecg_set_newton_cap(self.h, cap), "ecg_set_newton_cap")
+
+    def set_newton_cap_mode(self, mode: int):
+        """CAP_FALLBACK (interface pressure at the cap, the reference's) or CAP_ACCEPT (keep the iterate)."""
+        check(lib().ecg_set_newton_cap_mode(self.h, mode), "ecg_set_newton_cap_mode")
 
     def set_seed_model(self, mlp: Optional["Mlp"]):
         check(lib().ecg_set_seed_model(self.h, C.byref(mlp) if mlp is not None else None), "ecg_set_seed_model")

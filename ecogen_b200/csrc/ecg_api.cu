@@ -126,6 +126,7 @@ struct ecg_ctx {
   DevStats* h_stats = nullptr;
   int cur = 0;
   int newton_cap = 100;
+  int newton_accept = 0;
   int ptmu_seed_p = 0;  // ECG_PTMU_SEED_P_T: the network's p* starts the saturation Newton too
   MlpDev* mlp = nullptr;
   float* rec_x = nullptr;
@@ -256,6 +257,7 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.stats = x->stats;
   for (int i = 0; i < 4; i++) P.lim[i] = x->c.limiter[i];
   P.newton_cap = x->newton_cap;
+  P.newton_accept = x->newton_accept;
   P.mlp = x->mlp;
   P.rec_x = x->rec_x;
   P.rec_y = x->rec_y;
@@ -684,6 +686,13 @@ extern "C" int32_t ecg_face_staging(const ecg_ctx* x) {
 extern "C" ecg_status ecg_set_newton_cap(ecg_ctx* x, int32_t cap) {
   if (!x || cap < 1 || cap > 100000) { set_error("bad Newton cap"); return ECG_ERR_INVALID; }
   x->newton_cap = cap;
+  x->graph_dirty = true;
+  return ECG_OK;
+}
+
+extern "C" ecg_status ecg_set_newton_cap_mode(ecg_ctx* x, int32_t mode) {
+  if (!x || (mode != ECG_CAP_FALLBACK && mode != ECG_CAP_ACCEPT)) { set_error("bad Newton cap mode"); return ECG_ERR_INVALID; }
+  x->newton_accept = mode == ECG_CAP_ACCEPT ? 1 : 0;
   x->graph_dirty = true;
   return ECG_OK;
 }

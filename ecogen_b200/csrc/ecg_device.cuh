@@ -357,7 +357,7 @@ struct RelaxStats {
 template <int NP>
 __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], double r[NP], const double p[NP],
                                            double& pstar, RelaxStats& st, double seed, bool use_seed,
-                                           int max_iter) {
+                                           int max_iter, bool accept = false) {
   st.iters = 0;
   st.fallback = false;
   st.seeded = false;
@@ -401,7 +401,7 @@ __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], dou
     }
   } while (fabs(f) > 1e-10 && iteration < max_iter);
   st.iters = iteration;
-  if (iteration < max_iter) {
+  if (iteration < max_iter || accept) {  // accept: a capped iteration keeps its last iterate
 #pragma unroll
     for (int k = 0; k < NP; k++) { a[k] = aS[k]; r[k] = rS[k]; }
     pstar = ps;
@@ -554,14 +554,14 @@ __device__ __forceinline__ void pinf_first(const Model<NP>& M, const double a[NP
 template <int NP>
 __device__ __forceinline__ void pinf_finish(const Model<NP>& M, double a[NP], double r[NP], const double p[NP],
                                             NewtonState s, double aS[NP], double rS[NP], double& pstar, RelaxStats& st,
-                                            int max_iter) {
+                                            int max_iter, bool accept = false) {
   while (fabs(s.f) > 1e-10 && s.it < max_iter) {
     s.it++;
     s.ps -= s.f / s.df;
     pinf_eval<NP>(M, a, r, s, p, aS, rS);
   }
   st.iters = s.it;
-  if (s.it < max_iter) {
+  if (s.it < max_iter || accept) {
 #pragma unroll
     for (int k = 0; k < NP; k++) { a[k] = aS[k]; r[k] = rS[k]; }
     pstar = s.ps;

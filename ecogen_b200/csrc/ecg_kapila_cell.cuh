@@ -477,10 +477,10 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
           rs.rejected = true;
         }
       }
-      pinf_finish<NP>(M, a, r, pk, s, aS, rS, pstar, rs, P.newton_cap);
+      pinf_finish<NP>(M, a, r, pk, s, aS, rS, pstar, rs, P.newton_cap, P.newton_accept != 0);
     }
   } else {
-    relaxed = relax_pinf<NP>(M, a, r, pk, pstar, rs, 0., false, P.newton_cap);
+    relaxed = relax_pinf<NP>(M, a, r, pk, pstar, rs, 0., false, P.newton_cap, P.newton_accept != 0);
   }
   if (relaxed) {
 #pragma unroll

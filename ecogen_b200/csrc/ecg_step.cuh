@@ -112,6 +112,7 @@ struct StepParams {
   DevStats* stats;
   int lim[4];
   int newton_cap;
+  int newton_accept;  // 1: a relaxation that reaches the cap keeps its last iterate (no fallback)
   // learned seed (optional)
   const struct MlpDev* mlp;  // installed model (nullptr = plain start)
   // recording of (features, converged pressure) pairs of relaxations with at least rec_min_evals

@@ -217,6 +217,13 @@ void* ecg_stream(const ecg_ctx* ctx);
 /* Newton iteration cap (default 100, RelaxationP::NewtonRaphson src/Relaxations/RelaxationP.cpp:66);
  * a lower cap forces the interface-pressure fallback and is used to test that path. */
 ecg_status ecg_set_newton_cap(ecg_ctx* ctx, int32_t cap);
+/* What a pressure relaxation that reaches the Newton cap does: ECG_CAP_FALLBACK (the reference's
+ * interface pressure, the default) or ECG_CAP_ACCEPT (keep the last Newton iterate).  A measurement aid:
+ * with ECG_CAP_ACCEPT and a cap of 1 every relaxation costs one evaluation, what it would cost if started
+ * at p*, so the step time is the ceiling of any seed's gain (the fields then differ from the plain
+ * iteration's by the unconverged cells' residuals). */
+enum { ECG_CAP_FALLBACK = 0, ECG_CAP_ACCEPT = 1 };
+ecg_status ecg_set_newton_cap_mode(ecg_ctx* ctx, int32_t mode);
 /* Device-resident variants for callers that keep their own device buffers: fields[] point at
  * device memory laid out as above.  Run on the context's stream. */
 ecg_status ecg_upload_prim_device(ecg_ctx* ctx, const double* const* dfields, int64_t ncells);
