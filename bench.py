@@ -7,7 +7,8 @@ synthetic input generated by ecogen_b200.cases.cavity_collapse_3d and read throu
 XML reader.  The line reports the plain FP64 path (`value`) and the same workload with the learned
 pressure-relaxation seed installed (`mlp_seeded`; c5: the (p*, T) seed of the p-T-mu saturation
 solve), and beside it the ceiling of any pressure seed: the plain step with Newton stopped after one
-(three) evaluations (`mlp_seeded.ceiling`).  One "step" is one full time step of the whole
+(three) evaluations (`mlp_seeded.ceiling`); c5 also reports the p-T-mu warm start without a network
+(`ptmu_warm_start`).  One "step" is one full time step of the whole
 grid (predictor + corrector + relaxations + dt update).  The state (256^3 x 11 doubles = 1.48 GB per
 copy) is larger than L2, so no L2 flush is needed between steps.
 
@@ -505,6 +506,8 @@ def bench_batch(args, rank, world, local):
                 "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max}}
         if seeded is not None:
             line["mlp_seeded"] = seeded
+        if warm is not None:
+            line["ptmu_warm_start"] = warm
         print(json.dumps(line))
 
 
@@ -693,6 +696,38 @@ def main():
                 cctx.close()
             seeded["ceiling"] = ceil
 
+    # ---- p-T-mu warm start (no network): each cell's T_sat solves start from its previous solve
+    warm = None
+    if case.ptmu is not None and not args.no_seeded:
+        ref_w = new_context()
+        ref_w.upload(fields0)
+        ctxw = new_context()
+        ctxw.upload(fields0)
+        ctxw.set_ptmu_warm_start(True)
+        ref_w.step(args.warmup)
+        ctxw.step(args.warmup)
+        streamw = torch.cuda.ExternalStream(api.lib().ecg_stream(ctxw.h))
+        torch.cuda.synchronize()
+        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0.record(streamw)
+        stw = ctxw.step(args.steps)
+        w1.record(streamw)
+        w1.synchronize()
+        msw = w0.elapsed_time(w1)
+        st_rw = ref_w.step(args.steps)
+        a, b = ref_w.download_dict(), ctxw.download_dict()
+        warm = {"value": case.ncells * args.steps / (msw * 1e-3), "unit": "cell-updates/s",
+                "speedup_vs_plain": ms_max / msw,
+                "tsat_iters_per_solve": stw.ptmu_tsat_iters / max(1, stw.ptmu_solves),
+                "plain_tsat_iters_per_solve": st_rw.ptmu_tsat_iters / max(1, st_rw.ptmu_solves),
+                "ptmu_outer_iters_per_solve": stw.ptmu_outer_iters / max(1, stw.ptmu_solves),
+                "plain_ptmu_outer_iters_per_solve": st_rw.ptmu_outer_iters / max(1, st_rw.ptmu_solves),
+                "nonfinite_cells": stw.nonfinite_cells,
+                "field_rel_l1_vs_plain": max(float(np.abs(a[k] - b[k]).sum() / max(np.abs(a[k]).sum(), 1e-300))
+                                             for k in ("alpha", "rho", "p", "E"))}
+        ref_w.close()
+        ctxw.close()
+
     # ---- per-kernel attribution (separate launches, events between kernels)
     nprof = max(2, min(args.steps, 10))
     st_p, kms = ctx.step_profiled_kernels(nprof)
@@ -793,6 +828,8 @@ def main():
         }
         if seeded is not None:
             line["mlp_seeded"] = seeded
+        if warm is not None:
+            line["ptmu_warm_start"] = warm
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "cell-updates/s", "cores": cpu["cores"],
                                     "kind": "reference", "cpu": cpu["cpu"], "sample": cpu["sample"]}

@@ -125,6 +125,7 @@ def lib():
     L.ecg_face_staging.restype = C.c_int32
     L.ecg_face_staging.argtypes = [vp]
     L.ecg_set_ptmu_seed.argtypes = [vp, C.c_int32]
+    L.ecg_set_ptmu_warm_start.argtypes = [vp, C.c_int32]
     L.ecg_step_noalloc.argtypes = [P(Case), vp, vp, C.c_double, dp, P(StepStats), vp]
     L.ecg_ncells.restype = C.c_int64
     L.ecg_ncells.argtypes = [vp]
@@ -344,6 +345,10 @@ class Context:
     def face_staging(self) -> int:
         """The staging the next split-form step uses (ecg_face_staging)."""
         return int(lib().ecg_face_staging(self.h))
+
+    def set_ptmu_warm_start(self, on: bool):
+        """Start each cell's T_sat solves from its previous solve (ecg_set_ptmu_warm_start)."""
+        check(lib().ecg_set_ptmu_warm_start(self.h, 1 if on else 0), "ecg_set_ptmu_warm_start")
 
     def set_ptmu_seed(self, mode: int):
         """PTMU_SEED_T (default) or PTMU_SEED_P_T: what a p-T-mu seed model starts (ecg_set_ptmu_seed)."""

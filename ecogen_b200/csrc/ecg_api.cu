@@ -128,6 +128,7 @@ struct ecg_ctx {
   int newton_cap = 100;
   int newton_accept = 0;
   int ptmu_seed_p = 0;  // ECG_PTMU_SEED_P_T: the network's p* starts the saturation Newton too
+  double* tsat_hist = nullptr;  // p-T-mu warm start (ecg_set_ptmu_warm_start): T_sat of each cell's last solve
   MlpDev* mlp = nullptr;
   float* rec_x = nullptr;
   float* rec_y = nullptr;
@@ -272,6 +273,7 @@ ecg_status launch_step(ecg_ctx* x, int parity, cudaEvent_t* ev = nullptr) {
   P.ptmu_vap = x->c.ptmu_vapor;
   P.pcrit = x->pcrit;
   P.ptmu_seed_p = x->ptmu_seed_p;
+  P.tsat_hist = x->tsat_hist;
   for (int a = 0; a < 3; a++) P.flux[a] = x->split ? x->flux[a] : nullptr;
   P.fmaps = (x->split && x->staging == ECG_STAGING_TMA && x->fmaps.ok) ? &x->fmaps : nullptr;
   double* sn = x->state[parity];
@@ -655,6 +657,7 @@ extern "C" void ecg_destroy(ecg_ctx* x) {
   cudaFree(x->rec_x);
   cudaFree(x->rec_y);
   cudaFree(x->rec_count);
+  cudaFree(x->tsat_hist);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }
@@ -985,6 +988,23 @@ extern "C" ecg_status ecg_set_seed_model(ecg_ctx* x, const ecg_mlp* m) {
   if (x->c.model != ECG_MODEL_KAPILA) { set_error("the seed model applies to Kapila relaxation"); return ECG_ERR_UNSUPPORTED; }
   if (x->c.ntransports > 0) { set_error("the seeded kernels run without passive transports"); return ECG_ERR_UNSUPPORTED; }
   return mlp_upload(m, x->np, x->c.ptmu != 0, &x->mlp, x->stream);
+}
+
+extern "C" ecg_status ecg_set_ptmu_warm_start(ecg_ctx* x, int32_t on) {
+  if (!x || (on != 0 && on != 1)) { set_error("bad argument"); return ECG_ERR_INVALID; }
+  if (on && !x->c.ptmu) { set_error("the warm start applies to p-T-mu relaxation"); return ECG_ERR_UNSUPPORTED; }
+  x->graph_dirty = true;
+  if (!on) {
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    cudaFree(x->tsat_hist);
+    x->tsat_hist = nullptr;
+    return ECG_OK;
+  }
+  if (!x->tsat_hist) {
+    ECG_CUDA(cudaMalloc(&x->tsat_hist, sizeof(double) * (size_t)x->n));
+    ECG_CUDA(cudaMemsetAsync(x->tsat_hist, 0, sizeof(double) * (size_t)x->n, x->stream));  // 0: no solve yet
+  }
+  return ECG_OK;
 }
 
 extern "C" ecg_status ecg_set_ptmu_seed(ecg_ctx* x, int32_t mode) {

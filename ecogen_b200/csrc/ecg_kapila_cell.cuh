@@ -493,13 +493,17 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
     // RelaxationPTMu reads before any fulfillState
     const double emix = rebuilt_emix<NP>(M, a0, r0, p0, rhomix);
     bool err = false;
-    const double ps = SEED ? g.ptmu_p : -1., Ts = SEED ? g.ptmu_T : -1.;
+    const double ps = SEED ? g.ptmu_p : -1.;
+    // T_sat start: the network's (seeded kernels), else the cell's previous converged T_sat when the
+    // warm start is on (a value <= 0: no solve yet, cold start), else the reference's cold start
+    const double Ts = SEED ? g.ptmu_T : (P.tsat_hist != nullptr ? P.tsat_hist[cell] : -1.);
     if (relax_ptmu<NP>(M, P.ptmu_liq, P.ptmu_vap, P.pcrit, a, r, pk, rhomix, emix, err, &cc.pc, ps, Ts)) {
       rhomix = 0.;
 #pragma unroll
       for (int k = 0; k < NP; k++) rhomix += a[k] * r[k];
     }
-    if (SEED && cc.pc.solve && Ts > 0.) cc.pc.seeded = 1;
+    if (cc.pc.solve && Ts > 0.) cc.pc.seeded = 1;
+    if (P.tsat_hist != nullptr && cc.pc.solve && !err) P.tsat_hist[cell] = cc.pc.tsat;
     if (P.rec_x != nullptr && cc.pc.solve && !err && (int)cc.pc.outer >= P.rec_min_evals) {
       float x[PTMU_NIN];
       if (SEED) {

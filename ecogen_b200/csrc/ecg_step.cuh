@@ -126,6 +126,7 @@ struct StepParams {
   int ptmu, ptmu_liq, ptmu_vap;
   double pcrit;
   int ptmu_seed_p;  // seeded p-T-mu: 1 = the network's p* starts the saturation Newton too (else T only)
+  double* tsat_hist;  // p-T-mu warm start: per-cell T_sat of the cell's last saturation solve (nullptr: off)
   // THINC reconstruction of alpha (a volume-fraction limiter is THINC): cosh and tanh of the
   // sharpness beta = 1.6, evaluated once on the host like the reference does
   int thinc;

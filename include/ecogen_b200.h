@@ -119,7 +119,8 @@ typedef struct {
   int64_t ptmu_tsat_iters;
   int64_t ptmu_tsat_max;
   int64_t ptmu_outer_hist[16];
-  int64_t ptmu_seeded;          /* saturation solves started from the learned (p*, T) seed */
+  int64_t ptmu_seeded;          /* saturation solves whose T_sat Newton started from a seed (the learned
+                                   network's, or the cell's previous solve with the warm start) */
   int64_t ptmu_seed_rejected;   /* learned (p*, T) seeds rejected (plain start) */
   int64_t bounds_violations;    /* bounds-checked builds (-DECG_BOUNDS_CHECK) only: device accesses outside
                                    their buffer, counted and skipped; always 0 in the regular build */
@@ -294,6 +295,13 @@ ecg_status ecg_set_seed_model(ecg_ctx* ctx, const ecg_mlp* mlp);
  * ECG_PTMU_SEED_P_T: the saturation Newton starts from the network's p* as well. */
 enum { ECG_PTMU_SEED_T = 0, ECG_PTMU_SEED_P_T = 1 };
 ecg_status ecg_set_ptmu_seed(ecg_ctx* ctx, int32_t mode);
+/* p-T-mu warm start (no network): with on = 1 the context keeps, per cell, the T_sat of the cell's last
+ * saturation solve, and the next solve of that cell starts its T_sat(p) Newton there (then at the previous
+ * iteration's T_sat) instead of at the cold start 0.1 B / C; the saturation Newton on p* keeps the
+ * reference's start.  Every loop still stops at |f| <= 1e-10: the fields agree with the plain solve to
+ * that residual, not bit for bit.  A seed model, when installed, takes precedence.  on = 0 (the default)
+ * frees the per-cell record and restores the reference's starts. */
+ecg_status ecg_set_ptmu_warm_start(ecg_ctx* ctx, int32_t on);
 /* Records up to max_pairs (features, targets) pairs from the relaxations of the next ecg_step calls
  * into an internal device buffer; ecg_fetch_pairs copies them out.  Pressure relaxation: 3 N features,
  * one target (the relaxed pressure's place in the bracket of the phase pressures), relaxations that
