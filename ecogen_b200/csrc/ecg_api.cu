@@ -710,6 +710,8 @@ static ecg_status upload_impl(ecg_ctx* x, const double* const* f, int64_t ncells
   const size_t fb = sizeof(double) * (size_t)n;
   double* S = x->state[x->cur];
   const bool euler = x->c.model == ECG_MODEL_EULER;
+  // a new state: the p-T-mu warm start forgets the previous state's T_sat values
+  if (x->tsat_hist) ECG_CUDA(cudaMemsetAsync(x->tsat_hist, 0, fb, x->stream));
   if (x->c.model == ECG_MODEL_PTUEQ) {
     // ABI: alpha_0 alpha_1 rho_0 rho_1 p u_x u_y u_z E T -> device: alpha_0 alpha_1 p T u_0..u_{dim-1} E
     // (the phase densities are computeDensity(p, T); the uploaded ones are not read)

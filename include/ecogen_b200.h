@@ -299,8 +299,9 @@ ecg_status ecg_set_ptmu_seed(ecg_ctx* ctx, int32_t mode);
  * saturation solve, and the next solve of that cell starts its T_sat(p) Newton there (then at the previous
  * iteration's T_sat) instead of at the cold start 0.1 B / C; the saturation Newton on p* keeps the
  * reference's start.  Every loop still stops at |f| <= 1e-10: the fields agree with the plain solve to
- * that residual, not bit for bit.  A seed model, when installed, takes precedence.  on = 0 (the default)
- * frees the per-cell record and restores the reference's starts. */
+ * that residual, not bit for bit.  A seed model, when installed, takes precedence.  An upload clears the
+ * record (the next solves start cold).  on = 0 (the default) frees the per-cell record and restores the
+ * reference's starts. */
 ecg_status ecg_set_ptmu_warm_start(ecg_ctx* ctx, int32_t on);
 /* Records up to max_pairs (features, targets) pairs from the relaxations of the next ecg_step calls
  * into an internal device buffer; ecg_fetch_pairs copies them out.  Pressure relaxation: 3 N features,

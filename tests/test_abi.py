@@ -174,3 +174,16 @@ def test_stretch_zones_are_checked_without_gpu_work():
     assert zones((0.0, 0.9, 1.0, 100)) == 1               # does not reach the length
     assert zones((0.0, 1.0, 1.05, 90)) == 1               # 90 cells on a 100-cell axis
     assert not h.value
+
+
+def test_context_settings_refuse_a_null_context():
+    """The GPU-side settings check their context before any device work (no GPU needed)."""
+    L = api.lib()
+    assert L.ecg_set_step_form(None, api.FORM_SPLIT) == 1
+    assert L.ecg_set_face_staging(None, api.STAGING_TMA) == 1
+    assert L.ecg_set_ptmu_seed(None, api.PTMU_SEED_T) == 1
+    assert L.ecg_set_ptmu_warm_start(None, 1) == 1
+    assert L.ecg_set_newton_cap_mode(None, api.CAP_ACCEPT) == 1
+    assert L.ecg_set_newton_cap(None, 3) == 1
+    assert L.ecg_step_form(None) == api.FORM_FUSED
+    assert L.ecg_face_staging(None) == api.STAGING_PLAIN
