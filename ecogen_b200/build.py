@@ -79,12 +79,13 @@ def build(verbose: bool = False, jobs: int = 8, lib_only: bool = False) -> str:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     if lib_only:
         return LIB
-    # measurement probe (FP64 pipe peak for the bench's FP64 roofline), its own library
-    probe_src = os.path.join(HERE, "probe", "ecg_fp64_peak.cu")
-    if os.path.exists(probe_src):
-        pobj = _compile(probe_src)
-        if not os.path.exists(PROBE_LIB) or os.path.getmtime(pobj) > os.path.getmtime(PROBE_LIB):
-            cmd = [_nvcc()] + ARCH + ["-shared", "-o", PROBE_LIB, pobj, "-lcudart"]
+    # measurement and check probes (FP64 pipe peak for the bench's FP64 roofline; the branch-free
+    # division / square root against CUDA's), their own library
+    probe_srcs = sorted(glob.glob(os.path.join(HERE, "probe", "*.cu")))
+    if probe_srcs:
+        pobjs = [_compile(src) for src in probe_srcs]
+        if not os.path.exists(PROBE_LIB) or any(os.path.getmtime(o) > os.path.getmtime(PROBE_LIB) for o in pobjs):
+            cmd = [_nvcc()] + ARCH + ["-shared", "-o", PROBE_LIB] + pobjs + ["-lcudart"]
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -127,15 +127,15 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
         int rl = j - 1 + K::H, rr = rl + 1;
         // centre-to-centre distance with the reference's arithmetic (Element::distance)
         double pl = (gl + 0.5) * C.dx, pr = (gl + 1 + 0.5) * C.dx, x = pl - pr;
-        double d = sqrt(x * x);
+        double d = dsqrt(x * x);
 #pragma unroll
         for (int k = 0; k < NP; k++) {
-          ssl[k * SS + e] = (sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl]) / d;
-          ssl[(NP + k) * SS + e] = (sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl]) / d;
+          ssl[k * SS + e] = ddiv(sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl], d);
+          ssl[(NP + k) * SS + e] = ddiv(sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl], d);
           double pR = eos_fix_p(M.eos[k], sq[FL::P * RS + rr]), pL = eos_fix_p(M.eos[k], sq[FL::P * RS + rl]);
-          ssl[(2 * NP + k) * SS + e] = (pR - pL) / d;
+          ssl[(2 * NP + k) * SS + e] = ddiv(pR - pL, d);
         }
-        ssl[(3 * NP) * SS + e] = (sq[FL::U * RS + rr] - sq[FL::U * RS + rl]) / d;
+        ssl[(3 * NP) * SS + e] = ddiv(sq[FL::U * RS + rr] - sq[FL::U * RS + rl], d);
       }
       __syncthreads();
     }
@@ -159,9 +159,9 @@ __global__ void ECG_BATCH_BOUNDS(TB) k_batch(BatchParams B, Model<NP> M0) {
         double y = pf - pl, z = pf - pr;
         constexpr bool kThinc = (TYPES == EOS_DYNAMIC);
         constexpr int kLim = code_limiter(TYPES);
-        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, sqrt(y * y), 1.,
+        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rl, ssl, SS, f1, hasL ? j : -1, aL, aR, aLL, dsqrt(y * y), 1.,
                                               tl, ug);
-        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, sqrt(z * z),
+        reconstruct_side<NP, 1, kThinc, kLim>(M, P, sq, RS, rr, ssl, SS, f1, hasR ? j + 2 : -1, aR, aL, aRR, dsqrt(z * z),
                                               -1.,
                                 tr, vg);
       }

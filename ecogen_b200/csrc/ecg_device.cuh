@@ -2,9 +2,12 @@
 //
 // Every routine restates a reference routine (file:line relative to the ECOGEN
 // tree) with the same operation order, so that results agree with the CPU code
-// to the last bits except where CUDA's pow/log/exp differ from glibc's by an ulp.
-// Kernels are built with --fmad=false so that no multiply-add is contracted, as
-// in the reference's x86-64 SSE2 build.
+// to the last bits except where a math function's result differs from glibc's by
+// an ulp (epow, ecg_pow.cuh: in about 0.1 % of the calls, where glibc's pow is
+// not correctly rounded; exp of the THINC reconstruction).  Divisions and square
+// roots go through ddiv / dsqrt (ecg_ieee.cuh), which return the IEEE quotient and
+// root bit for bit without a branch.  Kernels are built with --fmad=false so that
+// no multiply-add is contracted, as in the reference's x86-64 SSE2 build.
 //
 // Compact state.  The reference keeps per phase (alpha, rho, p, T, e, c, Y) and per
 // cell a mixture record (rho, p, u, e, E, cF, cWood).  After each full step every
@@ -16,6 +19,8 @@
 #pragma once
 #include <cstdint>
 
+#include "ecg_ieee.cuh"
+#include "ecg_pow.cuh"
 #include "ecg_types.h"
 
 // Inlining of the two largest face routines (HLLC and the MUSCL side reconstruction).  Inlined, the
@@ -38,27 +43,27 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 // src/Eos/EosIG.cpp:64-257, src/Eos/EosSG.cpp:66-257, src/Eos/EosNASG.cpp:68-280
 
 __device__ __forceinline__ double eos_T(const EosParams& q, double eps, double rho, double p) {
-  if (q.type == ECG_EOS_IG) return p / (q.gamma - 1.) / dmax(rho, eps) / q.cv;
-  if (q.type == ECG_EOS_SG) return (p + q.pinf) / (q.gamma - 1.) / dmax(rho, eps) / q.cv;
-  return (p + q.pinf) * dmax(1. - rho * q.b, eps) / (q.gamma - 1.) / q.cv / dmax(rho, eps);
+  if (q.type == ECG_EOS_IG) return ddiv(ddiv(ddiv(p, q.gamma - 1.), dmax(rho, eps)), q.cv);
+  if (q.type == ECG_EOS_SG) return ddiv(ddiv(ddiv(p + q.pinf, q.gamma - 1.), dmax(rho, eps)), q.cv);
+  return ddiv(ddiv(ddiv((p + q.pinf) * dmax(1. - rho * q.b, eps), q.gamma - 1.), q.cv), dmax(rho, eps));
 }
 
 __device__ __forceinline__ double eos_e(const EosParams& q, double eps, double rho, double p) {
-  if (q.type == ECG_EOS_IG) return p / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
-  if (q.type == ECG_EOS_SG) return (p + q.gamma * q.pinf) / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
-  return (p + q.gamma * q.pinf) * dmax(1. - rho * q.b, eps) / (q.gamma - 1.) / dmax(rho, eps) + q.eref;
+  if (q.type == ECG_EOS_IG) return ddiv(ddiv(p, q.gamma - 1.), dmax(rho, eps)) + q.eref;
+  if (q.type == ECG_EOS_SG) return ddiv(ddiv(p + q.gamma * q.pinf, q.gamma - 1.), dmax(rho, eps)) + q.eref;
+  return ddiv(ddiv((p + q.gamma * q.pinf) * dmax(1. - rho * q.b, eps), q.gamma - 1.), dmax(rho, eps)) + q.eref;
 }
 
 __device__ __forceinline__ double eos_p(const EosParams& q, double eps, double rho, double e) {
   if (q.type == ECG_EOS_IG) return (q.gamma - 1.) * rho * (e - q.eref);
   if (q.type == ECG_EOS_SG) return (q.gamma - 1.) * rho * (e - q.eref) - q.gamma * q.pinf;
-  return (rho * (q.gamma - 1.) * (e - q.eref) / dmax(1. - rho * q.b, eps) - q.gamma * q.pinf);
+  return (ddiv(rho * (q.gamma - 1.) * (e - q.eref), dmax(1. - rho * q.b, eps)) - q.gamma * q.pinf);
 }
 
 __device__ __forceinline__ double eos_c(const EosParams& q, double eps, double rho, double p) {
-  if (q.type == ECG_EOS_IG) return sqrt(q.gamma * p / dmax(rho, eps));
-  if (q.type == ECG_EOS_SG) return sqrt(q.gamma * (p + q.pinf) / dmax(rho, eps));
-  return sqrt(q.gamma * (p + q.pinf) / dmax(rho * (1. - rho * q.b), eps));
+  if (q.type == ECG_EOS_IG) return dsqrt(ddiv(q.gamma * p, dmax(rho, eps)));
+  if (q.type == ECG_EOS_SG) return dsqrt(ddiv(q.gamma * (p + q.pinf), dmax(rho, eps)));
+  return dsqrt(ddiv(q.gamma * (p + q.pinf), dmax(rho * (1. - rho * q.b), eps)));
 }
 
 __device__ __forceinline__ double nonzero(double a, double eps) {  // Tools::returnNonZeroValue src/Tools.cpp:134
@@ -69,9 +74,9 @@ __device__ __forceinline__ double nonzero(double a, double eps) {  // Tools::ret
 
 __device__ __forceinline__ double eos_p_isentropic(const EosParams& q, double eps, double p0, double rho0,
                                                    double rho1) {
-  if (q.type == ECG_EOS_IG) return p0 * pow(rho1 / dmax(rho0, eps), q.gamma);
-  if (q.type == ECG_EOS_SG) return (p0 + q.pinf) * pow(rho1 / dmax(rho0, eps), q.gamma) - q.pinf;
-  return (p0 + q.pinf) * pow(rho1 / dmax(rho0, eps), q.gamma) * pow((1. - rho0 * q.b) / (1. - rho1 * q.b), q.gamma) -
+  if (q.type == ECG_EOS_IG) return p0 * epow(ddiv(rho1, dmax(rho0, eps)), q.gamma);
+  if (q.type == ECG_EOS_SG) return (p0 + q.pinf) * epow(ddiv(rho1, dmax(rho0, eps)), q.gamma) - q.pinf;
+  return (p0 + q.pinf) * epow(ddiv(rho1, dmax(rho0, eps)), q.gamma) * epow(ddiv(1. - rho0 * q.b, 1. - rho1 * q.b), q.gamma) -
          q.pinf;
 }
 
@@ -81,21 +86,21 @@ __device__ __forceinline__ double eos_rho_pfinal(const EosParams& q, double eps,
   if (q.type == ECG_EOS_IG) {
     num = q.gamma * p1;
     denom = num + p0 - p1;
-    rho1 = rho0 * num / dmax(denom, eps);
-    *drhodp = rho0 * q.gamma * p0 / dmax(denom * denom, eps);
+    rho1 = ddiv(rho0 * num, dmax(denom, eps));
+    *drhodp = ddiv(rho0 * q.gamma * p0, dmax(denom * denom, eps));
     return rho1;
   }
   if (q.type == ECG_EOS_SG) {
     num = q.gamma * (p1 + q.pinf);
     denom = num + p0 - p1;
-    rho1 = rho0 * num / nonzero(denom, eps);
-    *drhodp = rho0 * q.gamma * (p0 + q.pinf) / dmax(denom * denom, eps);
+    rho1 = ddiv(rho0 * num, nonzero(denom, eps));
+    *drhodp = ddiv(rho0 * q.gamma * (p0 + q.pinf), dmax(denom * denom, eps));
     return rho1;
   }
   num = q.gamma * (p1 + q.pinf);
   denom = num + p0 - p1 + q.b * rho0 * (p1 - p0);
-  rho1 = rho0 * num / nonzero(denom, eps);
-  *drhodp = rho0 * q.gamma * (p0 + q.pinf - q.b * rho0 * (p0 + q.pinf)) / nonzero(denom * denom, eps);
+  rho1 = ddiv(rho0 * num, nonzero(denom, eps));
+  *drhodp = ddiv(rho0 * q.gamma * (p0 + q.pinf - q.b * rho0 * (p0 + q.pinf)), nonzero(denom * denom, eps));
   return rho1;
 }
 
@@ -107,7 +112,7 @@ __device__ __forceinline__ double eos_fix_p(const EosParams& q, double p) {
 }
 
 __device__ __forceinline__ void eos_rho_max(const EosParams& q, double& rho) {  // verifyAndCorrectDensityMax(density)
-  if (q.type == ECG_EOS_NASG && rho > 1. / q.b - 1.) rho = 1. / q.b - 1.;
+  if (q.type == ECG_EOS_NASG && rho > ddiv(1., q.b) - 1.) rho = ddiv(1., q.b) - 1.;
 }
 
 // ------------------------------------------------------------------------------ model parameters
@@ -180,10 +185,10 @@ __device__ __forceinline__ void fulfill(const Model<NP>& M, Thermo<NP>& t) {
   double cF = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
-    t.Y[k] = t.a[k] * t.r[k] / dmax(t.rho, M.eps);
+    t.Y[k] = ddiv(t.a[k] * t.r[k], dmax(t.rho, M.eps));
     cF += t.Y[k] * c[k] * c[k];
   }
-  t.cF = sqrt(cF);
+  t.cF = dsqrt(cF);
 }
 
 // PhaseUEq::extendedCalculusPhase energies and MixUEq::computeMixtureVariables' e = sum_k Y_k e_k.
@@ -244,10 +249,10 @@ __device__ ECG_HLLC_INLINE void hllc(const Model<NP>& M, const Thermo<NP>& L, co
   double uR = ur[0], cR = R.cF, pR = R.pm, rhoR = R.rho;
   double sL = dmin(uL - cL, uR - cR);
   double sR = dmax(uR + cR, uL + cL);
-  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * dxL / fabs(sL));
-  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, 1. * dxR / fabs(sR));
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * dxL, fabs(sL)));
+  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * dxR, fabs(sR)));
   double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
-  double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+  double sM = ddiv(pR - pL + mL * uL - mR * uR, mL - mR);
   if (fabs(sM) < 1.e-8) sM = 0.;
   F.sM = sM;
   if (sL >= 0. || sR <= 0.) {
@@ -279,13 +284,13 @@ __device__ ECG_HLLC_INLINE void hllc(const Model<NP>& M, const Thermo<NP>& L, co
     double e[NP];
     const double em = side_energy<NP>(M, S, e);
     double Et = em + 0.5 * (us[0] * us[0] + us[1] * us[1] + us[2] * us[2]);
-    double rhoStar = mK / (sK - sM);
-    double EStar = Et + (sM - uK) * (sM + pK / mK);
+    double rhoStar = ddiv(mK, sK - sM);
+    double EStar = Et + (sM - uK) * (sM + ddiv(pK, mK));
     double pStar = mK * (sM - uK) + pK;
 #pragma unroll
     for (int k = 0; k < NP; k++) {
       double mk = S.r[k] * (sK - uK);
-      double rks = mk / (sK - sM);
+      double rks = ddiv(mk, sK - sM);
       eos_rho_max(M.eos[k], rks);
       double pks = eos_p_isentropic(M.eos[k], M.eps, S.p[k], S.r[k], rks);
       double eks = eos_e(M.eos[k], M.eps, rks, pks);
@@ -314,13 +319,13 @@ __device__ __forceinline__ double limiter(int kind, double s1, double s2) {
       return slope;
     case ECG_LIM_VANLEER: {
       double sum = s1 + s2;
-      if ((fabs(sum) > 1e-6) && (prod > 1e-6)) slope = 2. * prod / sum;
+      if ((fabs(sum) > 1e-6) && (prod > 1e-6)) slope = ddiv(2. * prod, sum);
       return slope;
     }
     case ECG_LIM_VANALBADA: {
       double sum = s1 + s2;
       if ((fabs(s1) > 1e-6) && (fabs(s2) > 1e-6) && (fabs(sum) > 1e-6) && (prod > 1e-6))
-        slope = prod * sum / (s1 * s1 + s2 * s2);
+        slope = ddiv(prod * sum, s1 * s1 + s2 * s2);
       return slope;
     }
     case ECG_LIM_SUPERBEE:
@@ -386,7 +391,7 @@ __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], dou
   int iteration = 0;
   do {
     iteration++;
-    ps -= f / df;
+    ps -= ddiv(f, df);
 #pragma unroll
     for (int k = 0; k < NP; k++) ps = eos_fix_p(M.eos[k], ps);
     f = -1.;
@@ -394,8 +399,8 @@ __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], dou
 #pragma unroll
     for (int k = 0; k < NP; k++) {
       rS[k] = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], ps, &drhodp);
-      aS[k] = a[k] * r[k] / rS[k];
-      double dalpha = a[k] * r[k] * drhodp / (rS[k] * rS[k]);
+      aS[k] = ddiv(a[k] * r[k], rS[k]);
+      double dalpha = ddiv(a[k] * r[k] * drhodp, rS[k] * rS[k]);
       f += aS[k];
       df -= dalpha;
     }
@@ -420,13 +425,13 @@ __device__ __forceinline__ bool relax_pinf(const Model<NP>& M, double a[NP], dou
       if (j != k) sumZj += zk[j];
     pI += sumZj * (p[k] - 0.);
   }
-  pI /= sumZk * (NP - 1);
+  pI = ddiv(pI, sumZk * (NP - 1));
 #pragma unroll
   for (int k = 0; k < NP; k++) pI = eos_fix_p(M.eos[k], pI);
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     double rr = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], pI, &drhodp);
-    a[k] = a[k] * r[k] / rr;
+    a[k] = ddiv(a[k] * r[k], rr);
     r[k] = rr;
   }
   pstar = pI;
@@ -465,12 +470,21 @@ __device__ __forceinline__ DD dd_mul(DD a, DD b) {
   e += a.hi * b.lo + a.lo * b.hi;
   return dd_fast_sum(p, e);
 }
-__device__ __forceinline__ DD dd_div(DD a, DD b) {
+// dd_div_c: the same quotient with the `/` operator, for constant operands the compiler folds
+__device__ __forceinline__ DD dd_div_c(DD a, DD b) {
   double q1 = a.hi / b.hi;
   DD r = dd_add(a, dd_mul(b, DD{-q1, 0.}));
   double q2 = r.hi / b.hi;
   r = dd_add(r, dd_mul(b, DD{-q2, 0.}));
   double q3 = r.hi / b.hi;
+  return dd_add(dd_fast_sum(q1, q2), DD{q3, 0.});
+}
+__device__ __forceinline__ DD dd_div(DD a, DD b) {
+  double q1 = ddiv(a.hi, b.hi);
+  DD r = dd_add(a, dd_mul(b, DD{-q1, 0.}));
+  double q2 = ddiv(r.hi, b.hi);
+  r = dd_add(r, dd_mul(b, DD{-q2, 0.}));
+  double q3 = ddiv(r.hi, b.hi);
   return dd_add(dd_fast_sum(q1, q2), DD{q3, 0.});
 }
 static __device__ __noinline__ double cr_log(double x) {
@@ -487,8 +501,8 @@ static __device__ __noinline__ double cr_log(double x) {
   DD s2 = dd_mul(s, s);
   double t = 1. / 45.;                // tail sum_{i>=3} s^(2(i-3)) / (2i+1), i = 3..22, in double
   for (int i = 21; i >= 3; i--) t = t * s2.hi + 1. / (2. * i + 1.);
-  DD P = dd_add(dd_div(DD{1., 0.}, DD{5., 0.}), dd_mul(s2, DD{t, 0.}));
-  P = dd_add(dd_div(DD{1., 0.}, DD{3., 0.}), dd_mul(s2, P));
+  DD P = dd_add(dd_div_c(DD{1., 0.}, DD{5., 0.}), dd_mul(s2, DD{t, 0.}));
+  P = dd_add(dd_div_c(DD{1., 0.}, DD{3., 0.}), dd_mul(s2, P));
   P = dd_add(DD{1., 0.}, dd_mul(s2, P));
   DD lm = dd_mul(s, P);
   lm.hi *= 2.;
@@ -531,8 +545,8 @@ __device__ __forceinline__ void pinf_eval(const Model<NP>& M, const double a[NP]
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     rS[k] = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], s.ps, &drhodp);
-    aS[k] = a[k] * r[k] / rS[k];
-    double dalpha = a[k] * r[k] * drhodp / (rS[k] * rS[k]);
+    aS[k] = ddiv(a[k] * r[k], rS[k]);
+    double dalpha = ddiv(a[k] * r[k] * drhodp, rS[k] * rS[k]);
     s.f += aS[k];
     s.df -= dalpha;
   }
@@ -557,7 +571,7 @@ __device__ __forceinline__ void pinf_finish(const Model<NP>& M, double a[NP], do
                                             int max_iter, bool accept = false) {
   while (fabs(s.f) > 1e-10 && s.it < max_iter) {
     s.it++;
-    s.ps -= s.f / s.df;
+    s.ps -= ddiv(s.f, s.df);
     pinf_eval<NP>(M, a, r, s, p, aS, rS);
   }
   st.iters = s.it;
@@ -581,13 +595,13 @@ __device__ __forceinline__ void pinf_finish(const Model<NP>& M, double a[NP], do
       if (j != k) sumZj += zk[j];
     pI += sumZj * (p[k] - 0.);
   }
-  pI /= sumZk * (NP - 1);
+  pI = ddiv(pI, sumZk * (NP - 1));
 #pragma unroll
   for (int k = 0; k < NP; k++) pI = eos_fix_p(M.eos[k], pI);
 #pragma unroll
   for (int k = 0; k < NP; k++) {
     double rr = eos_rho_pfinal(M.eos[k], M.eps, p[k], r[k], pI, &drhodp);
-    a[k] = a[k] * r[k] / rr;
+    a[k] = ddiv(a[k] * r[k], rr);
     r[k] = rr;
   }
   pstar = pI;
@@ -616,37 +630,37 @@ __device__ __forceinline__ double compute_tsat(const EosParams& L, const EosPara
                                                bool& err, PtmuCount* pc = nullptr, double T0 = -1.) {
   double gL = L.gamma, piL = (L.type == ECG_EOS_IG) ? 0. : L.pinf, cvL = L.cv, e0L = L.eref, s0L = L.sref;
   double gV = V.gamma, piV = (V.type == ECG_EOS_IG) ? 0. : V.pinf, cvV = V.cv, e0V = V.eref, s0V = V.sref;
-  double A = (gL * cvL - gV * cvV + s0V - s0L) / (gV * cvV - cvV);
-  double B = (e0L - e0V) / (gV * cvV - cvV);
-  double C = (gV * cvV - gL * cvL) / (gV * cvV - cvV);
-  double D = (gL * cvL - cvL) / (gV * cvV - cvV);
+  double A = ddiv(gL * cvL - gV * cvV + s0V - s0L, gV * cvV - cvV);
+  double B = ddiv(e0L - e0V, gV * cvV - cvV);
+  double C = ddiv(gV * cvV - gL * cvL, gV * cvV - cvV);
+  double D = ddiv(gL * cvL - cvL, gV * cvV - cvV);
   int iteration = 0;
-  bool seeded = T0 > 0. && T0 < 0.5 * B / C;
-  double Tsat = seeded ? T0 : 0.1 * B / C, f = 0., df = 1.;
+  bool seeded = T0 > 0. && T0 < ddiv(0.5 * B, C);
+  double Tsat = seeded ? T0 : ddiv(0.1 * B, C), f = 0., df = 1.;
   // ln(p + pInf) of both phases do not depend on the iterate: evaluated once per solve (the same
   // values enter the same sum, so f has the bits of the reference's per-iteration evaluation)
   const double lnV = cr_log(p + piV), lnL = cr_log(p + piL);
   do {
-    Tsat -= f / df;
-    if (seeded && !(Tsat > 0. && Tsat < B / C)) {  // a seeded iterate left the root's branch
+    Tsat -= ddiv(f, df);
+    if (seeded && !(Tsat > 0. && Tsat < ddiv(B, C))) {  // a seeded iterate left the root's branch
       seeded = false;
-      Tsat = 0.1 * B / C;
+      Tsat = ddiv(0.1 * B, C);
     }
     iteration++;
     if (iteration > 50) {
       err = true;
       break;
     }
-    f = A + B / Tsat + C * cr_log(Tsat) - lnV + D * lnL;
-    df = C / Tsat - B / (Tsat * Tsat);
+    f = A + ddiv(B, Tsat) + C * cr_log(Tsat) - lnV + D * lnL;
+    df = ddiv(C, Tsat) - ddiv(B, Tsat * Tsat);
   } while (fabs(f) > 1e-10);
   if (pc) {
     pc->tsat_calls++;
     pc->tsat_iters += (unsigned int)iteration;
     pc->tsat_max = max(pc->tsat_max, (unsigned int)iteration);
   }
-  double dfdp = -1. / (p + piV) + D / (p + piL);
-  *dTsat = -dfdp / df;
+  double dfdp = ddiv(-1., p + piV) + ddiv(D, p + piL);
+  *dTsat = ddiv(-dfdp, df);
   return Tsat;
 }
 
@@ -657,23 +671,23 @@ __device__ __forceinline__ double eos_rho_sat(const EosParams& q, double eps, do
   double g1cvT = (q.gamma - 1.) * q.cv * Tsat;
   double den = (q.type == ECG_EOS_NASG) ? g1cvT + q.b * (p + q.pinf) : g1cvT;
   double d = (q.gamma - 1.) * q.cv * Tsat - pp * (q.gamma - 1.) * q.cv * dTsat;
-  *drhodp = d / dmax(den * den, eps);
-  return pp / dmax(den, eps);
+  *drhodp = ddiv(d, dmax(den * den, eps));
+  return ddiv(pp, dmax(den, eps));
 }
 
 // computeDensityEnergySaturation (EosIG.cpp:184, EosSG.cpp:186, EosNASG.cpp:203)
 __device__ __forceinline__ double eos_rhoe_sat(const EosParams& q, double p, double rho, double drhodp,
                                                double* drhoedp) {
   if (q.type == ECG_EOS_IG) {
-    *drhoedp = 1. / (q.gamma - 1.) + drhodp * q.eref;
-    return p / (q.gamma - 1.) + rho * q.eref;
+    *drhoedp = ddiv(1., q.gamma - 1.) + drhodp * q.eref;
+    return ddiv(p, q.gamma - 1.) + rho * q.eref;
   }
   if (q.type == ECG_EOS_SG) {
-    *drhoedp = 1. / (q.gamma - 1.) + drhodp * q.eref;
-    return (p + q.gamma * q.pinf) / (q.gamma - 1.) + rho * q.eref;
+    *drhoedp = ddiv(1., q.gamma - 1.) + drhodp * q.eref;
+    return ddiv(p + q.gamma * q.pinf, q.gamma - 1.) + rho * q.eref;
   }
-  *drhoedp = (1. - rho * q.b) / (q.gamma - 1.) + drhodp * (q.eref - q.b * (p + q.gamma * q.pinf) / (q.gamma - 1.));
-  return (p + q.gamma * q.pinf) * (1. - rho * q.b) / (q.gamma - 1.) + rho * q.eref;
+  *drhoedp = ddiv(1. - rho * q.b, q.gamma - 1.) + drhodp * (q.eref - ddiv(q.b * (p + q.gamma * q.pinf), q.gamma - 1.));
+  return ddiv((p + q.gamma * q.pinf) * (1. - rho * q.b), q.gamma - 1.) + rho * q.eref;
 }
 
 // RelaxationPTMu::relaxation src/Relaxations/RelaxationPTMu.cpp:73-200.  rhomix / emix are the
@@ -728,7 +742,7 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
   double Tstart = T_seed;  // start of the next T_sat solve (seeded form)
   if (p_seed > 0.) pStar = p_seed;
   do {
-    pStar -= f / df;
+    pStar -= ddiv(f, df);
     iteration++;
     if (iteration > 50) {
       err = true;
@@ -740,9 +754,9 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
     if (T_seed > 0.) Tstart = Tsat;
     rhoLSat = eos_rho_sat(EL, M.eps, pStar, Tsat, dTsat, &drhoLSat);
     rhoVSat = eos_rho_sat(EV, M.eps, pStar, Tsat, dTsat, &drhoVSat);
-    aLSat = (rho - rhoVSat) / (rhoLSat - rhoVSat);
-    daLSat = (-drhoVSat * (rhoLSat - rhoVSat) - (rho - rhoVSat) * (drhoLSat - drhoVSat)) /
-             ((rhoLSat - rhoVSat) * (rhoLSat - rhoVSat));
+    aLSat = ddiv(rho - rhoVSat, rhoLSat - rhoVSat);
+    daLSat = ddiv(-drhoVSat * (rhoLSat - rhoVSat) - (rho - rhoVSat) * (drhoLSat - drhoVSat),
+                  (rhoLSat - rhoVSat) * (rhoLSat - rhoVSat));
     aVSat = 1. - aLSat;
     daVSat = -daLSat;
     f = rhoe;
@@ -751,8 +765,8 @@ __device__ __forceinline__ bool relax_ptmu(const Model<NP>& M, int liq, int vap,
     rhoeVSat = eos_rhoe_sat(EV, pStar, rhoVSat, drhoVSat, &drhoeVSat);
     f -= (aLSat * rhoeLSat + aVSat * rhoeVSat);
     df -= (daLSat * rhoeLSat + aLSat * drhoeLSat + daVSat * rhoeVSat + aVSat * drhoeVSat);
-    f /= rhoe;
-    df /= rhoe;
+    f = ddiv(f, rhoe);
+    df = ddiv(df, rhoe);
   } while (fabs(f) > 1e-10);
   if (pc) {
     pc->solve = 1;
@@ -787,7 +801,7 @@ __device__ __forceinline__ double correction_pressure(const Model<NP>& M, const 
     pp -= a[k] * (gpi * (1. - r[k] * cov) + r[k] * q.eref);
     denom += a[k] * ig * (1. - r[k] * cov);
   }
-  return pp / denom;
+  return ddiv(pp, denom);
 }
 
 }  // namespace ecg

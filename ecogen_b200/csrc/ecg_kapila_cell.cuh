@@ -71,11 +71,11 @@ __device__ ECG_RECON_INLINE void reconstruct_side(const Model<NP>& M, const Step
     const double sg = (hi - lo > 0.) ? 1. : -1.;
     const double qmin = dmin(hi, lo);
     const double qmax = dmax(hi, lo) - qmin;
-    const double C = (alphaCell - qmin + 1.e-20) / (qmax + 1.e-20);
+    const double C = ddiv(alphaCell - qmin + 1.e-20, qmax + 1.e-20);
     const double B = exp(sg * beta * (2. * C - 1.));
-    const double A = (B / P.thinc_cosh - 1.) / P.thinc_tanh;
+    const double A = ddiv(ddiv(B, P.thinc_cosh) - 1., P.thinc_tanh);
     double na = right ? qmin + 0.5 * qmax * (1. + sg * A)
-                      : qmin + 0.5 * qmax * (1. + sg * (P.thinc_tanh + A) / (1. + A * P.thinc_tanh));
+                      : qmin + 0.5 * qmax * (1. + ddiv(sg * (P.thinc_tanh + A), 1. + A * P.thinc_tanh));
     if (na < eps) na = eps;
     if (na > 1. - eps) na = 1. - eps;
     t.a[0] = na;
@@ -207,7 +207,7 @@ template <int NP>
 __device__ __forceinline__ double wall_pstar(const Thermo<NP>& t, const double ul[3], double lcfl, double& dtmax) {
   const double uL = ul[0], cL = t.cF, pL = t.pm, rhoL = t.rho;
   const double sL = dmin(uL - cL, -uL - cL);
-  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * lcfl / fabs(sL));
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * lcfl, fabs(sL)));
   return rhoL * (uL - sL) * uL + pL;
 }
 
@@ -292,15 +292,15 @@ __device__ __forceinline__ void kapila_rebuild(const StepParams& P, const Model<
   double rhoMel = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
-    aa[k] /= un_sum;
+    aa[k] = ddiv(aa[k], un_sum);
     rhoMel += am[k];
     a[k] = aa[k];
-    r[k] = am[k] / dmax(aa[k], M.eps);
-    if (M.eos[k].type == ECG_EOS_NASG && r[k] > 1. / M.eos[k].b - 1.) {  // verifyAndCorrectDensityMax(mass)
-      r[k] = 1. / M.eos[k].b - 1.;
-      a[k] = am[k] / r[k];
+    r[k] = ddiv(am[k], dmax(aa[k], M.eps));
+    if (M.eos[k].type == ECG_EOS_NASG && r[k] > ddiv(1., M.eos[k].b) - 1.) {  // verifyAndCorrectDensityMax(mass)
+      r[k] = ddiv(1., M.eos[k].b) - 1.;
+      a[k] = ddiv(am[k], r[k]);
     }
-    double ek = ae[k] / dmax(am[k], M.eps);
+    double ek = ddiv(ae[k], dmax(am[k], M.eps));
     pk[k] = eos_p(M.eos[k], M.eps, r[k], ek);
     phase_fix_ar(M.eps, a[k], r[k]);
     pk[k] = eos_fix_p(M.eos[k], pk[k]);
@@ -309,12 +309,12 @@ __device__ __forceinline__ void kapila_rebuild(const StepParams& P, const Model<
   double usq = 0.;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    u[d] = amom[d] / rhoMel;
+    u[d] = ddiv(amom[d], rhoMel);
     if (fabs(u[d]) < 1.e-8) u[d] = 0.;
     usq += u[d] * u[d];
   }
   cp.usq = usq;
-  cp.E = aE / rhoMel;
+  cp.E = ddiv(aE, rhoMel);
   // mixture density (and internal energy for p-T-mu) of the rebuilt state
   double rhomix = 0.;
 #pragma unroll
@@ -345,7 +345,7 @@ __device__ __forceinline__ double rebuilt_emix(const Model<NP>& M, const double 
   double emix = 0.;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
-    double Y = a[k] * r[k] / dmax(rhomix, M.eps);
+    double Y = ddiv(a[k] * r[k], dmax(rhomix, M.eps));
     emix += Y * eos_e(M.eos[k], M.eps, r[k], p[k]);
   }
   return emix;
@@ -411,21 +411,21 @@ __device__ __forceinline__ void relax_pt(const Model<NP>& M, double a[NP], doubl
   const double pInf1 = (E1.type == ECG_EOS_IG) ? 0. : E1.pinf, pInf2 = (E2.type == ECG_EOS_IG) ? 0. : E2.pinf;
   const double q = Y[0] * E1.eref + Y[1] * E2.eref;
   const double cvMel = Y[0] * E1.cv + Y[1] * E2.cv;
-  const double A1 = Y[0] * (E1.gamma - 1.) * E1.cv / cvMel * (rho0 * (emix - q) - pInf1);
-  const double A2 = Y[1] * (E2.gamma - 1.) * E2.cv / cvMel * (rho0 * (emix - q) - pInf2);
+  const double A1 = ddiv(Y[0] * (E1.gamma - 1.) * E1.cv, cvMel) * (rho0 * (emix - q) - pInf1);
+  const double A2 = ddiv(Y[1] * (E2.gamma - 1.) * E2.cv, cvMel) * (rho0 * (emix - q) - pInf2);
   const double pressure = 0.5 * (A1 + A2 - (pInf1 + pInf2)) +
-                          sqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
+                          dsqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
   double temperature = 0.;
-  temperature += Y[0] * (E1.gamma - 1.) * E1.cv / (pressure + pInf1);
-  temperature += Y[1] * (E2.gamma - 1.) * E2.cv / (pressure + pInf2);
-  temperature = 1. / (temperature * rho0);
+  temperature += ddiv(Y[0] * (E1.gamma - 1.) * E1.cv, pressure + pInf1);
+  temperature += ddiv(Y[1] * (E2.gamma - 1.) * E2.cv, pressure + pInf2);
+  temperature = ddiv(1., temperature * rho0);
   double rS[2], aS[2];
 #pragma unroll
   for (int k = 0; k < 2; k++) {
     const EosParams& E = M.eos[k];
     const double den = dmax((E.gamma - 1.) * E.cv * temperature, M.eps);
-    rS[k] = (E.type == ECG_EOS_IG) ? pressure / den : (pressure + E.pinf) / den;
-    aS[k] = a[k] * r[k] / rS[k];
+    rS[k] = (E.type == ECG_EOS_IG) ? ddiv(pressure, den) : ddiv(pressure + E.pinf, den);
+    aS[k] = ddiv(a[k] * r[k], rS[k]);
   }
 #pragma unroll
   for (int k = 0; k < 2; k++) {
@@ -521,7 +521,7 @@ __device__ __forceinline__ void kapila_finish(const StepParams& P, const Model<N
     double Y[NP], emix = 0.;
 #pragma unroll
     for (int k = 0; k < NP; k++) {
-      Y[k] = a0[k] * r0[k] / dmax(rhomix, M.eps);
+      Y[k] = ddiv(a0[k] * r0[k], dmax(rhomix, M.eps));
       emix += Y[k] * eos_e(M.eos[k], M.eps, r0[k], p0[k]);
     }
     relax_pt<NP>(M, a, r, pk, Y, emix, rhomix);

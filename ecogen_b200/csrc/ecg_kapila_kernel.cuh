@@ -150,23 +150,23 @@ __global__ void __launch_bounds__(KapilaStep<NP, DIM, PASS, NTM>::NTH,
 #pragma unroll
           for (int f = 0; f < FL::NSL + NTM; f++) ssl[f * SS + e] = 0.;
           const double wd = G.wslope[2 * ax + sd];
-          if (fabs(wd) > 1.e-8) ssl[(3 * NP + ax) * SS + e] = sq[(FL::U + ax) * RS + (sd ? rl : rr)] / wd;
+          if (fabs(wd) > 1.e-8) ssl[(3 * NP + ax) * SS + e] = ddiv(sq[(FL::U + ax) * RS + (sd ? rl : rr)], wd);
           continue;
         }
         double d = G.dcc[ax][gl];
 #pragma unroll
         for (int k = 0; k < NP; k++) {
-          ssl[k * SS + e] = (sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl]) / d;
-          ssl[(NP + k) * SS + e] = (sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl]) / d;
+          ssl[k * SS + e] = ddiv(sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl], d);
+          ssl[(NP + k) * SS + e] = ddiv(sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl], d);
           double pr = eos_fix_p(M.eos[k], sq[FL::P * RS + rr]), pl = eos_fix_p(M.eos[k], sq[FL::P * RS + rl]);
-          ssl[(2 * NP + k) * SS + e] = (pr - pl) / d;
+          ssl[(2 * NP + k) * SS + e] = ddiv(pr - pl, d);
         }
 #pragma unroll
         for (int dd = 0; dd < DIM; dd++)
-          ssl[(3 * NP + dd) * SS + e] = (sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl]) / d;
+          ssl[(3 * NP + dd) * SS + e] = ddiv(sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl], d);
 #pragma unroll
         for (int j = 0; j < NTM; j++)  // Transport::computeSlopeTransport
-          if (j < P.ntr) ssl[(FL::NSL + j) * SS + e] = (str[j * RS + rr] - str[j * RS + rl]) / d;
+          if (j < P.ntr) ssl[(FL::NSL + j) * SS + e] = ddiv(str[j * RS + rr] - str[j * RS + rl], d);
       }
       __syncthreads();
     }

@@ -163,20 +163,20 @@ __global__ void __launch_bounds__(FaceTile<AX>::NTH, DIM == 2 ? ECG_FACE_MINB_2D
 #pragma unroll
         for (int f = 0; f < FL::NSL; f++) ssl[f * SS + e] = 0.;
         const double wd = G.wslope[2 * AX + sd];
-        if (fabs(wd) > 1.e-8) ssl[(3 * NP + AX) * SS + e] = sq[(FL::U + AX) * RS + (sd ? rl : rr)] / wd;
+        if (fabs(wd) > 1.e-8) ssl[(3 * NP + AX) * SS + e] = ddiv(sq[(FL::U + AX) * RS + (sd ? rl : rr)], wd);
         continue;
       }
       const double d = G.dcc[AX][gl];
 #pragma unroll
       for (int k = 0; k < NP; k++) {
-        ssl[k * SS + e] = (sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl]) / d;
-        ssl[(NP + k) * SS + e] = (sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl]) / d;
+        ssl[k * SS + e] = ddiv(sq[(FL::A + k) * RS + rr] - sq[(FL::A + k) * RS + rl], d);
+        ssl[(NP + k) * SS + e] = ddiv(sq[(FL::R + k) * RS + rr] - sq[(FL::R + k) * RS + rl], d);
         double pr = eos_fix_p(M.eos[k], sq[FL::P * RS + rr]), pl = eos_fix_p(M.eos[k], sq[FL::P * RS + rl]);
-        ssl[(2 * NP + k) * SS + e] = (pr - pl) / d;
+        ssl[(2 * NP + k) * SS + e] = ddiv(pr - pl, d);
       }
 #pragma unroll
       for (int dd = 0; dd < DIM; dd++)
-        ssl[(3 * NP + dd) * SS + e] = (sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl]) / d;
+        ssl[(3 * NP + dd) * SS + e] = ddiv(sq[(FL::U + dd) * RS + rr] - sq[(FL::U + dd) * RS + rl], d);
     }
     __syncthreads();
   }

@@ -171,7 +171,7 @@ __device__ __forceinline__ double cell_coefA(const Geometry& G, int ax, int i, i
   const double dx = G.dsz[0][i], dy = G.dsz[1][j], dz = G.dsz[2][k];
   const double vol = dx * dy * dz;
   const double s = (ax == 0) ? dy * dz : ((ax == 1) ? dx * dz : dx * dy);
-  return s / vol * 1.;
+  return ddiv(s, vol) * 1.;
 }
 
 // Bounds-checked builds (-DECG_BOUNDS_CHECK, libecg_bounds.so): every state, face-array and output

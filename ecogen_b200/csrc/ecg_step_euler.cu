@@ -61,10 +61,10 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
   double uR = ur[0], vR = ur[1], wR = ur[2], pR = R.p, rhoR = R.rho, cR = R.c, ER = R.E;
   double sL = dmin(uL - cL, uR - cR);
   double sR = dmax(uR + cR, uL + cL);
-  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * dxL / fabs(sL));
-  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, 1. * dxR / fabs(sR));
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * dxL, fabs(sL)));
+  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * dxR, fabs(sR)));
   double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
-  double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+  double sM = ddiv(pR - pL + mL * uL - mR * uR, mL - mR);
   if (fabs(sM) < 1.e-8) sM = 0.;
   if (sM_out) *sM_out = sM;
   if (sL > 0.) {
@@ -81,8 +81,8 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
     FE = (rhoR * ER + pR) * uR;
   } else if (sM >= 0.) {
     double pStar = mL * (sM - uL) + pL;
-    double rhoStar = mL / (sL - sM);
-    double Estar = EL + (sM - uL) * (sM + pL / mL);
+    double rhoStar = ddiv(mL, sL - sM);
+    double Estar = EL + (sM - uL) * (sM + ddiv(pL, mL));
     Fm = rhoStar * sM;
     Fn[0] = rhoStar * sM * sM + pStar;
     Fn[1] = rhoStar * sM * vL;
@@ -90,8 +90,8 @@ __device__ __forceinline__ void hllc_euler(const EulerSide& L, const double ul[3
     FE = (rhoStar * Estar + pStar) * sM;
   } else {
     double pStar = mR * (sM - uR) + pR;
-    double rhoStar = mR / (sR - sM);
-    double Estar = ER + (sM - uR) * (sM + pR / mR);
+    double rhoStar = ddiv(mR, sR - sM);
+    double Estar = ER + (sM - uR) * (sM + ddiv(pR, mR));
     Fm = rhoStar * sM;
     Fn[0] = rhoStar * sM * sM + pStar;
     Fn[1] = rhoStar * sM * vR;
@@ -185,15 +185,15 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
 #pragma unroll
           for (int f = 0; f < K::NSL + NTM; f++) ssl[f * SS + e] = 0.;
           const double wd = G.wslope[2 * ax + sd];
-          if (fabs(wd) > 1.e-8) ssl[(2 + ax) * SS + e] = sq[(2 + ax) * RS + (sd ? rl : rr)] / wd;
+          if (fabs(wd) > 1.e-8) ssl[(2 + ax) * SS + e] = ddiv(sq[(2 + ax) * RS + (sd ? rl : rr)], wd);
           continue;
         }
         double d = G.dcc[ax][gl];
 #pragma unroll
-        for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = (sq[f * RS + rr] - sq[f * RS + rl]) / d;
+        for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = ddiv(sq[f * RS + rr] - sq[f * RS + rl], d);
 #pragma unroll
         for (int t = 0; t < NTM; t++)  // Transport::computeSlopeTransport
-          if (t < P.ntr) ssl[(K::NSL + t) * SS + e] = (str[t * RS + rr] - str[t * RS + rl]) / d;
+          if (t < P.ntr) ssl[(K::NSL + t) * SS + e] = ddiv(str[t * RS + rr] - str[t * RS + rl], d);
       }
       __syncthreads();
     }
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
         // ModEuler::solveRiemannWall src/Models/Euler/ModEuler.cpp:368-409
         const double uL = ul[0], cL = S.c, pL = S.p, rhoL = S.rho;
         const double sL = dmin(uL - cL, -uL - cL);
-        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, 1. * cell_lcfl(G, gc[0], gc[1], gc[2]) / fabs(sL));
+        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(1. * cell_lcfl(G, gc[0], gc[1], gc[2]), fabs(sL)));
         wallp[ax] = rhoL * uL * (uL - sL) + pL;
       }
     }
@@ -406,11 +406,11 @@ __global__ void __launch_bounds__(EulerStep<DIM, PASS, NTM>::NTH,
     aE = aE * scale + 1. * (rn * En);
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      u[d] = amom[d] / am;
+      u[d] = ddiv(amom[d], am);
       if (fabs(u[d]) < 1.e-8) u[d] = 0.;
       usq += u[d] * u[d];
     }
-    double E = aE / am;
+    double E = ddiv(aE, am);
     double e = E - 0.5 * usq;
     double p = eos_p(q, eps, am, e);
     P.out[cell] = am;

@@ -56,7 +56,7 @@ __device__ __forceinline__ double pt_pinf(const EosParams& q) { return q.type ==
 // computeDensity(p, T) of an IG or SG phase (EosIG.cpp:85, EosSG.cpp:87).
 __device__ __forceinline__ double pt_rho(const EosParams& q, double p, double T) {
   const double den = dmax(((q.gamma - 1.) * q.cv * T), 0.);
-  return q.type == ECG_EOS_IG ? p / den : (p + q.pinf) / den;
+  return q.type == ECG_EOS_IG ? ddiv(p, den) : ddiv(p + q.pinf, den);
 }
 
 // One side of a face (or a cell) with its derived quantities.
@@ -80,7 +80,7 @@ __device__ __forceinline__ void pt_complete(const PtEos& M, PtSide& s) {
   for (int k = 0; k < 2; k++) s.rho += s.a[k] * s.r[k];
   double Y[2];
 #pragma unroll
-  for (int k = 0; k < 2; k++) Y[k] = s.a[k] * s.r[k] / s.rho;
+  for (int k = 0; k < 2; k++) Y[k] = ddiv(s.a[k] * s.r[k], s.rho);
   s.e = 0.;
   s.c = 0.;
 #pragma unroll
@@ -88,7 +88,7 @@ __device__ __forceinline__ void pt_complete(const PtEos& M, PtSide& s) {
     s.e += Y[k] * ek[k];
     s.c += Y[k] * ck[k] * ck[k];
   }
-  s.c = sqrt(s.c);
+  s.c = dsqrt(s.c);
 }
 
 // ModPTUEq::solveRiemannIntern src/Models/PTUEq/ModPTUEq.cpp:113-227 on face-frame velocities;
@@ -100,10 +100,10 @@ __device__ __forceinline__ void hllc_pt(const PtSide& L, const double ul[3], con
   const double uR = ur[0], cR = R.c, pR = R.p, rhoR = R.rho;
   const double sL = dmin(uL - cL, uR - cR);
   const double sR = dmax(uR + cR, uL + cL);
-  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, dxL / fabs(sL));
-  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, dxR / fabs(sR));
+  if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(dxL, fabs(sL)));
+  if (fabs(sR) > 1.e-3) dtmax = dmin(dtmax, ddiv(dxR, fabs(sR)));
   const double mL = rhoL * (sL - uL), mR = rhoR * (sR - uR);
-  double sM = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+  double sM = ddiv(pR - pL + mL * uL - mR * uR, mL - mR);
   if (fabs(sM) < 1.e-8) sM = 0.;
   if (sL >= 0.) {
 #pragma unroll
@@ -123,22 +123,22 @@ __device__ __forceinline__ void hllc_pt(const PtSide& L, const double ul[3], con
     FE = (rhoR * Et + pR) * uR;
   } else if (sM >= 0.) {
     const double Et = L.e + 0.5 * (ul[0] * ul[0] + ul[1] * ul[1] + ul[2] * ul[2]);
-    const double rhoStar = mL / (sL - sM);
-    const double EStar = Et + (sM - uL) * (sM + pL / mL);
+    const double rhoStar = ddiv(mL, sL - sM);
+    const double EStar = Et + (sM - uL) * (sM + ddiv(pL, mL));
     const double pStar = mL * (sM - uL) + pL;
 #pragma unroll
-    for (int k = 0; k < 2; k++) Fm[k] = L.a[k] * L.r[k] * (sL - uL) / (sL - sM) * sM;
+    for (int k = 0; k < 2; k++) Fm[k] = ddiv(L.a[k] * L.r[k] * (sL - uL), sL - sM) * sM;
     Fn[0] = rhoStar * sM * sM + pStar;
     Fn[1] = rhoStar * ul[1] * sM;
     Fn[2] = rhoStar * ul[2] * sM;
     FE = (rhoStar * EStar + pStar) * sM;
   } else {
     const double Et = R.e + 0.5 * (ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2]);
-    const double rhoStar = mR / (sR - sM);
-    const double EStar = Et + (sM - uR) * (sM + pR / mR);
+    const double rhoStar = ddiv(mR, sR - sM);
+    const double EStar = Et + (sM - uR) * (sM + ddiv(pR, mR));
     const double pStar = mR * (sM - uR) + pR;
 #pragma unroll
-    for (int k = 0; k < 2; k++) Fm[k] = R.a[k] * R.r[k] * (sR - uR) / (sR - sM) * sM;
+    for (int k = 0; k < 2; k++) Fm[k] = ddiv(R.a[k] * R.r[k] * (sR - uR), sR - sM) * sM;
     Fn[0] = rhoStar * sM * sM + pStar;
     Fn[1] = rhoStar * ur[1] * sM;
     Fn[2] = rhoStar * ur[2] * sM;
@@ -219,7 +219,7 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
         int rl = line * RL + (j - 1 + K::H), rr = rl + 1;
         double d = G.dcc[ax][gl];
 #pragma unroll
-        for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = (sq[f * RS + rr] - sq[f * RS + rl]) / d;
+        for (int f = 0; f < K::NSL; f++) ssl[f * SS + e] = ddiv(sq[f * RS + rr] - sq[f * RS + rl], d);
       }
       __syncthreads();
     }
@@ -282,11 +282,11 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
             const double sg = (hi - lo > 0.) ? 1. : -1.;
             const double qmin = dmin(hi, lo);
             const double qmax = dmax(hi, lo) - qmin;
-            const double C = (aCell - qmin + 1.e-20) / (qmax + 1.e-20);
+            const double C = ddiv(aCell - qmin + 1.e-20, qmax + 1.e-20);
             const double B = exp(sg * beta * (2. * C - 1.));
-            const double A = (B / P.thinc_cosh - 1.) / P.thinc_tanh;
+            const double A = ddiv(ddiv(B, P.thinc_cosh) - 1., P.thinc_tanh);
             double na = right ? qmin + 0.5 * qmax * (1. + sg * A)
-                              : qmin + 0.5 * qmax * (1. + sg * (P.thinc_tanh + A) / (1. + A * P.thinc_tanh));
+                              : qmin + 0.5 * qmax * (1. + ddiv(sg * (P.thinc_tanh + A), 1. + A * P.thinc_tanh));
             if (na < eps) na = eps;
             if (na > 1. - eps) na = 1. - eps;
             s.a[0] = na;
@@ -370,7 +370,7 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
         // ModPTUEq::solveRiemannWall src/Models/PTUEq/ModPTUEq.cpp:233-265 (first order only)
         const double uL = ul[0];
         const double sL = dmin(uL - s.c, -uL - s.c);
-        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, lc / fabs(sL));
+        if (fabs(sL) > 1.e-3) dtmax = dmin(dtmax, ddiv(lc, fabs(sL)));
         Fn[0] = s.rho * (uL - sL) * uL + s.p;
         Fn[1] = Fn[2] = 0.;
         to_global(ax, neg, Fn, Fg);
@@ -415,31 +415,31 @@ __global__ void ECG_PTUEQ_BOUNDS(DIM, PASS) k_ptueq_step(StepParams P, Geometry 
     double u[3] = {0., 0., 0.};
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      u[d] = mom[d] / rhoMel;
+      u[d] = ddiv(mom[d], rhoMel);
       if (fabs(u[d]) < 1.e-8) u[d] = 0.;
     }
-    const double ie = rE / rhoMel - 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double ie = ddiv(rE, rhoMel) - 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     const EosParams& E1 = M.e[0];
     const EosParams& E2 = M.e[1];
     const double pInf1 = pt_pinf(E1), pInf2 = pt_pinf(E2);
-    const double Y1 = m[0] / rhoMel, Y2 = m[1] / rhoMel;
+    const double Y1 = ddiv(m[0], rhoMel), Y2 = ddiv(m[1], rhoMel);
     const double q = Y1 * E1.eref + Y2 * E2.eref;
     const double cvMel = Y1 * E1.cv + Y2 * E2.cv;
-    const double A1 = Y1 * (E1.gamma - 1.) * E1.cv / cvMel * (rhoMel * (ie - q) - pInf1);
-    const double A2 = Y2 * (E2.gamma - 1.) * E2.cv / cvMel * (rhoMel * (ie - q) - pInf2);
+    const double A1 = ddiv(Y1 * (E1.gamma - 1.) * E1.cv, cvMel) * (rhoMel * (ie - q) - pInf1);
+    const double A2 = ddiv(Y2 * (E2.gamma - 1.) * E2.cv, cvMel) * (rhoMel * (ie - q) - pInf2);
     const double p = 0.5 * (A1 + A2 - (pInf1 + pInf2)) +
-                     sqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
+                     dsqrt(0.25 * (A2 - A1 - (pInf2 - pInf1)) * (A2 - A1 - (pInf2 - pInf1)) + A1 * A2);
     double Tm = 0.;
-    Tm += m[0] / rhoMel * (E1.gamma - 1.) * E1.cv / (p + pInf1);
-    Tm += m[1] / rhoMel * (E2.gamma - 1.) * E2.cv / (p + pInf2);
-    Tm = 1. / (Tm * rhoMel);
-    P.out[cell] = m[0] / pt_rho(E1, p, Tm);
-    P.out[nn + cell] = m[1] / pt_rho(E2, p, Tm);
+    Tm += ddiv(ddiv(m[0], rhoMel) * (E1.gamma - 1.) * E1.cv, p + pInf1);
+    Tm += ddiv(ddiv(m[1], rhoMel) * (E2.gamma - 1.) * E2.cv, p + pInf2);
+    Tm = ddiv(1., Tm * rhoMel);
+    P.out[cell] = ddiv(m[0], pt_rho(E1, p, Tm));
+    P.out[nn + cell] = ddiv(m[1], pt_rho(E2, p, Tm));
     P.out[(int64_t)FP * nn + cell] = p;
     P.out[(int64_t)FT * nn + cell] = Tm;
 #pragma unroll
     for (int d = 0; d < DIM; d++) P.out[(int64_t)(FU + d) * nn + cell] = u[d];
-    if (PASS != PASS_PRED) P.out[(int64_t)(FU + DIM) * nn + cell] = rE / rhoMel;
+    if (PASS != PASS_PRED) P.out[(int64_t)(FU + DIM) * nn + cell] = ddiv(rE, rhoMel);
   }
   __shared__ double red[32];
   double v = dtmax;

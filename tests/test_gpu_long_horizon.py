@@ -24,8 +24,8 @@ the change then spreads.  Two sensitivity builds of the oracle (oracle/ecg_powul
 ulp in 1 call in 100; oracle/ecg_crlog.h: a correctly rounded ln in the saturation solve, which
 differs from the host libm's in about 1 call in 600,000) run each checked case on the CPU, and the
 envelope of a field is the larger of their distances to the stock oracle (or to the reference, which
-the stock oracle matches bit for bit).  The GPU, which uses CUDA's pow and a correctly rounded ln,
-must stay within max(1e-12, 3 x envelope) per field.  Measured envelopes: the 2D shock-bubble
+the stock oracle matches bit for bit).  The GPU, whose pow (ecg::epow) is correctly rounded where
+glibc's is not (about 1 call in 1000) and whose ln is correctly rounded, must stay within max(1e-12, 3 x envelope) per field.  Measured envelopes: the 2D shock-bubble
 ~1e-14 (300 steps), the 3D three-phase cavity ~1e-15 but 9.7e-13 in p at 32^3 x 30 steps, the p-T-mu
 expansion 1.6e-12 in alpha and 4.5e-9 in p at 256^2 x 50 steps.
 """

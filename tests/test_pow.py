@@ -1,0 +1,81 @@
+"""The table-driven pow of the step kernels (ecogen_b200/csrc/ecg_pow.cuh), host build, against the host
+libm's pow (the reference's and the oracle's) and 300-bit arithmetic.
+
+The HLLC star state raises density ratios to the EOS gammas (EosSG::computePressureIsentropic
+src/Eos/EosSG.cpp).  The kernels compute those powers with ecg::epow, whose result before its single
+rounding is within about 2^-64 of x^y: it is the correctly rounded power except within that distance of
+a midpoint.  glibc's pow is accurate to about half an ulp plus 2^-7 ulp, so the two differ by one ulp in
+a small fraction of the calls, and there it is epow that is correctly rounded.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import mpmath as mp
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+P = C.POINTER(C.c_double)
+
+
+@pytest.fixture(scope="module")
+def host(tmp_path_factory):
+    so = str(tmp_path_factory.mktemp("pow") / "pow_host.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", so,
+                    os.path.join(ROOT, "tests", "pow", "pow_host.cpp")], check=True)
+    lib = C.CDLL(so)
+    for f in (lib.host_epow, lib.host_libm_pow):
+        f.argtypes = [P, P, P, C.c_long]
+
+    def run(fn, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(np.broadcast_to(y, x.shape), dtype=np.float64)
+        out = np.empty_like(x)
+        fn(x.ctypes.data_as(P), y.ctypes.data_as(P), out.ctypes.data_as(P), x.size)
+        return out
+
+    return lambda x, y: (run(lib.host_epow, x, y), run(lib.host_libm_pow, x, y))
+
+
+@pytest.mark.parametrize("lo,hi", [(0.996, 1.0), (0.999, 1.001), (0.9, 1.1), (0.2, 5.0), (1e-6, 1e6)])
+@pytest.mark.parametrize("g", [4.4, 1.4, 1.67, 2.35, 1.43])
+def test_epow_within_one_ulp_of_libm_and_rarely_different(host, lo, hi, g):
+    rng = np.random.default_rng(int(1e6 * lo) + int(100 * g))
+    x = np.exp(rng.uniform(np.log(lo), np.log(hi), 400_000))
+    a, b = host(x, g)
+    d = a.view(np.int64) - b.view(np.int64)
+    assert np.abs(d).max() <= 1
+    assert np.count_nonzero(d) / d.size < 2e-3
+
+
+def test_epow_is_the_correctly_rounded_one_where_it_differs(host):
+    mp.mp.prec = 300
+    rng = np.random.default_rng(5)
+    checked = epow_ok = 0
+    for lo, hi, g in ((0.996, 1.0, 4.4), (0.9, 1.1, 1.4), (0.2, 5.0, 1.67), (1e-6, 1e6, 4.4)):
+        x = np.exp(rng.uniform(np.log(lo), np.log(hi), 400_000))
+        a, b = host(x, g)
+        for i in np.nonzero(a != b)[0][:60]:
+            checked += 1
+            epow_ok += float(mp.power(mp.mpf(float(x[i])), mp.mpf(g))) == a[i]
+    assert checked >= 100
+    assert epow_ok >= 0.95 * checked
+
+
+def test_epow_error_below_half_an_ulp_near_one(host):
+    mp.mp.prec = 300
+    rng = np.random.default_rng(9)
+    x = np.exp(rng.uniform(np.log(0.98), np.log(1.02), 3000))
+    a, _ = host(x, 4.4)
+    worst = max(float(abs(mp.mpf(float(a[i])) - mp.power(mp.mpf(float(x[i])), mp.mpf(4.4))) /
+                      mp.mpf(float(np.spacing(a[i])))) for i in range(x.size))
+    assert worst <= 0.5
+
+
+def test_epow_outside_its_domain_is_libm_pow(host):
+    x = np.array([0.0, -0.0, -2.0, np.inf, np.nan, 1e-300, 1e300, 2.0, 2.0, 2.0])
+    y = np.array([1.4, 1.4, 1.4, 1.4, 1.4, 1.4, 1.4, 0.0, -1.5, 12.0])
+    a, b = host(x, y)
+    assert np.array_equal(a, b, equal_nan=True)
+    assert np.array_equal(np.signbit(a), np.signbit(b))
