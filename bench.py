@@ -187,13 +187,13 @@ NCU_TRAFFIC_PER_CELL = {("kapila", 2, 2, True, "fused", "pass2_cells"): 190.96,
 # kernel), ncu on one launch at 1536^2 (2D two-phase), 128^3 (3D three-phase) and 1024^2 (p-T-mu); the
 # traffic of a launch grows with its units, so a full-size launch is the per-unit figure times its units.
 _SPLIT_NCU = {  # (model, phases, dim): {slot: (FP64 thread instructions per unit, DRAM bytes per unit)}
-    ("kapila", 2, 2): {"pass1_faces_x": (877, 127), "pass1_faces_y": (902, 128), "pass1_cells": (482, 290),
-                       "pass2_faces_x": (877, 137), "pass2_faces_y": (902, 136), "pass2_cells": (481, 298)},
-    ("kapila", 3, 3): {"pass1_faces_x": (1184, 184), "pass1_faces_y": (1213, 181), "pass1_faces_z": (1210, 181),
-                       "pass1_cells": (843, 540), "pass2_faces_x": (1160, 193), "pass2_faces_y": (1211, 188),
-                       "pass2_faces_z": (1208, 189), "pass2_cells": (858, 549)},
-    ("kapila_ptmu", 2, 2): {"pass1_faces_x": (884, 102), "pass1_faces_y": (913, 104), "pass1_cells": (4158, 302),
-                            "pass2_faces_x": (884, 112), "pass2_faces_y": (913, 113), "pass2_cells": (4167, 310)},
+    ("kapila", 2, 2): {"pass1_faces_x": (742, 124), "pass1_faces_y": (751, 123), "pass1_cells": (498, 290),
+                       "pass2_faces_x": (742, 133), "pass2_faces_y": (751, 132), "pass2_cells": (498, 297)},
+    ("kapila", 3, 3): {"pass1_faces_x": (988, 184), "pass1_faces_y": (1003, 183), "pass1_faces_z": (997, 181),
+                       "pass1_cells": (879, 534), "pass2_faces_x": (982, 191), "pass2_faces_y": (1005, 191),
+                       "pass2_faces_z": (999, 190), "pass2_cells": (899, 542)},
+    ("kapila_ptmu", 2, 2): {"pass1_faces_x": (753, 98), "pass1_faces_y": (763, 97), "pass1_cells": (4251, 306),
+                            "pass2_faces_x": (753, 106), "pass2_faces_y": (763, 105), "pass2_cells": (4260, 313)},
 }
 for (_m, _np, _d), _slots in _SPLIT_NCU.items():
     for _slot, (_fp, _dram) in _slots.items():
@@ -280,9 +280,10 @@ def fp64_pipe_peak(device_index: int):
             "how": "148 SMs x 8 blocks x 256 threads, 8 independent DFMA chains per thread, best of 5 launches"}
 
 
-# FP64 thread instructions per cell of one launch of a step kernel, counted by ncu
-# (smsp__sass_thread_inst_executed_op_fp64_pred_on.sum / cells), keyed like NCU_TRAFFIC_PER_CELL.  The
-# count does not depend on the mesh size beyond boundary cells (measured at 512^2 in 2D, 64^3 in 3D).
+# FP64 thread instructions per unit (face or cell) of one launch of a step kernel, counted by ncu
+# (smsp__sass_thread_inst_executed_op_fp64_pred_on.sum / units), keyed like NCU_TRAFFIC_PER_CELL.  The
+# count does not depend on the mesh size beyond boundary cells (measured at 1536^2 in 2D, 128^3 in 3D,
+# 1024^2 for the p-T-mu workload).
 NCU_FP64_PER_CELL: dict = {(_m, _np, _d, True, "split", _slot): float(_fp)
                            for (_m, _np, _d), _slots in _SPLIT_NCU.items() for _slot, (_fp, _dram) in _slots.items()}
 

@@ -51,17 +51,19 @@ struct FaceKernelShape {
 };
 
 // Resident blocks per SM asked of the face and cell kernels (registers 65536 / (128 x MINB)).  Measured
-// on one B200 (cell-updates/s): 2D shock-bubble 2048^2: face kernels at 6 blocks 1459 M, at 8 1533 M,
-// cell kernel at 8 1470 M; 3D three-phase cavity 256^3: face kernels at 6 blocks 656 M, at 8 642 M, cell
-// kernel at 8 604 M.
+// on one B200 with the branch-free division (per-kernel CUDA events, 100 steps): 3D three-phase cavity
+// 256^3: face kernels at 6 blocks (80 registers) 2.35 / 2.11 ms (X / Y faces), at 5 2.43 / 2.13 ms;
+// cell kernel at 6 blocks 2.96 ms, at 5 (96 registers, fewer spills) 2.90 ms; 2D shock-bubble 2048^2:
+// face kernels at 8 blocks 0.353 / 0.328 ms, at 7 0.354 / 0.322 ms; cell kernel at 6 0.393 ms, at 5
+// 0.390 ms.
 #ifndef ECG_FACE_MINB_2D
-#define ECG_FACE_MINB_2D 8
+#define ECG_FACE_MINB_2D 7
 #endif
 #ifndef ECG_FACE_MINB_3D
 #define ECG_FACE_MINB_3D 6
 #endif
 #ifndef ECG_CELL_MINB
-#define ECG_CELL_MINB 6
+#define ECG_CELL_MINB 5
 #endif
 // The p-T-mu cell kernels run one warp per block: their cells take very different numbers of Newton
 // iterations, and in 4-warp blocks the warps that finish first waited at the block's counter reduction

@@ -38,11 +38,17 @@
 #include <cstring>
 
 #if defined(__CUDACC__)
+// inlining of epow itself (three call sites per face in a three-phase case): build-time choice
+#ifndef ECG_EPOW_INLINE
+#define ECG_EPOW_INLINE __forceinline__
+#endif
+#define ECG_EPOW_FN __device__ ECG_EPOW_INLINE
 #define ECG_POW_FN __device__ __forceinline__
 #define ECG_POW_TABLE static __device__ const
 #define ECG_POW_LD(p) __ldg(p)
 #else
 #define ECG_POW_FN static inline
+#define ECG_EPOW_FN static inline
 #define ECG_POW_TABLE static const
 #define ECG_POW_LD(p) (*(p))
 #endif
@@ -72,7 +78,7 @@ ECG_POW_FN double pow_outside(double x, double y) { return std::pow(x, y); }
 #endif
 
 // x^y by the tables (see above); pow_fma is the fused multiply-add of the device or of the host libm
-ECG_POW_FN double epow(double x, double y) {
+ECG_EPOW_FN double epow(double x, double y) {
   if (!(x >= 0x1p-60 && x <= 0x1p60 && y > 0. && y <= 10.)) return pow_outside(x, y);
   // ---- ln x = Lh + Ll
   const uint64_t ix = pow_bits(x);
