@@ -507,8 +507,6 @@ def bench_batch(args, rank, world, local):
                 "newton": {"relax_calls": st.relax_calls, "evals": st.newton_evals, "max": st.newton_max}}
         if seeded is not None:
             line["mlp_seeded"] = seeded
-        if warm is not None:
-            line["ptmu_warm_start"] = warm
         print(json.dumps(line))
 
 

@@ -42,7 +42,7 @@
 #ifndef ECG_EPOW_INLINE
 #define ECG_EPOW_INLINE __forceinline__
 #endif
-#define ECG_EPOW_FN __device__ ECG_EPOW_INLINE
+#define ECG_EPOW_FN static __device__ ECG_EPOW_INLINE  // internal linkage: one copy per unit when not inlined
 #define ECG_POW_FN __device__ __forceinline__
 #define ECG_POW_TABLE static __device__ const
 #define ECG_POW_LD(p) __ldg(p)

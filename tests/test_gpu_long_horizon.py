@@ -145,6 +145,7 @@ def test_long_horizon(key, cpu_results, tmp_path):
         env = max(rel_l1(display(e["fields"][name], name) if kind == "reference" else e["fields"][name], want)
                   for e in envs)
         tol = max(TOL, ENVELOPE_FACTOR * env)
+        print(f"{key}: {name} rel L1 {err:.3e} (envelope {env:.3e}, bound {tol:.3e})")
         assert err <= tol, f"{key}: {name} rel L1 {err:.3e} after {case.iterations} steps (envelope {env:.3e})"
     if kind == "oracle":
         for q in ("dt", "t"):
