@@ -13,3 +13,18 @@ void host_libm_pow(const double* x, const double* y, double* out, long n) {
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// ln x by elog (the first stage of epow, rounded once), and the host libm's log
+void host_elog(const double* x, double* out, long n) {
+  for (long i = 0; i < n; i++) {
+    out[i] = ecg::elog(x[i]);
+  }
+}
+
+void host_libm_log(const double* x, double* out, long n) {
+  for (long i = 0; i < n; i++) out[i] = std::log(x[i]);
+}
+
+}  // extern "C"

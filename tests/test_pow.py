@@ -1,5 +1,5 @@
-"""The table-driven pow of the step kernels (ecogen_b200/csrc/ecg_pow.cuh), host build, against the host
-libm's pow (the reference's and the oracle's) and 300-bit arithmetic.
+"""The table-driven pow and log of the step kernels (ecogen_b200/csrc/ecg_pow.cuh), host build, against
+the host libm's pow and log (the reference's and the oracle's) and 300-bit arithmetic.
 
 The HLLC star state raises density ratios to the EOS gammas (EosSG::computePressureIsentropic
 src/Eos/EosSG.cpp).  The kernels compute those powers with ecg::epow, whose result before its single
@@ -27,6 +27,8 @@ def host(tmp_path_factory):
     lib = C.CDLL(so)
     for f in (lib.host_epow, lib.host_libm_pow):
         f.argtypes = [P, P, P, C.c_long]
+    for f in (lib.host_elog, lib.host_libm_log):
+        f.argtypes = [P, P, C.c_long]
 
     def run(fn, x, y):
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -35,7 +37,18 @@ def host(tmp_path_factory):
         fn(x.ctypes.data_as(P), y.ctypes.data_as(P), out.ctypes.data_as(P), x.size)
         return out
 
-    return lambda x, y: (run(lib.host_epow, x, y), run(lib.host_libm_pow, x, y))
+    def run1(fn, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.empty_like(x)
+        fn(x.ctypes.data_as(P), out.ctypes.data_as(P), x.size)
+        return out
+
+    def call(x, y=None):
+        if y is None:  # the logarithm
+            return run1(lib.host_elog, x), run1(lib.host_libm_log, x)
+        return run(lib.host_epow, x, y), run(lib.host_libm_pow, x, y)
+
+    return call
 
 
 @pytest.mark.parametrize("lo,hi", [(0.996, 1.0), (0.999, 1.001), (0.9, 1.1), (0.2, 5.0), (1e-6, 1e6)])
@@ -79,3 +92,31 @@ def test_epow_outside_its_domain_is_libm_pow(host):
     a, b = host(x, y)
     assert np.array_equal(a, b, equal_nan=True)
     assert np.array_equal(np.signbit(a), np.signbit(b))
+
+
+@pytest.mark.parametrize("lo,hi", [(50.0, 2000.0), (1e3, 1e10)])
+def test_elog_equals_libm_on_the_saturation_solve_arguments(host, lo, hi):
+    """The p-T-mu saturation solve takes logs of temperatures and of pressures plus p_inf
+    (Mixture::computeTsat src/Models/Mixture.cpp:59-100); there elog and glibc's log agree."""
+    rng = np.random.default_rng(int(lo))
+    x = np.exp(rng.uniform(np.log(lo), np.log(hi), 1_000_000))
+    a, b = host(x)
+    assert np.array_equal(a, b)
+
+
+def test_elog_is_the_correctly_rounded_one_where_it_differs(host):
+    mp.mp.prec = 300
+    rng = np.random.default_rng(13)
+    x = np.exp(rng.uniform(np.log(0.5), np.log(2.0), 400_000))
+    a, b = host(x)
+    d = a.view(np.int64) - b.view(np.int64)
+    assert np.abs(d).max() <= 1
+    idx = np.nonzero(d)[0][:80]
+    assert len(idx) >= 20
+    assert all(float(mp.log(mp.mpf(float(x[i])))) == a[i] for i in idx)
+
+
+def test_elog_outside_its_domain_is_libm_log(host):
+    x = np.array([0.0, -0.0, -1.0, np.inf, np.nan, 5e-324, 1.0])
+    a, b = host(x)
+    assert np.array_equal(a, b, equal_nan=True)
