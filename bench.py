@@ -192,8 +192,8 @@ _SPLIT_NCU = {  # (model, phases, dim): {slot: (FP64 thread instructions per uni
     ("kapila", 3, 3): {"pass1_faces_x": (988, 184), "pass1_faces_y": (1003, 183), "pass1_faces_z": (997, 181),
                        "pass1_cells": (879, 534), "pass2_faces_x": (982, 191), "pass2_faces_y": (1005, 191),
                        "pass2_faces_z": (999, 190), "pass2_cells": (899, 542)},
-    ("kapila_ptmu", 2, 2): {"pass1_faces_x": (753, 98), "pass1_faces_y": (763, 97), "pass1_cells": (4251, 306),
-                            "pass2_faces_x": (753, 106), "pass2_faces_y": (763, 105), "pass2_cells": (4260, 313)},
+    ("kapila_ptmu", 2, 2): {"pass1_faces_x": (753, 96), "pass1_faces_y": (763, 95), "pass1_cells": (1722, 303),
+                            "pass2_faces_x": (753, 105), "pass2_faces_y": (763, 106), "pass2_cells": (1731, 310)},
 }
 for (_m, _np, _d), _slots in _SPLIT_NCU.items():
     for _slot, (_fp, _dram) in _slots.items():
