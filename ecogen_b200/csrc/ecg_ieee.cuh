@@ -13,23 +13,26 @@
 //     starts within one ulp of 1/b and returns RN(1/b) (Markstein's reciprocal theorem), except for a
 //     divisor whose significand is all ones, 2^e (2 - 2^-52): there 1/b lies just above the midpoint
 //     of its two neighbours and every step from either of them rounds a tie to the lower one, so y is
-//     moved up by one ulp; then q = RN(a y), the exact remainder r = a - b q (one FMA) and RN(q + r y), which is
-//     RN(a / b) when y = RN(1/b) and q is within one ulp of a / b (Markstein's division theorem,
-//     P. Markstein, "Computation of elementary functions on the IBM RISC System/6000 processor",
-//     IBM J. Res. Dev. 34(1), 1990).  The sign of a zero quotient is taken from q (the sign of a b).
+//     moved up by one ulp; then q = RN(a y), the exact remainder r = a - b q (one FMA) and
+//     RN(q + r y), which is RN(a / b) when y = RN(1/b) and q is within one ulp of a / b (Markstein's
+//     division theorem, P. Markstein, "Computation of elementary functions on the IBM RISC
+//     System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  The sign of a zero quotient is taken
+//     from q (the sign of a b).
 //   dsqrt(x): y0 = rsqrt.approx(x), two coupled Newton steps on g ~ sqrt(x) and h ~ 1/(2 sqrt(x)),
 //     then the exact residual d = x - g^2 (one FMA) and RN(g + d h) (the same correction scheme).
 //
 // Operands outside the normal range: a zero, infinite or NaN divisor or dividend makes the Newton
 // sequence NaN, and then the raw product a * rcp.approx(b), which is IEEE's answer there (+-inf, +-0
-// or NaN), is returned; dsqrt returns x for +-0 and +inf and NaN for x < 0.  What is not reproduced: subnormal operands and results (the
-// approximations flush them to zero) and divisors above 2^1022 in magnitude, far outside every
-// quantity of the step (densities, pressures, velocities, energies, cell sizes).
+// or NaN), is returned; dsqrt returns x for +-0 and +inf and NaN for x < 0.  What is not reproduced:
+// subnormal operands and results (the approximations flush them to zero) and divisors above 2^1022 in
+// magnitude, far outside every quantity of the step (densities, pressures, velocities, energies, cell
+// sizes).
 //
-// Both functions are checked against `/` and `sqrt()` bit for bit on 2.5e9 hashed operands over
-// binades 2^-300 .. 2^300 and on zero, infinite and NaN operands (tests/test_gpu_ieee.py runs the same check through the library), and every
-// parity test of the step kernels compares their fields with the oracle, which divides with the
-// host's IEEE division.
+// Both functions are checked against `/` and `sqrt()` bit for bit on hashed operands with exponents
+// from -500 to 500, exact quotients, all-ones-significand divisors and zero, infinite and NaN operands
+// (tests/test_gpu_ieee.py, 3e8 pairs per run; 2.5e9 when the method was chosen), and every parity
+// test of the step kernels compares their fields with the oracle, which divides with the host's IEEE
+// division.
 #pragma once
 
 namespace ecg {

@@ -44,7 +44,8 @@ __global__ void k_ieee_check(uint64_t seed, int emin, int emax, int iters, unsig
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nd = 0, ns = 0, n = 0;
   for (int it = 0; it < iters; it++) {
-    const uint64_t h1 = mix64(seed ^ (t * 0x100000001B3ull + (uint64_t)it)), h2 = mix64(h1 + 0x2545F4914F6CDD1Dull);
+    const uint64_t h1 = mix64(seed ^ (t * 0x100000001B3ull + (uint64_t)it));
+    const uint64_t h2 = mix64(h1 + 0x2545F4914F6CDD1Dull);
     double a = draw(h1, emin, emax), b = draw(h2, emin, emax);
     const uint64_t h3 = mix64(h2);
     if ((h3 & 255) == 0) a = (double)((h3 >> 8) & 1023) * 0.25 - 64.;
@@ -65,9 +66,10 @@ __global__ void k_ieee_check(uint64_t seed, int emin, int emax, int iters, unsig
 extern "C" {
 
 // Runs the check on the current device: blocks x 256 threads x iters operand pairs with exponents in
-// [emin, emax] (-500 <= emin <= emax <= 500, so that every quotient of finite operands is a normal number).  Writes counts[0] = pairs checked, counts[1] = divisions
-// and counts[2] = square roots that differ from CUDA's.  Returns 0 on success, otherwise the CUDA error
-// code, or -1 for an exponent range outside the limits.
+// [emin, emax] (-500 <= emin <= emax <= 500, so that every quotient of finite operands is a normal
+// number).  Writes counts[0] = pairs checked, counts[1] = divisions and counts[2] = square roots that
+// differ from CUDA's.  Returns 0 on success, otherwise the CUDA error code, or -1 for arguments outside
+// the limits.
 int ecg_probe_ieee_check(unsigned long long seed, int emin, int emax, int blocks, int iters,
                          unsigned long long counts[3]) {
   if (emin < -500 || emax > 500 || emin > emax || blocks <= 0 || iters <= 0) return -1;

@@ -7,7 +7,8 @@
 
 namespace {
 
-__global__ void k_epow(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ out, long n) {
+__global__ void k_epow(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ out,
+                       long n) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = ecg::epow(x[i], y[i]);
 }
