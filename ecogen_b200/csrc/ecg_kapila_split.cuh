@@ -65,6 +65,13 @@ struct FaceKernelShape {
 #ifndef ECG_CELL_MINB
 #define ECG_CELL_MINB 5
 #endif
+// The cell kernels with the learned pressure seed: the network's MMA fragments and features need
+// registers (at 96 the seeded kernels spilled about 600 B).  Measured (seeded arm, CUDA events, 100
+// steps): 3D cavity 256^3 at 5 blocks per SM 684.8 M cell-updates/s, at 4 (128 registers) 708.8 M, at 3
+// 681.9 M; 2D shock-bubble 2048^2 1668.8 M, 1851.1 M and 1700.3 M.
+#ifndef ECG_CELL_SEED_MINB
+#define ECG_CELL_SEED_MINB 4
+#endif
 // The p-T-mu cell kernels run one warp per block: their cells take very different numbers of Newton
 // iterations, and in 4-warp blocks the warps that finish first waited at the block's counter reduction
 // for the slowest one (barrier stalls were 5.6 of 12.4 cycles between issues on the 1024^2 expansion),
@@ -324,7 +331,8 @@ __device__ __forceinline__ void load_face_flux(const double* __restrict__ fl, in
 }
 
 template <int NP, int DIM, int PASS, bool PTMU, bool SEED, int TYPES>
-__global__ void __launch_bounds__(cell_threads(PTMU), PTMU ? ECG_CELL_PTMU_MINB : ECG_CELL_MINB)
+__global__ void __launch_bounds__(cell_threads(PTMU),
+                                  PTMU ? ECG_CELL_PTMU_MINB : (SEED ? ECG_CELL_SEED_MINB : ECG_CELL_MINB))
     k_kapila_cells(StepParams P, Geometry G, Model<NP> M0, const double* __restrict__ fx,
                    const double* __restrict__ fy, const double* __restrict__ fz) {
   const Model<NP> M = specialize_eos<NP, TYPES>(M0);
